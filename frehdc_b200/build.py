@@ -1,0 +1,84 @@
+"""Build of the in-tree native library ``frehdc_b200/libfrehd_b200.so``.
+
+All device code is compiled for sm_100a only.  The plain FP64 kernels are built
+with --fmad=false so that a*b+c is never contracted: together with an unchanged
+evaluation order this keeps their doubles identical to the host restatement of
+the reference step.  Objects are cached under ``frehdc_b200/_build`` and rebuilt
+when a source or header is newer.
+"""
+from __future__ import annotations
+
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(REPO, "include")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libfrehd_b200.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-fno-fast-math",
+          "-I", INCLUDE, "-I", CSRC]
+# Per-source extra flags: files whose kernels must reproduce host doubles exactly
+# are built without FMA contraction; the mixed-precision kernels keep FMA.
+EXTRA = {
+    "default": ["--fmad=false"],
+}
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _headers() -> list[str]:
+    return glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh")) + \
+        glob.glob(os.path.join(INCLUDE, "*.h"))
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build_library(verbose: bool = False, force: bool = False) -> str:
+    """Compile every CUDA/C++ source under csrc/ and link the shared library."""
+    os.makedirs(BUILD, exist_ok=True)
+    nvcc = _nvcc()
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
+    hdrs = _headers()
+    objs = []
+    for src in srcs:
+        base = os.path.basename(src)
+        obj = os.path.join(BUILD, base + ".o")
+        objs.append(obj)
+        if not force and not _stale(obj, [src] + hdrs + [__file__]):
+            continue
+        extra = EXTRA.get(base, EXTRA["default"])
+        cmd = [nvcc] + ARCH + COMMON + extra + ["-dc" if src.endswith(".cu") else "-c", src, "-o", obj]
+        if src.endswith(".cpp"):
+            cmd = [shutil.which("g++") or "g++", "-O2", "-fPIC", "-std=c++17", "-fno-fast-math",
+                   "-I", INCLUDE, "-I", CSRC, "-I", "/usr/local/cuda/include", "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    if force or _stale(LIB, objs):
+        cmd = [nvcc] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", LIB] + objs + \
+            ["-lcudart", "-lpthread"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build_library(verbose=True, force="--force" in sys.argv)

@@ -1,0 +1,182 @@
+/*
+ * subgrid_levels.h -- the subgrid lookup-table values of one coarse cell at one
+ * water level, computed from the cell's r x r fine bottom elevations.
+ *
+ * This is the single definition of the subgrid tables in this code base.  The
+ * host deck writer calls it to produce the V.dat/Z.dat/Vxp.dat/... files that the
+ * reference model reads (level-major, x fastest), and the device calls the very
+ * same inline function to evaluate a level on the fly (no N x Ne tables are held
+ * on the GPU for large domains).  Both sides therefore see identical doubles as
+ * long as neither contracts a*b+c into an FMA: the host is built without -mfma and
+ * the kernels that use this header are built with --fmad=false.
+ *
+ * Semantics follow the reference's MATLAB pre-processor (not runnable here):
+ *   preProcessing/script_CreateSubAreaWithBlockV16.m:153      bottom = min of block
+ *   preProcessing/script_CreateSubAreaWithBlockV16.m:159-175  bottomXP/YP
+ *   preProcessing/script_CreateSubAreaWithBlockV16.m:221-259  V, Z, Vxp/Vxm/Vyp/Vym
+ *   preProcessing/ComputeSubgridFaceArea.m:8-40               Np/Nm/Op/Om
+ * MATLAB arrays there are (x, y, level) with x the first (fastest) index, which is
+ * the reference C layout ii = j*nx + i.  Summation order is fixed here: MATLAB's
+ * sum(A(:)) is a flat x-fastest sweep and sum(sum(A)) is a sum of column (x) sums.
+ * The block-check option (checkBlock=1, bwlabel based) is not implemented.
+ *
+ * Fine array layout: zf[fj * fpitch + fi], fi in [0, nx*r) along x, fj along y.
+ */
+#ifndef FREHD_SUBGRID_LEVELS_H
+#define FREHD_SUBGRID_LEVELS_H
+
+#ifdef __CUDACC__
+#define FREHD_HD __host__ __device__ __forceinline__
+#else
+#define FREHD_HD static inline
+#endif
+
+typedef struct frehd_cell_levels {
+  double V, Z, Vxp, Vxm, Vyp, Vym, Np, Nm, Op, Om;
+} frehd_cell_levels;
+
+/* max(h - z, 0) of the pre-processor (script_CreateSubAreaWithBlockV16.m:221). */
+FREHD_HD double frehd_fine_depth(double h, double z) {
+  double d = h - z;
+  return d > 0.0 ? d : 0.0;
+}
+
+FREHD_HD double frehd_min2(double a, double b) { return b < a ? b : a; }
+
+/* Half-block split round(r/2) of the pre-processor (MATLAB round: .5 away from 0). */
+FREHD_HD int frehd_half(int r) { return (r + 1) / 2; }
+
+/*
+ * All ten table values of cell (i, j) at level h (level in the deck's own datum,
+ * i.e. without the model's bathymetry offset).
+ *   zf      fine bottom elevations, pitch fpitch (elements)
+ *   dA      fine pixel area dxf*dyf, dxf fine width (face areas use dxf, as in
+ *           ComputeSubgridFaceArea.m:18,30 which multiplies both by dx)
+ */
+FREHD_HD void frehd_cell_levels_at(const double *zf, long fpitch, int nx, int ny, int r,
+                                   int i, int j, double h, double dA, double dxf,
+                                   frehd_cell_levels *o) {
+  const long fi0 = (long)i * r, fj0 = (long)j * r;
+  const double *b = zf + fj0 * fpitch + fi0;
+  if (r == 1) {
+    /* script_CreateSubAreaWithBlockV16.m:246-255 (r == 1 branch) */
+    double d = frehd_fine_depth(h, b[0]);
+    o->V = dA * d;
+    o->Z = dA * (d > 0.0 ? 1.0 : 0.0);
+    o->Vxp = o->Vyp = o->Vxm = o->Vym = dA * d / 2.0;
+    o->Np = o->Op = o->Nm = o->Om = dxf * d;
+    return;
+  }
+  const int hf = frehd_half(r);
+  double sV = 0.0, cnt = 0.0, sxp = 0.0, sxm = 0.0, syp = 0.0, sym = 0.0;
+  for (int fj = 0; fj < r; ++fj) {
+    const double *row = b + (long)fj * fpitch;
+    double cxp = 0.0, cxm = 0.0, call = 0.0;
+    for (int fi = 0; fi < r; ++fi) {
+      double d = frehd_fine_depth(h, row[fi]);
+      sV += d;                         /* sum(localDepth(:)), x fastest */
+      if (d > 0.0) cnt += 1.0;         /* sum(sum(localDepth > 0)) */
+      if (fi < hf) cxm += d; else cxp += d;
+      call += d;                       /* column sum over x for this y */
+    }
+    sxp += cxp;                        /* sum(sum(localDepth(hf+1:r, :))) */
+    sxm += cxm;
+    if (fj < hf) sym += call; else syp += call;
+  }
+  o->V = dA * sV;
+  o->Z = dA * cnt;
+  o->Vxp = dA * sxp;
+  o->Vxm = dA * sxm;
+  o->Vyp = dA * syp;
+  o->Vym = dA * sym;
+
+  /* Np: own last x-row against the east neighbour's first x-row. */
+  double s = 0.0;
+  if (i < nx - 1) {
+    for (int fj = 0; fj < r; ++fj) {
+      const double *row = b + (long)fj * fpitch;
+      s += frehd_min2(frehd_fine_depth(h, row[r - 1]), frehd_fine_depth(h, row[r]));
+    }
+  } else {
+    for (int fj = 0; fj < r; ++fj) s += frehd_fine_depth(h, b[(long)fj * fpitch + r - 1]);
+  }
+  o->Np = s * dxf;
+  /* Nm: west neighbour's last x-row against own first x-row; the first column of
+   * the domain uses its own first row (ComputeSubgridFaceArea.m:23-24). */
+  s = 0.0;
+  if (i > 0) {
+    for (int fj = 0; fj < r; ++fj) {
+      const double *row = b + (long)fj * fpitch;
+      s += frehd_min2(frehd_fine_depth(h, row[-1]), frehd_fine_depth(h, row[0]));
+    }
+  } else {
+    for (int fj = 0; fj < r; ++fj) s += frehd_fine_depth(h, b[(long)fj * fpitch]);
+  }
+  o->Nm = s * dxf;
+  /* Op: own last y-row against the north neighbour's first y-row. */
+  s = 0.0;
+  if (j < ny - 1) {
+    const double *r0 = b + (long)(r - 1) * fpitch, *r1 = b + (long)r * fpitch;
+    for (int fi = 0; fi < r; ++fi)
+      s += frehd_min2(frehd_fine_depth(h, r0[fi]), frehd_fine_depth(h, r1[fi]));
+  } else {
+    const double *r0 = b + (long)(r - 1) * fpitch;
+    for (int fi = 0; fi < r; ++fi) s += frehd_fine_depth(h, r0[fi]);
+  }
+  o->Op = s * dxf;
+  /* Om: south neighbour's last y-row against own first y-row. */
+  s = 0.0;
+  if (j > 0) {
+    const double *r0 = b - fpitch;
+    for (int fi = 0; fi < r; ++fi)
+      s += frehd_min2(frehd_fine_depth(h, r0[fi]), frehd_fine_depth(h, b[fi]));
+  } else {
+    for (int fi = 0; fi < r; ++fi) s += frehd_fine_depth(h, b[fi]);
+  }
+  o->Om = s * dxf;
+}
+
+/* Coarse bottom and face-bottom elevations of cell (i, j) (host pre-processing;
+ * script_CreateSubAreaWithBlockV16.m:153,159-175). */
+FREHD_HD void frehd_cell_bottoms(const double *zf, long fpitch, int nx, int ny, int r,
+                                 int i, int j, double *bottom, double *bxp, double *byp) {
+  const long fi0 = (long)i * r, fj0 = (long)j * r;
+  const double *b = zf + fj0 * fpitch + fi0;
+  double m = b[0];
+  for (int fj = 0; fj < r; ++fj)
+    for (int fi = 0; fi < r; ++fi) {
+      double z = b[(long)fj * fpitch + fi];
+      if (z < m) m = z;
+    }
+  *bottom = m;
+  /* bottomXP = max over the two fine x-rows at the face of (min along y). */
+  double m0 = b[r - 1];
+  for (int fj = 1; fj < r; ++fj) m0 = frehd_min2(m0, b[(long)fj * fpitch + r - 1]);
+  if (i < nx - 1) {
+    double m1 = b[r];
+    for (int fj = 1; fj < r; ++fj) m1 = frehd_min2(m1, b[(long)fj * fpitch + r]);
+    *bxp = m1 > m0 ? m1 : m0;
+  } else {
+    *bxp = m0;
+  }
+  /* bottomYP = max over the two fine y-rows at the face of (min along x). */
+  const double *r0 = b + (long)(r - 1) * fpitch;
+  double n0 = r0[0];
+  for (int fi = 1; fi < r; ++fi) n0 = frehd_min2(n0, r0[fi]);
+  if (j < ny - 1) {
+    const double *r1 = b + (long)r * fpitch;
+    double n1 = r1[0];
+    for (int fi = 1; fi < r; ++fi) n1 = frehd_min2(n1, r1[fi]);
+    *byp = n1 > n0 ? n1 : n0;
+  } else {
+    *byp = n0;
+  }
+}
+
+/* Level h_k of the reference's level vector before the offset is added
+ * (subgrid.c:2118: allSurf[k] = surfmin + k*dsurf + offset, evaluated left to right). */
+FREHD_HD double frehd_level(double surfmin, double dsurf, int k) {
+  return surfmin + (double)k * dsurf;
+}
+
+#endif /* FREHD_SUBGRID_LEVELS_H */

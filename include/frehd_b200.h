@@ -1,0 +1,202 @@
+/*
+ * frehd_b200.h -- C ABI of the B200 implementation of FrehdC's semi-implicit
+ * (Casulli) time step with subgrid bathymetry.
+ *
+ * Everything here is plain C: integers, doubles and pointers to host arrays.
+ * Host arrays use the reference model's own linear layout (map.c:45-127):
+ *   interior cell (i, j)      -> ii = j*nx + i,            ii in [0, N),  N = nx*ny
+ *   ghost ring appended after the interior, N2ct = (nx+2)*(ny+2) entries in total:
+ *     [N,        N+nx)        row j = ny   (north / "jP" ghosts)
+ *     [N+nx,     N+2nx)       row j = -1   (south / "jM" ghosts)
+ *     [N+2nx,    N+2nx+ny)    column i = nx (east / "iP" ghosts)
+ *     [N+2nx+ny, N+2nx+2ny)   column i = -1 (west / "iM" ghosts)
+ *     N2ct-4 .. N2ct-1        corners (i,j) = (-1,ny), (nx,ny), (nx,-1), (-1,-1)
+ * An array documented as "N2ct" carries the ghost ring, "N" is interior only.
+ * Subgrid tables are level-major like the reference's all* arrays:
+ *   table[N*k + ii] is the value of cell ii at level k (subgrid.c:118-119).
+ *
+ * The device keeps every domain resident in HBM in a padded 2-D layout and only
+ * copies to the host when asked to.  All entry points return a status code
+ * (FREHD_OK == 0); none of them aborts the process.
+ */
+#ifndef FREHD_B200_H
+#define FREHD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+enum frehd_status {
+  FREHD_OK = 0,
+  FREHD_ERR_INVALID = 1,        /* bad argument, size or null pointer */
+  FREHD_ERR_UNSUPPORTED = 2,    /* a Config option this build does not implement */
+  FREHD_ERR_CUDA = 3,           /* CUDA runtime error (message: frehd_last_error) */
+  FREHD_ERR_NOMEM = 4,          /* device allocation failed */
+  FREHD_ERR_CG_NOCONVERGE = 5,  /* CG reached maxIter before ||r|| < eps*||b|| */
+  FREHD_ERR_CFL = 6,            /* max CFL > 20; the reference exits here (nsfunctions.c:1226-1231) */
+  FREHD_ERR_TIMEOUT = 7,        /* a bounded device-side wait gave up */
+  FREHD_ERR_STATE = 8           /* call out of order (e.g. step before geometry is set) */
+};
+
+/* Human-readable name of a status code. */
+const char *frehd_status_string(int status);
+/* Text of the last error raised in this thread (empty when none). */
+const char *frehd_last_error(void);
+/* Library version string. */
+const char *frehd_version(void);
+/* Number of CUDA devices visible to the library. */
+int frehd_device_count(int *count);
+
+/* ------------------------------------------------------------------ config */
+/*
+ * The fields of the reference's Config (configuration.h:4-111) that the step
+ * reads, with the same names and meaning.  frehd_config_defaults() fills in the
+ * values of the shipped data.dat (frehdc5+/data.dat:1-103).
+ */
+typedef struct frehd_config {
+  int nx, ny;                 /* interior cells (NX, NY with one rank) */
+  double dx, dy, dt;
+  double g, NUx, NUy, Kx, Ky;
+  double CDx, CDy, manningN, CDmax, hD, CwT;
+  int CDnotN, useThinLayer;
+  int useSubgrid, useSubDrag, staggeredV, useminA, useminV;
+  double dxf, dyf, subR;      /* fine grid and r = dx/dxf */
+  double surfmin, surfmax, dsurf;
+  int bcType;                 /* 1: tide on the YP row (j = ny-1) */
+  int tideLocFirstP, tideLocLengthP; /* tidal cells (tideLocFirstP + k, ny-1) */
+  int useScalar, scalarAdv, useConstTidePS;
+  double tidePS;
+  int useWind, useEvap, useRain, inflowLocLength, useSubStep, checkConservation;
+  double minDepth, wtfh, CFLl, CFLh;
+  double eps;                 /* CG stop: ||r||_2 < eps*||b||_2 (rtc.c:53) */
+  int maxIter;
+  double offset;              /* bathymetry offset -min(z) (bathymetry.c:98-102) */
+} frehd_config;
+
+void frehd_config_defaults(frehd_config *cfg);
+
+/* ------------------------------------------------------- host pre-processing */
+/*
+ * Subgrid tables of a deck from its fine bottoms (no GPU needed).  Replaces the
+ * reference's MATLAB pre-processor (preProcessing/script_CreateSubAreaWithBlockV16.m
+ * with checkBlock = 0) whose output files subgrid.c:2089-2284 reads.
+ *   zf      fine bottoms, zf[fj*fpitch + fi], (ny*r) rows of (nx*r) pixels
+ *   tables  10*Ne*N doubles: V, Z, Vxp, Vxm, Vyp, Vym, Np, Nm, Op, Om, each level-major
+ */
+int frehd_build_tables(const double *zf, long fpitch, int nx, int ny, int r,
+                       double dxf, double dyf, double surfmin, double dsurf, int Ne,
+                       double *tables);
+/* Coarse bottom.dat / bottomXP.dat / bottomYP.dat of a deck (N doubles each). */
+int frehd_build_bottoms(const double *zf, long fpitch, int nx, int ny, int r,
+                        double *bottom, double *bottomXP, double *bottomYP);
+
+/* ------------------------------------------------------------ one domain */
+typedef struct frehd_domain frehd_domain;
+
+/*
+ * State of one domain in the reference layout; every pointer may be NULL (skipped).
+ * Field names are those of Data (initialize.h:10-21), Sub (subgrid.h:8-29) and
+ * Bath (bathymetry.h:7-14).
+ */
+typedef struct frehd_state {
+  /* persistent model state */
+  double *surf;              /* N2ct  free surface incl. offset */
+  double *uuXP, *vvYP;       /* N2ct  face velocities */
+  double *S;                 /* N2ct  scalar */
+  double *depth;             /* N     cell depth */
+  double *CDXP, *CDYP;       /* N2ct  drag coefficients */
+  double *CFLx, *CFLy;       /* N2ct  previous step's CFL numbers (read by advection) */
+  double *V, *Z, *Nx, *Oy, *Vx, *Vy, *Zx, *Zy; /* N2ct subgrid geometry at the current level */
+  int *ind;                  /* N2ct  persistent subgrid level index */
+  /* static bathymetry */
+  double *bottomZ, *bottomXP, *bottomYP;      /* N2ct incl. offset */
+  /* per-step quantities (download only) */
+  double *surfOld;           /* N2ct  */
+  double *uuYP, *vvXP;       /* N     interpolated velocities (velocityInterp) */
+  double *EnXP, *EnYP;       /* N     explicit velocities after drag inversion */
+  double *cellV, *Sm;        /* N     cell volume and scalar mass after the update */
+  double *Fuu, *Fvv;         /* N2ct  face flow rates */
+} frehd_state;
+
+/* Per-domain counters of the last step. */
+typedef struct frehd_step_stats {
+  int step;                  /* tt of the last completed step */
+  int cg_iters;              /* CG iterations of the last solve */
+  int status;                /* status of the last step */
+  double cg_rel_residual;    /* ||r||/||b|| at exit */
+  double max_cflx, max_cfly; /* monitorCFL maxima (nsfunctions.c:1196-1223) */
+  int n_cfl_warn;            /* cells with CFL > 2 (the reference prints one line each) */
+  double volume;             /* sum of cellV over the domain after the step */
+} frehd_step_stats;
+
+/* Create an empty domain on CUDA device `device`.  Unsupported Config options
+ * give FREHD_ERR_UNSUPPORTED. */
+int frehd_domain_create(const frehd_config *cfg, int device, frehd_domain **out);
+int frehd_domain_destroy(frehd_domain *d);
+
+/* Geometry source, one of the two:
+ *   tables: the reference's subgrid tables (10*Ne*N, see frehd_build_tables);
+ *   fine bottoms: the r x r fine pixels; level values are evaluated on the device
+ *   with the same arithmetic as frehd_build_tables (no tables in HBM). */
+int frehd_domain_set_tables(frehd_domain *d, int Ne, const double *tables);
+int frehd_domain_set_fine_bottoms(frehd_domain *d, int r, const double *zf, long fpitch);
+
+/* Tidal elevation series bc->tideP (initialize.h:28-32), indexed by step tt. */
+int frehd_domain_set_tide(frehd_domain *d, int n, const double *tideP);
+
+/* Copy state in the reference layout to/from the device (NULL fields skipped). */
+int frehd_domain_upload_state(frehd_domain *d, const frehd_state *st);
+int frehd_domain_download_state(frehd_domain *d, frehd_state *st);
+
+/*
+ * Run the reference's initialisation sequence on the device (initialize.c:40-155,
+ * subgrid path) from the deck's coarse fields (N doubles each, deck datum, the
+ * offset is added here as in bathymetry.c:104-121 and initialize.c:401):
+ * bottom / bottomXP / bottomYP (bottom.dat, bottomXP.dat, bottomYP.dat), surf0,
+ * u0, v0 and S0 (surfic/uuic/vvic/scalaric.dat).  Geometry and the tide series
+ * must be set first.  round_trip_output applies the surface round trip through
+ * the output datum that DataOutput performs at tt = 0 (fileio.c:65-66,120-121).
+ */
+int frehd_domain_init(frehd_domain *d, const double *bottom, const double *bottomXP,
+                      const double *bottomYP, const double *surf0, const double *u0,
+                      const double *v0, const double *S0, int round_trip_output);
+
+/* One complete step tt (oneCompleteStep, nssolve.c:110-118) followed by
+ * monitorCFL (nsfunctions.c:1192-1232).  Returns FREHD_ERR_CFL when the max CFL
+ * exceeds 20 (the state is left as the reference leaves it before exiting). */
+int frehd_domain_step(frehd_domain *d, int tt);
+/* Steps t0 .. t0+nsteps-1 back to back without host synchronisation; the status
+ * is checked once at the end.  Stops early (and reports) on CFL > 20. */
+int frehd_domain_run(frehd_domain *d, int t0, int nsteps);
+
+/* Phases of one step, for parity testing against the reference's functions:
+ *   FREHD_PHASE_EXPLICIT  solveSourceTerm + matrixCoeffSub/adjust*Boundary (nssolve.c:121-166)
+ *   FREHD_PHASE_SOLVE     the free-surface solve (nsfunctions.c:1004-1017)
+ *   FREHD_PHASE_UPDATE    getFreeSurface .. enforceTidalBC, updateData, scalarTransport,
+ *                         monitorCFL (nssolve.c:169-290, scalar.c:30-57, nsfunctions.c:1192)
+ * FREHD_PHASE_UPDATE may take an externally solved surface (x_ext, N doubles in
+ * the reference's transposed order k = i*ny + j, as the laspack vector x). */
+enum { FREHD_PHASE_EXPLICIT = 1, FREHD_PHASE_SOLVE = 2, FREHD_PHASE_UPDATE = 3 };
+int frehd_domain_phase(frehd_domain *d, int phase, int tt, const double *x_ext);
+
+/* Download the assembled system of the last FREHD_PHASE_EXPLICIT in the
+ * reference's terms: GnCt/GnXP/GnXM/GnYP/GnYM (row-major, N each) and the
+ * right-hand side z (transposed order, N).  NULL pointers skipped. */
+int frehd_domain_download_system(frehd_domain *d, double *GnCt, double *GnXP, double *GnXM,
+                                 double *GnYP, double *GnYM, double *z);
+/* Download the last solution x (transposed order, N). */
+int frehd_domain_download_solution(frehd_domain *d, double *x);
+
+int frehd_domain_stats(frehd_domain *d, frehd_step_stats *out);
+/* Wait for all work queued on the domain's stream. */
+int frehd_domain_sync(frehd_domain *d);
+
+/* Solver options (defaults: warm start from the current surface, Jacobi PCG). */
+enum { FREHD_X0_ZERO = 0, FREHD_X0_SURFACE = 1 };
+int frehd_domain_set_solver(frehd_domain *d, int x0_mode);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FREHD_B200_H */

@@ -1,0 +1,64 @@
+"""Shared helpers of the parity tests (decks, phase comparison)."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+from frehdc_b200 import deck as D
+
+# Arrays of one step's state, in the reference layout, compared between runs.
+STATE = ["surf", "uuXP", "vvYP", "uuYP", "vvXP", "S", "depth", "CDXP", "CDYP", "CFLx", "CFLy",
+         "V", "Z", "Nx", "Oy", "Vx", "Vy", "Zx", "Zy", "ind"]
+TEMPS = ["surfOld", "EnXP", "EnYP", "DragXP", "DragYP", "Fuu", "Fvv", "cellV", "Sm", "rmvCFL",
+         "wtfXP", "wtfYP", "advX", "advY", "depthXP", "depthYP", "GnCt", "GnXP", "GnXM", "GnYP",
+         "GnYM", "z", "Vxp", "Vyp", "Vxm", "Vym", "Np", "Nm", "Op", "Om"]
+EXPLICIT_OUT = ["EnXP", "EnYP", "DragXP", "DragYP", "advX", "advY", "GnCt", "GnXP", "GnXM",
+                "GnYP", "GnYM", "z"]
+
+# The small decks of the CPU parity suite.
+SPECS = {
+    "wet48x40": D.DeckSpec(nx=48, ny=40, steps=30, seed=3),
+    "dry40x36": D.DeckSpec(nx=40, ny=36, steps=40, seed=5, dry_frac=0.3),
+    "dry37x29": D.DeckSpec(nx=37, ny=29, steps=40, seed=9, dry_frac=0.35, dt=2.0, depth_max=3.0),
+}
+
+_cache: dict = {}
+
+
+def deck_for(name: str, root: str):
+    """Generated deck (with tables) and its reference-format directory."""
+    if name in _cache:
+        return _cache[name]
+    spec = SPECS[name]
+    d = D.make_deck(spec, with_tables=True)
+    path = os.path.join(root, name)
+    D.write_reference_deck(d, path)
+    _cache[name] = (d, path)
+    return d, path
+
+
+def mismatches(a: dict, b: dict, names, exact: bool = True, rtol: float = 0.0):
+    """List of (name, count, first indices) where a[name] != b[name]."""
+    out = []
+    for n in names:
+        x = np.asarray(a[n], dtype=np.float64)
+        y = np.asarray(b[n], dtype=np.float64)
+        if x.shape != y.shape:
+            out.append((n, "shape", x.shape, y.shape))
+            continue
+        same = (x == y) | (np.isnan(x) & np.isnan(y))
+        if not exact:
+            scale = max(np.max(np.abs(y)), 1e-300)
+            same = np.abs(x - y) <= rtol * scale
+        bad = np.where(~same)[0]
+        if len(bad):
+            out.append((n, int(len(bad)), bad[:4].tolist(), x[bad[:2]].tolist(), y[bad[:2]].tolist()))
+    return out
+
+
+def max_rel(a, b) -> float:
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    scale = max(float(np.max(np.abs(b))), 1e-300)
+    return float(np.max(np.abs(a - b))) / scale

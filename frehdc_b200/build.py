@@ -28,6 +28,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-fno-fast-m
 # are built without FMA contraction; the mixed-precision kernels keep FMA.
 EXTRA = {
     "default": ["--fmad=false"],
+    "cg.cu": ["--fmad=true"],
 }
 
 

@@ -1,0 +1,737 @@
+// C ABI of one domain (include/frehd_b200.h): device allocation, layout
+// conversion, the host-side initialisation sequence and the step driver.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "domain.cuh"
+#include "frehd_internal.h"
+#include "kernels.cuh"
+
+using namespace frehd;
+
+#define CUDA_TRY(expr)                                                                 \
+  do {                                                                                 \
+    cudaError_t e_ = (expr);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(FREHD_ERR_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_),     \
+                  __FILE__, __LINE__);                                                 \
+  } while (0)
+
+struct frehd_domain {
+  frehd_config cfg;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Grid gr;
+  Params p;
+  long N = 0, T = 0;
+  double *surf[2] = {}, *depth[2] = {}, *S[2] = {};
+  int *ind[2] = {};
+  double *u = nullptr, *v = nullptr, *CDXP = nullptr, *CDYP = nullptr, *CFLx = nullptr,
+         *CFLy = nullptr;
+  double *V = nullptr, *Z = nullptr, *Nx = nullptr, *Oy = nullptr, *Vx = nullptr, *Vy = nullptr,
+         *Zx = nullptr, *Zy = nullptr;
+  double *bottomZ = nullptr, *bottomXP = nullptr, *bottomYP = nullptr;
+  double *EnXP = nullptr, *EnYP = nullptr, *Gx = nullptr, *Gy = nullptr, *Ct = nullptr,
+         *b = nullptr;
+  double *x = nullptr, *r = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr;
+  double *cellV = nullptr, *Sm = nullptr, *Fuu = nullptr, *Fvv = nullptr;
+  unsigned char *rmv = nullptr;
+  int *fix_list = nullptr;
+  double *partials = nullptr;
+  long npartials = 0;
+  double *tide = nullptr;
+  int ntide = 0;
+  double *tables = nullptr, *zf = nullptr;
+  Scratch *sc = nullptr;
+  StepOut *out = nullptr;
+  StepOut *out_host = nullptr;  // pinned
+  double *stage = nullptr;      // device staging, T doubles
+  double *stage2 = nullptr;
+  int cur = 0;
+  int x0_mode = FREHD_X0_SURFACE;
+  int cg_blocks = 1;
+  int geom_set = 0, ready = 0;
+  frehd_step_stats last{};
+  std::vector<void *> allocs;
+  // profiling: one event before each kernel of a step plus one after
+  int profiling = 0;
+  std::vector<cudaEvent_t> ev;
+  frehd_kernel_times times{};
+  long long iters_at_prof_start = 0;
+};
+
+namespace {
+
+template <class T>
+int dalloc(frehd_domain *d, T **p, long n) {
+  void *q = nullptr;
+  cudaError_t e = cudaMalloc(&q, sizeof(T) * (size_t)std::max(n, 1L));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(FREHD_ERR_NOMEM, "cudaMalloc of %ld bytes: %s", (long)(sizeof(T) * n),
+                cudaGetErrorString(e));
+  }
+  cudaMemsetAsync(q, 0, sizeof(T) * (size_t)std::max(n, 1L), d->stream);
+  d->allocs.push_back(q);
+  *p = (T *)q;
+  return FREHD_OK;
+}
+
+int check_config(const frehd_config *c) {
+  if (c->nx < 2 || c->ny < 2) return fail(FREHD_ERR_INVALID, "grid %d x %d too small", c->nx, c->ny);
+  if ((long)c->nx * c->ny > 2000000000L) return fail(FREHD_ERR_INVALID, "grid too large");
+  if (c->useSubgrid != 1) return fail(FREHD_ERR_UNSUPPORTED, "useSubgrid=%d (only 1)", c->useSubgrid);
+  if (c->staggeredV != 1) return fail(FREHD_ERR_UNSUPPORTED, "staggeredV=%d (only 1)", c->staggeredV);
+  if (c->useSubDrag != 0) return fail(FREHD_ERR_UNSUPPORTED, "useSubDrag=%d (only 0)", c->useSubDrag);
+  if (c->CDnotN != 0) return fail(FREHD_ERR_UNSUPPORTED, "CDnotN=%d (only 0)", c->CDnotN);
+  if (c->useminA != 0) return fail(FREHD_ERR_UNSUPPORTED, "useminA=%d (only 0)", c->useminA);
+  if (c->useminV == 1 || c->useminV == 2)
+    return fail(FREHD_ERR_UNSUPPORTED, "useminV=%d (1 and 2 not implemented)", c->useminV);
+  if (c->bcType != 1) return fail(FREHD_ERR_UNSUPPORTED, "bcType=%d (only 1)", c->bcType);
+  if (c->useWind || c->useEvap || c->useRain || c->inflowLocLength || c->useSubStep ||
+      c->checkConservation)
+    return fail(FREHD_ERR_UNSUPPORTED, "wind/evaporation/rain/inflow/sub-stepping not implemented");
+  if (c->useScalar && (c->scalarAdv != 1 || c->useConstTidePS != 1))
+    return fail(FREHD_ERR_UNSUPPORTED, "scalar: only scalarAdv=1 with a constant tidal scalar");
+  if (c->tideLocFirstP < 0 || c->tideLocLengthP < 0 || c->tideLocFirstP + c->tideLocLengthP > c->nx)
+    return fail(FREHD_ERR_INVALID, "tidal cells outside the YP row");
+  if (!(c->dsurf > 0) || !(c->dx > 0) || !(c->dy > 0) || !(c->dt > 0))
+    return fail(FREHD_ERR_INVALID, "dx, dy, dt and dsurf must be positive");
+  return FREHD_OK;
+}
+
+View make_view(const frehd_domain *d) {
+  View w;
+  w.p = d->p;
+  w.gr = d->gr;
+  const int c = d->cur, n = d->cur ^ 1;
+  w.surf_cur = d->surf[c]; w.surf_nxt = d->surf[n];
+  w.depth_cur = d->depth[c]; w.depth_nxt = d->depth[n];
+  w.S_cur = d->S[c]; w.S_nxt = d->S[n];
+  w.ind_cur = d->ind[c]; w.ind_nxt = d->ind[n];
+  w.u = d->u; w.v = d->v; w.CDXP = d->CDXP; w.CDYP = d->CDYP; w.CFLx = d->CFLx; w.CFLy = d->CFLy;
+  w.V = d->V; w.Z = d->Z; w.Nx = d->Nx; w.Oy = d->Oy; w.Vx = d->Vx; w.Vy = d->Vy; w.Zx = d->Zx;
+  w.Zy = d->Zy;
+  w.bottomZ = d->bottomZ; w.bottomXP = d->bottomXP; w.bottomYP = d->bottomYP;
+  w.EnXP = d->EnXP; w.EnYP = d->EnYP; w.Gx = d->Gx; w.Gy = d->Gy; w.Ct = d->Ct; w.b = d->b;
+  w.x = d->x; w.r = d->r; w.p0 = d->p0; w.p1 = d->p1; w.q = d->q;
+  w.cellV = d->cellV; w.Sm = d->Sm; w.Fuu = d->Fuu; w.Fvv = d->Fvv;
+  w.rmv = d->rmv; w.fix_list = d->fix_list; w.partials = d->partials;
+  w.tide = d->tide; w.ntide = d->ntide;
+  w.sc = d->sc;
+  return w;
+}
+
+dim3 tile_grid(const frehd_domain *d) {
+  return dim3((d->gr.nx + 31) / 32, (d->gr.ny + 7) / 8);
+}
+
+__global__ void k_set_tt(Scratch *sc, int tt) { sc->tt = tt; }
+
+// host copies in the reference layout: index helpers (map.c:45-143)
+struct RefMap {
+  int nx, ny;
+  long N, T;
+  long jPbd(int i) const { return N - nx + i; }
+  long jPgt(int i) const { return N + i; }
+  long jMbd(int i) const { return i; }
+  long jMgt(int i) const { return N + nx + i; }
+  long iPbd(int j) const { return (long)(j + 1) * nx - 1; }
+  long iPgt(int j) const { return N + 2L * nx + j; }
+  long iMbd(int j) const { return (long)j * nx; }
+  long iMgt(int j) const { return N + 2L * nx + ny + j; }
+  long iPjc(long ii) const { return ii % nx == nx - 1 ? N + 2L * nx + ii / nx : ii + 1; }
+  long icjP(long ii) const { return ii / nx == ny - 1 ? N + ii % nx : ii + nx; }
+  long iMjP() const { return T - 4; }
+  long iPjP() const { return T - 3; }
+  long iPjM() const { return T - 2; }
+  long iMjM() const { return T - 1; }
+};
+
+int upload_ref(frehd_domain *d, double *dst_padded, const double *host, long n) {
+  CUDA_TRY(cudaMemcpyAsync(d->stage, host, sizeof(double) * n, cudaMemcpyHostToDevice, d->stream));
+  k_ref_to_padded<<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>(dst_padded, d->stage, n,
+                                                                      d->gr.nx, d->gr.ny, d->gr.pitch);
+  CUDA_TRY(cudaGetLastError());
+  return FREHD_OK;
+}
+
+int download_ref(frehd_domain *d, double *host, const double *src_padded, long n) {
+  k_padded_to_ref<<<(unsigned)((n + 255) / 256), 256, 0, d->stream>>>(d->stage, src_padded, n,
+                                                                      d->gr.nx, d->gr.ny, d->gr.pitch);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(host, d->stage, sizeof(double) * n, cudaMemcpyDeviceToHost, d->stream));
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return FREHD_OK;
+}
+
+int read_stats(frehd_domain *d) {
+  CUDA_TRY(cudaMemcpyAsync(d->out_host, d->out, sizeof(StepOut), cudaMemcpyDeviceToHost, d->stream));
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  const StepOut &o = *d->out_host;
+  d->last.step = o.step;
+  d->last.cg_iters = o.cg_iters;
+  d->last.status = o.status;
+  d->last.cg_rel_residual = o.cg_bb > 0 ? std::sqrt(o.cg_rr) / std::sqrt(o.cg_bb) : 0.0;
+  d->last.max_cflx = o.max_cflx;
+  d->last.max_cfly = o.max_cfly;
+  d->last.n_cfl_warn = o.n_cfl_warn;
+  d->last.volume = o.volume;
+  return FREHD_OK;
+}
+
+int launch_cg(frehd_domain *d, const View &w) {
+  View wv = w;
+  int x0 = d->x0_mode;
+  void *args[] = {&wv, &x0};
+  CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_cg, dim3(d->cg_blocks), dim3(kCgThreads), args, 0,
+                                       d->stream));
+  return FREHD_OK;
+}
+
+// Event slots of step s (6 per step: before explicit, cg, geo, vel, finish, after).
+cudaEvent_t *step_events(frehd_domain *d, int s) {
+  if (!d->profiling) return nullptr;
+  const size_t need = (size_t)(s + 1) * 6;
+  while (d->ev.size() < need) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    d->ev.push_back(e);
+  }
+  return &d->ev[(size_t)s * 6];
+}
+
+void mark(cudaEvent_t *ev, int slot, cudaStream_t st) {
+  if (ev) cudaEventRecord(ev[slot], st);
+}
+
+int launch_update(frehd_domain *d, const View &w, cudaEvent_t *ev = nullptr) {
+  const dim3 gb = tile_grid(d), bb(32, 8);
+  mark(ev, 2, d->stream);
+  k_update_geo<false><<<gb, bb, 0, d->stream>>>(w);
+  mark(ev, 3, d->stream);
+  k_update_vel<<<gb, bb, 0, d->stream>>>(w);
+  mark(ev, 4, d->stream);
+  k_finish<<<1, 256, 0, d->stream>>>(w, (int)(gb.x * gb.y), d->out);
+  mark(ev, 5, d->stream);
+  CUDA_TRY(cudaGetLastError());
+  return FREHD_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- lifecycle
+extern "C" int frehd_device_count(int *count) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    n = 0;
+  }
+  if (count) *count = n;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_domain **out) {
+  clear_error();
+  if (!cfg || !out) return fail(FREHD_ERR_INVALID, "null argument");
+  *out = nullptr;
+  int rc = check_config(cfg);
+  if (rc) return rc;
+  CUDA_TRY(cudaSetDevice(device));
+  frehd_domain *d = new frehd_domain();
+  d->cfg = *cfg;
+  d->device = device;
+  if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete d;
+    return fail(FREHD_ERR_CUDA, "cudaStreamCreate failed");
+  }
+  d->gr = Grid::make(cfg->nx, cfg->ny);
+  d->N = (long)cfg->nx * cfg->ny;
+  d->T = (long)(cfg->nx + 2) * (cfg->ny + 2);
+  Params &p = d->p;
+  std::memset(&p, 0, sizeof(p));
+  p.nx = cfg->nx; p.ny = cfg->ny; p.pitch = d->gr.pitch;
+  p.dx = cfg->dx; p.dy = cfg->dy; p.dt = cfg->dt; p.g = cfg->g; p.NUx = cfg->NUx; p.NUy = cfg->NUy;
+  p.Kx = cfg->Kx; p.Ky = cfg->Ky; p.manningN = cfg->manningN; p.hD = cfg->hD;
+  p.minDepth = cfg->minDepth; p.wtfh = cfg->wtfh; p.CFLl = cfg->CFLl; p.CFLh = cfg->CFLh;
+  p.offset = cfg->offset; p.surfmin = cfg->surfmin; p.dsurf = cfg->dsurf; p.tidePS = cfg->tidePS;
+  p.subR = cfg->subR; p.dxf = cfg->dxf; p.dyf = cfg->dyf; p.eps = cfg->eps;
+  p.Ne = (int)std::lround((cfg->surfmax - cfg->surfmin) / cfg->dsurf);  // subgrid.c:2115
+  p.useThinLayer = cfg->useThinLayer; p.useScalar = cfg->useScalar;
+  p.tideFirst = cfg->tideLocFirstP; p.tideLen = cfg->tideLocLengthP; p.maxIter = cfg->maxIter;
+  const long tot = d->gr.total;
+  int r = 0;
+  for (int a = 0; a < 2 && !r; ++a) {
+    r |= dalloc(d, &d->surf[a], tot);
+    r |= dalloc(d, &d->depth[a], tot);
+    r |= dalloc(d, &d->S[a], tot);
+    r |= dalloc(d, &d->ind[a], tot);
+  }
+  double **arrs[] = {&d->u, &d->v, &d->CDXP, &d->CDYP, &d->CFLx, &d->CFLy, &d->V, &d->Z, &d->Nx,
+                     &d->Oy, &d->Vx, &d->Vy, &d->Zx, &d->Zy, &d->bottomZ, &d->bottomXP,
+                     &d->bottomYP, &d->EnXP, &d->EnYP, &d->Gx, &d->Gy, &d->Ct, &d->b, &d->x, &d->r,
+                     &d->p0, &d->p1, &d->q, &d->cellV, &d->Sm, &d->Fuu, &d->Fvv};
+  for (auto a : arrs)
+    if (!r) r |= dalloc(d, a, tot);
+  if (!r) r |= dalloc(d, &d->rmv, tot);
+  if (!r) r |= dalloc(d, &d->fix_list, d->N);
+  if (!r) r |= dalloc(d, &d->stage, d->T);
+  if (!r) r |= dalloc(d, &d->stage2, d->T);
+  if (!r) r |= dalloc(d, &d->sc, 1);
+  if (!r) r |= dalloc(d, &d->out, 1);
+  // CG launch size: all blocks co-resident (cooperative launch), no more blocks
+  // than 256-cell chunks
+  int nsm = 0, per = 0;
+  if (!r) {
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg, kCgThreads, 0);
+    long want = (d->N + kCgThreads - 1) / kCgThreads;
+    long cap = (long)nsm * std::max(per, 1);
+    d->cg_blocks = (int)std::max(1L, std::min(want, cap));
+    const long nvel = (long)((d->gr.nx + 31) / 32) * ((d->gr.ny + 7) / 8);
+    d->npartials = std::max(nvel, 8L * d->cg_blocks);
+    r |= dalloc(d, &d->partials, d->npartials);
+  }
+  if (!r && cudaMallocHost((void **)&d->out_host, sizeof(StepOut)) != cudaSuccess)
+    r = fail(FREHD_ERR_NOMEM, "pinned host allocation failed");
+  if (r) {
+    frehd_domain_destroy(d);
+    return r;
+  }
+  // Ct ghosts mark "no unknown" (negative) so the CG treats them as decoupled
+  k_fill<<<(unsigned)((tot + 255) / 256), 256, 0, d->stream>>>(d->Ct, tot, -1.0);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  *out = d;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_destroy(frehd_domain *d) {
+  if (!d) return FREHD_OK;
+  cudaSetDevice(d->device);
+  if (d->stream) cudaStreamSynchronize(d->stream);
+  for (void *p : d->allocs) cudaFree(p);
+  if (d->tables) cudaFree(d->tables);
+  if (d->zf) cudaFree(d->zf);
+  if (d->tide) cudaFree(d->tide);
+  if (d->out_host) cudaFreeHost(d->out_host);
+  for (cudaEvent_t e : d->ev) cudaEventDestroy(e);
+  if (d->stream) cudaStreamDestroy(d->stream);
+  delete d;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_set_tables(frehd_domain *d, int Ne, const double *tables) {
+  if (!d || !tables) return fail(FREHD_ERR_INVALID, "null argument");
+  if (Ne != d->p.Ne)
+    return fail(FREHD_ERR_INVALID, "tables hold %d levels, the config implies Ne=%d", Ne, d->p.Ne);
+  CUDA_TRY(cudaSetDevice(d->device));
+  const size_t bytes = sizeof(double) * 10 * (size_t)Ne * d->N;
+  if (d->tables) cudaFree(d->tables);
+  d->tables = nullptr;
+  if (cudaMalloc(&d->tables, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(FREHD_ERR_NOMEM, "tables: %zu bytes", bytes);
+  }
+  CUDA_TRY(cudaMemcpyAsync(d->tables, tables, bytes, cudaMemcpyHostToDevice, d->stream));
+  d->p.geom_fine = 0;
+  d->p.tab = d->tables;
+  d->geom_set = 1;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_set_fine_bottoms(frehd_domain *d, int r, const double *zf, long fpitch) {
+  if (!d || !zf || r <= 0) return fail(FREHD_ERR_INVALID, "bad argument");
+  if (fpitch < (long)d->gr.nx * r) return fail(FREHD_ERR_INVALID, "fine pitch too small");
+  if (std::fabs(d->cfg.dx / d->cfg.dxf - r) > 1e-9 * r)
+    return fail(FREHD_ERR_INVALID, "r=%d does not match dx/dxf", r);
+  CUDA_TRY(cudaSetDevice(d->device));
+  const long rows = (long)d->gr.ny * r, cols = (long)d->gr.nx * r;
+  if (d->zf) cudaFree(d->zf);
+  d->zf = nullptr;
+  if (cudaMalloc(&d->zf, sizeof(double) * rows * cols) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(FREHD_ERR_NOMEM, "fine bottoms: %ld bytes", (long)(sizeof(double) * rows * cols));
+  }
+  CUDA_TRY(cudaMemcpy2DAsync(d->zf, sizeof(double) * cols, zf, sizeof(double) * fpitch,
+                             sizeof(double) * cols, rows, cudaMemcpyHostToDevice, d->stream));
+  d->p.geom_fine = 1;
+  d->p.zf = d->zf;
+  d->p.fpitch = cols;
+  d->p.r = r;
+  d->geom_set = 1;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_set_tide(frehd_domain *d, int n, const double *tideP) {
+  if (!d || (n > 0 && !tideP) || n < 0) return fail(FREHD_ERR_INVALID, "bad argument");
+  CUDA_TRY(cudaSetDevice(d->device));
+  if (d->tide) cudaFree(d->tide);
+  d->tide = nullptr;
+  CUDA_TRY(cudaMalloc(&d->tide, sizeof(double) * std::max(n, 1)));
+  if (n) CUDA_TRY(cudaMemcpyAsync(d->tide, tideP, sizeof(double) * n, cudaMemcpyHostToDevice, d->stream));
+  d->ntide = n;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_set_solver(frehd_domain *d, int x0_mode) {
+  if (!d || (x0_mode != FREHD_X0_ZERO && x0_mode != FREHD_X0_SURFACE))
+    return fail(FREHD_ERR_INVALID, "bad solver option");
+  d->x0_mode = x0_mode;
+  return FREHD_OK;
+}
+
+// ---------------------------------------------------------------- state I/O
+extern "C" int frehd_domain_upload_state(frehd_domain *d, const frehd_state *st) {
+  if (!d || !st) return fail(FREHD_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaSetDevice(d->device));
+  const long N = d->N, T = d->T;
+  const int c = d->cur;
+  struct Item {
+    const double *h;
+    double *dv;
+    long n;
+  } items[] = {
+      {st->surf, d->surf[c], T}, {st->uuXP, d->u, T}, {st->vvYP, d->v, T}, {st->S, d->S[c], T},
+      {st->depth, d->depth[c], N}, {st->CDXP, d->CDXP, T}, {st->CDYP, d->CDYP, T},
+      {st->CFLx, d->CFLx, T}, {st->CFLy, d->CFLy, T}, {st->V, d->V, T}, {st->Z, d->Z, T},
+      {st->Nx, d->Nx, T}, {st->Oy, d->Oy, T}, {st->Vx, d->Vx, T}, {st->Vy, d->Vy, T},
+      {st->Zx, d->Zx, T}, {st->Zy, d->Zy, T}, {st->bottomZ, d->bottomZ, T},
+      {st->bottomXP, d->bottomXP, T}, {st->bottomYP, d->bottomYP, T},
+  };
+  for (auto &it : items)
+    if (it.h) {
+      int rc = upload_ref(d, it.dv, it.h, it.n);
+      if (rc) return rc;
+    }
+  if (st->ind) {
+    CUDA_TRY(cudaMemcpyAsync(d->stage, st->ind, sizeof(int) * T, cudaMemcpyHostToDevice, d->stream));
+    k_ref_to_padded_int<<<(unsigned)((T + 255) / 256), 256, 0, d->stream>>>(
+        d->ind[c], (const int *)d->stage, T, d->gr.nx, d->gr.ny, d->gr.pitch);
+    CUDA_TRY(cudaGetLastError());
+  }
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  d->ready = 1;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_download_state(frehd_domain *d, frehd_state *st) {
+  if (!d || !st) return fail(FREHD_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaSetDevice(d->device));
+  const long N = d->N, T = d->T;
+  const int c = d->cur, o = d->cur ^ 1;
+  struct Item {
+    double *h;
+    const double *dv;
+    long n;
+  } items[] = {
+      {st->surf, d->surf[c], T}, {st->uuXP, d->u, T}, {st->vvYP, d->v, T}, {st->S, d->S[c], T},
+      {st->depth, d->depth[c], N}, {st->CDXP, d->CDXP, T}, {st->CDYP, d->CDYP, T},
+      {st->CFLx, d->CFLx, T}, {st->CFLy, d->CFLy, T}, {st->V, d->V, T}, {st->Z, d->Z, T},
+      {st->Nx, d->Nx, T}, {st->Oy, d->Oy, T}, {st->Vx, d->Vx, T}, {st->Vy, d->Vy, T},
+      {st->Zx, d->Zx, T}, {st->Zy, d->Zy, T}, {st->bottomZ, d->bottomZ, T},
+      {st->bottomXP, d->bottomXP, T}, {st->bottomYP, d->bottomYP, T},
+      {st->surfOld, d->surf[o], T}, {st->EnXP, d->EnXP, T}, {st->EnYP, d->EnYP, T},
+      {st->cellV, d->cellV, N}, {st->Sm, d->Sm, N}, {st->Fuu, d->Fuu, T}, {st->Fvv, d->Fvv, T},
+  };
+  for (auto &it : items)
+    if (it.h) {
+      int rc = download_ref(d, it.h, it.dv, it.n);
+      if (rc) return rc;
+    }
+  if (st->ind) {
+    k_padded_to_ref_int<<<(unsigned)((T + 255) / 256), 256, 0, d->stream>>>(
+        (int *)d->stage, d->ind[c], T, d->gr.nx, d->gr.ny, d->gr.pitch);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(st->ind, d->stage, sizeof(int) * T, cudaMemcpyDeviceToHost, d->stream));
+  }
+  if (st->uuYP || st->vvXP) {
+    View w = make_view(d);
+    k_interp_velocity<<<(unsigned)((N + 255) / 256), 256, 0, d->stream>>>(w, d->stage, d->stage2);
+    CUDA_TRY(cudaGetLastError());
+    if (st->uuYP)
+      CUDA_TRY(cudaMemcpyAsync(st->uuYP, d->stage, sizeof(double) * N, cudaMemcpyDeviceToHost, d->stream));
+    if (st->vvXP)
+      CUDA_TRY(cudaMemcpyAsync(st->vvXP, d->stage2, sizeof(double) * N, cudaMemcpyDeviceToHost, d->stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return FREHD_OK;
+}
+
+// ---------------------------------------------------------------- init
+// Init (initialize.c:40-155) for the subgrid path, restated on the host in the
+// reference layout; the subgrid evaluation (computeSubArea + combineSubArea) runs
+// on the device with the step's own kernel.
+extern "C" int frehd_domain_init(frehd_domain *d, const double *bottom, const double *bxp,
+                                 const double *byp, const double *surf0, const double *u0,
+                                 const double *v0, const double *S0, int round_trip_output) {
+  if (!d || !bottom || !bxp || !byp || !surf0) return fail(FREHD_ERR_INVALID, "null argument");
+  if (!d->geom_set) return fail(FREHD_ERR_STATE, "set tables or fine bottoms before init");
+  CUDA_TRY(cudaSetDevice(d->device));
+  const frehd_config &c = d->cfg;
+  RefMap m{c.nx, c.ny, d->N, d->T};
+  const long N = d->N, T = d->T;
+  const double off = c.offset;
+  std::vector<double> bz(T, 0.0), bx(T, 0.0), by(T, 0.0), s(T, 0.0), u(T, 0.0), v(T, 0.0),
+      S(T, 0.0), cdx(T, c.CDx), cdy(T, c.CDy), dep(N, 0.0), hx(T, 0.0), hy(T, 0.0);
+  std::vector<double> ex(N), ey(N);
+  for (long ii = 0; ii < N; ++ii) {  // InitBathymetry (bathymetry.c:104-121)
+    bz[ii] = bottom[ii] + off;
+    ex[ii] = bxp[ii] + off;
+    ey[ii] = byp[ii] + off;
+  }
+  for (int i = 0; i < c.nx; ++i) { bz[m.jMgt(i)] = bz[m.jMbd(i)]; bz[m.jPgt(i)] = bz[m.jPbd(i)]; }
+  for (int j = 0; j < c.ny; ++j) { bz[m.iMgt(j)] = bz[m.iMbd(j)]; bz[m.iPgt(j)] = bz[m.iPbd(j)]; }
+  // updateAllFaceElev, subgrid branch (nsfunctions.c:76-140)
+  for (long ii = 0; ii < N; ++ii) bx[ii] = ex[ii];
+  for (int j = 0; j < c.ny; ++j) { bx[m.iMgt(j)] = bz[m.iMbd(j)]; bx[m.iPgt(j)] = bx[m.iPbd(j)]; }
+  for (int i = 0; i < c.nx; ++i) { bx[m.jMgt(i)] = bx[m.jMbd(i)]; bx[m.jPgt(i)] = bx[m.jPbd(i)]; }
+  for (long ii = 0; ii < N; ++ii) by[ii] = ey[ii];
+  for (int i = 0; i < c.nx; ++i) {
+    const long gi = m.jMgt(i);
+    by[gi] = bz[gi] > bz[i] ? bz[gi] : bz[i];
+    by[m.jPgt(i)] = by[m.jPbd(i)];
+  }
+  for (int j = 0; j < c.ny; ++j) { by[m.iMgt(j)] = by[m.iMbd(j)]; by[m.iPgt(j)] = by[m.iPbd(j)]; }
+  // initFieldValues (initialize.c:393-443)
+  for (long ii = 0; ii < N; ++ii) {
+    s[ii] = surf0[ii] + off;
+    u[ii] = u0 ? u0[ii] : 0.0;
+    v[ii] = v0 ? v0[ii] : 0.0;
+    if (c.useScalar) S[ii] = S0 ? S0[ii] : 0.0;
+  }
+  for (long ii = 0; ii < N; ++ii)  // zeroNegSurf
+    if (s[ii] < bz[ii]) s[ii] = bz[ii];
+  // enforceFreeSurfaceBC / enforceVelocityBC with corners (nsfunctions.c:289-334)
+  for (int i = 0; i < c.nx; ++i) {
+    s[m.jPgt(i)] = s[m.jPbd(i)]; s[m.jMgt(i)] = s[m.jMbd(i)];
+    u[m.jPgt(i)] = u[m.jPbd(i)]; u[m.jMgt(i)] = u[m.jMbd(i)];
+    v[m.jPgt(i)] = v[m.jPbd(i)]; v[m.jMgt(i)] = v[m.jMbd(i)];
+  }
+  for (int j = 0; j < c.ny; ++j) {
+    s[m.iPgt(j)] = s[m.iPbd(j)]; s[m.iMgt(j)] = s[m.iMbd(j)];
+    u[m.iPgt(j)] = u[m.iPbd(j)]; u[m.iMgt(j)] = u[m.iMbd(j)];
+    v[m.iPgt(j)] = v[m.iPbd(j)]; v[m.iMgt(j)] = v[m.iMbd(j)];
+  }
+  s[m.iPjP()] = s[m.iPgt(c.ny - 1)]; s[m.iPjM()] = s[m.iMgt(c.ny - 1)];
+  s[m.iMjP()] = s[m.iPgt(0)]; s[m.iMjM()] = s[m.iMgt(0)];
+  u[m.iPjP()] = u[m.jPgt(c.nx - 1)]; u[m.iPjM()] = u[m.jMgt(c.nx - 1)];
+  u[m.iMjP()] = u[m.jPgt(0)]; u[m.iMjM()] = u[m.jMgt(0)];
+  v[m.iPjP()] = v[m.iPgt(c.ny - 1)]; v[m.iPjM()] = v[m.iMgt(c.ny - 1)];
+  v[m.iMjP()] = v[m.iPgt(0)]; v[m.iMjM()] = v[m.iMgt(0)];
+  // enforceTidalBC at tt = 0
+  std::vector<double> tide0(1, 0.0);
+  if (d->ntide > 0) {
+    CUDA_TRY(cudaMemcpyAsync(tide0.data(), d->tide, sizeof(double), cudaMemcpyDeviceToHost, d->stream));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+  }
+  for (int k = 0; k < c.tideLocLengthP; ++k) {
+    const long cc = c.tideLocFirstP + k + (long)c.nx * (c.ny - 1);
+    if (tide0[0] + off > bz[cc]) s[cc] = tide0[0] + off;
+  }
+  for (long ii = 0; ii < N; ++ii) {  // updateDepth
+    dep[ii] = s[ii] - bz[ii];
+    if (dep[ii] < 0) dep[ii] = 0;
+  }
+  // updateAllFaceDepth (nsfunctions.c:143-236): only the interior face depths
+  // feed thinLayerDrag
+  for (long ii = 0; ii < N; ++ii) {
+    const double a = s[ii], bE = s[m.iPjc(ii)], bN = s[m.icjP(ii)];
+    hx[ii] = (a > bE ? a : bE) - bx[ii];
+    hy[ii] = (a > bN ? a : bN) - by[ii];
+  }
+  for (int j = 0; j < c.ny; ++j) hx[m.iPbd(j)] = 0;
+  for (int i = 0; i < c.nx; ++i) hy[m.jPbd(i)] = 0;
+  for (long ii = 0; ii < N; ++ii) {
+    if (hx[ii] < 0) hx[ii] = 0;
+    if (hy[ii] < 0) hy[ii] = 0;
+  }
+  // thinLayerDrag, called unconditionally by Init (initialize.c:140), CDnotN = 0
+  const double coeff = c.g * c.manningN * c.manningN;
+  for (long ii = 0; ii < N; ++ii)
+    if (dep[ii] > 0) {
+      if (hx[ii] <= c.hD) cdx[ii] = coeff / std::pow(dep[ii], 2.0 / 3.0);
+      if (hy[ii] <= c.hD) cdy[ii] = coeff / std::pow(dep[ii], 2.0 / 3.0);
+    }
+  if (c.useScalar)
+    for (long ii = 0; ii < N; ++ii)
+      if (dep[ii] <= 0) S[ii] = 0;
+  std::vector<int> ind(T, d->p.Ne / 2);  // subgrid.c:2268-2270
+  // upload and evaluate the subgrid geometry
+  frehd_state st;
+  std::memset(&st, 0, sizeof(st));
+  st.surf = s.data(); st.uuXP = u.data(); st.vvYP = v.data(); st.S = S.data();
+  st.depth = dep.data(); st.CDXP = cdx.data(); st.CDYP = cdy.data();
+  st.bottomZ = bz.data(); st.bottomXP = bx.data(); st.bottomYP = by.data(); st.ind = ind.data();
+  int rc = frehd_domain_upload_state(d, &st);
+  if (rc) return rc;
+  {
+    View w = make_view(d);
+    k_update_geo<true><<<tile_grid(d), dim3(32, 8), 0, d->stream>>>(w);
+    CUDA_TRY(cudaGetLastError());
+    std::swap(d->ind[0], d->ind[1]);  // the evaluated indices become current
+  }
+  if (round_trip_output) {  // DataOutput at tt = 0 (fileio.c:65-66,120-121)
+    for (long ii = 0; ii < N; ++ii) s[ii] = s[ii] - off;
+    for (long ii = 0; ii < N; ++ii) s[ii] = s[ii] + off;
+    rc = upload_ref(d, d->surf[d->cur], s.data(), T);
+    if (rc) return rc;
+  }
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  d->ready = 1;
+  return FREHD_OK;
+}
+
+// ---------------------------------------------------------------- stepping
+extern "C" int frehd_domain_phase(frehd_domain *d, int phase, int tt, const double *x_ext) {
+  if (!d) return fail(FREHD_ERR_INVALID, "null domain");
+  if (!d->ready) return fail(FREHD_ERR_STATE, "domain has no state (init or upload first)");
+  CUDA_TRY(cudaSetDevice(d->device));
+  View w = make_view(d);
+  if (phase == FREHD_PHASE_EXPLICIT) {
+    k_set_tt<<<1, 1, 0, d->stream>>>(d->sc, tt);
+    k_explicit<<<tile_grid(d), dim3(32, 8), 0, d->stream>>>(w);
+    CUDA_TRY(cudaGetLastError());
+  } else if (phase == FREHD_PHASE_SOLVE) {
+    int rc = launch_cg(d, w);
+    if (rc) return rc;
+  } else if (phase == FREHD_PHASE_UPDATE) {
+    k_set_tt<<<1, 1, 0, d->stream>>>(d->sc, tt);
+    if (x_ext) {
+      CUDA_TRY(cudaMemcpyAsync(d->stage, x_ext, sizeof(double) * d->N, cudaMemcpyHostToDevice, d->stream));
+      k_solution_from_ref<<<(unsigned)((d->N + 255) / 256), 256, 0, d->stream>>>(w, d->stage);
+      CUDA_TRY(cudaGetLastError());
+    }
+    int rc = launch_update(d, w);
+    if (rc) return rc;
+    d->cur ^= 1;
+    rc = read_stats(d);
+    if (rc) return rc;
+    return d->last.status == FREHD_ERR_CFL ? FREHD_ERR_CFL : FREHD_OK;
+  } else {
+    return fail(FREHD_ERR_INVALID, "unknown phase %d", phase);
+  }
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_run(frehd_domain *d, int t0, int nsteps) {
+  if (!d) return fail(FREHD_ERR_INVALID, "null domain");
+  if (!d->ready) return fail(FREHD_ERR_STATE, "domain has no state (init or upload first)");
+  if (nsteps <= 0) return FREHD_OK;
+  CUDA_TRY(cudaSetDevice(d->device));
+  const int cur0 = d->cur;
+  k_set_tt<<<1, 1, 0, d->stream>>>(d->sc, t0);
+  for (int s = 0; s < nsteps; ++s) {
+    View w = make_view(d);
+    cudaEvent_t *ev = step_events(d, s);
+    mark(ev, 0, d->stream);
+    k_explicit<<<tile_grid(d), dim3(32, 8), 0, d->stream>>>(w);
+    mark(ev, 1, d->stream);
+    int rc = launch_cg(d, w);
+    if (rc) return rc;
+    rc = launch_update(d, w, ev);
+    if (rc) return rc;
+    d->cur ^= 1;
+  }
+  int rc = read_stats(d);
+  if (rc) return rc;
+  if (d->profiling) {
+    for (int s = 0; s < nsteps; ++s) {
+      cudaEvent_t *ev = &d->ev[(size_t)s * 6];
+      float ms[5];
+      for (int k = 0; k < 5; ++k) cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]);
+      d->times.explicit_ms += ms[0];
+      d->times.cg_ms += ms[1];
+      d->times.update_geo_ms += ms[2];
+      d->times.update_vel_ms += ms[3];
+      d->times.finish_ms += ms[4];
+    }
+    d->times.steps += nsteps;
+    d->times.cg_iters = d->out_host->cg_iters_total - d->iters_at_prof_start;
+  }
+  // after a fatal step the later steps are skipped on the device; recover the
+  // buffer parity from the last completed step
+  const int done = d->last.step - t0 + 1;
+  if (done != nsteps) d->cur = cur0 ^ (done & 1);
+  if (d->last.status == FREHD_ERR_CFL) return fail(FREHD_ERR_CFL, "max CFL > 20 at step %d", d->last.step);
+  if (d->last.status != FREHD_OK)
+    return fail(d->last.status, "step %d: %s", d->last.step, frehd_status_string(d->last.status));
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_step(frehd_domain *d, int tt) { return frehd_domain_run(d, tt, 1); }
+
+extern "C" int frehd_domain_download_system(frehd_domain *d, double *GnCt, double *GnXP,
+                                            double *GnXM, double *GnYP, double *GnYM, double *z) {
+  if (!d) return fail(FREHD_ERR_INVALID, "null domain");
+  CUDA_TRY(cudaSetDevice(d->device));
+  const long N = d->N;
+  double *h[6] = {GnCt, GnXP, GnXM, GnYP, GnYM, z};
+  View w = make_view(d);
+  for (int a = 0; a < 6; ++a) {
+    if (!h[a]) continue;
+    double *o[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    o[a] = d->stage;
+    k_system_to_ref<<<(unsigned)((N + 255) / 256), 256, 0, d->stream>>>(w, o[0], o[1], o[2], o[3],
+                                                                          o[4], o[5], o[6]);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(h[a], d->stage, sizeof(double) * N, cudaMemcpyDeviceToHost, d->stream));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+  }
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_download_solution(frehd_domain *d, double *xs) {
+  if (!d || !xs) return fail(FREHD_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaSetDevice(d->device));
+  View w = make_view(d);
+  k_system_to_ref<<<(unsigned)((d->N + 255) / 256), 256, 0, d->stream>>>(
+      w, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, d->stage);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(xs, d->stage, sizeof(double) * d->N, cudaMemcpyDeviceToHost, d->stream));
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_stats(frehd_domain *d, frehd_step_stats *out) {
+  if (!d || !out) return fail(FREHD_ERR_INVALID, "null argument");
+  int rc = read_stats(d);
+  if (rc) return rc;
+  *out = d->last;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_set_profiling(frehd_domain *d, int on) {
+  if (!d) return fail(FREHD_ERR_INVALID, "null domain");
+  d->profiling = on ? 1 : 0;
+  d->times = frehd_kernel_times{};
+  int rc = read_stats(d);
+  if (rc) return rc;
+  d->iters_at_prof_start = d->out_host->cg_iters_total;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_kernel_times(frehd_domain *d, frehd_kernel_times *out) {
+  if (!d || !out) return fail(FREHD_ERR_INVALID, "null argument");
+  *out = d->times;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_stream(frehd_domain *d, void **stream) {
+  if (!d || !stream) return fail(FREHD_ERR_INVALID, "null argument");
+  *stream = (void *)d->stream;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_sync(frehd_domain *d) {
+  if (!d) return fail(FREHD_ERR_INVALID, "null domain");
+  CUDA_TRY(cudaSetDevice(d->device));
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return FREHD_OK;
+}

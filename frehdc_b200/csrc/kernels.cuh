@@ -1,0 +1,51 @@
+// Kernel declarations and small device helpers shared by the .cu files.
+#ifndef FREHD_KERNELS_CUH
+#define FREHD_KERNELS_CUH
+
+#include "domain.cuh"
+
+namespace frehd {
+
+// Step statistics written by k_finish (device memory, read by the host).
+struct StepOut {
+  int step, cg_iters, status, n_cfl_warn, n_fix, pad;
+  double cg_rr, cg_bb, max_cflx, max_cfly, volume;
+  long long cg_iters_total;
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ int warp_sum_int(int v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+__global__ void k_explicit(View w);
+template <bool kInit>
+__global__ void k_update_geo(View w);
+__global__ void k_update_vel(View w);
+__global__ void k_finish(View w, int nblocks_vel, StepOut *out);
+__global__ void k_ref_to_padded(double *dst, const double *src, long n, int nx, int ny, int pitch);
+__global__ void k_padded_to_ref(double *dst, const double *src, long n, int nx, int ny, int pitch);
+__global__ void k_ref_to_padded_int(int *dst, const int *src, long n, int nx, int ny, int pitch);
+__global__ void k_padded_to_ref_int(int *dst, const int *src, long n, int nx, int ny, int pitch);
+__global__ void k_fill(double *a, long n, double v);
+__global__ void k_interp_velocity(View w, double *uuYP, double *vvXP);
+__global__ void k_system_to_ref(View w, double *GnCt, double *GnXP, double *GnXM, double *GnYP,
+                                double *GnYM, double *z, double *xs);
+__global__ void k_solution_from_ref(View w, const double *xs);
+
+// Persistent Jacobi-preconditioned CG (cg.cu).
+__global__ void k_cg(View w, int x0_surface);
+
+constexpr int kCgThreads = 256;
+
+}  // namespace frehd
+
+#endif

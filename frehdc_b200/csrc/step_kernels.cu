@@ -1,0 +1,836 @@
+// Stencil kernels of one FrehdC step (plain FP64 form).
+//
+// Every expression keeps the reference's evaluation order and this file is
+// built with --fmad=false, so the doubles produced here equal those of the
+// reference's sequential loops (reference functions cited per block).  The
+// reference's order-dependent loops are restated in closed form where they are
+// order dependent only through a fixed neighbour set (the advection CFL limiter,
+// the dry-cell outflow rule, the waterfall flag precedence).
+//
+// Kernels per step (after the persistent CG in cg.cu):
+//   k_explicit   solveSourceTerm + matrixCoeffSub + adjustMatrixBoundary +
+//                adjustTidalBoundary (nssolve.c:121-166)
+//   k_update_geo getFreeSurface .. enforceTidalBC, limiterCFL, computeSubArea,
+//                combineSubArea, updateDepth (nssolve.c:169-225)
+//   k_update_vel detectWaterfall .. thinLayerDrag, scalarTransport, monitorCFL
+//                (nssolve.c:237-290, scalar.c:30-57, nsfunctions.c:1192-1232)
+//   k_finish     scalar-singularity surface fix-up, step statistics
+#include <cmath>
+
+#include "domain.cuh"
+#include "kernels.cuh"
+#include "subgrid_levels.h"
+
+namespace frehd {
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ double rd(const double *a, const Grid &g, int i, int j) {
+  return a[g.at(i, j)];
+}
+
+// velocityInterp (nsfunctions.c:337-347): the reference indexes the linear
+// array directly, so "ii - 1" of the first column is the last cell of the
+// previous row, "ii + nx" of the last row is the north ghost row, and indices
+// before the array start read 0.
+__device__ __forceinline__ double uuYP_at(const View &w, int i, int j) {
+  const Grid &g = w.gr;
+  const double a = rd(w.u, g, i, j);
+  const double b = (i > 0) ? rd(w.u, g, i - 1, j) : (j > 0 ? rd(w.u, g, g.nx - 1, j - 1) : 0.0);
+  const double c = rd(w.u, g, i, j + 1);
+  const double d = (i > 0) ? rd(w.u, g, i - 1, j + 1) : rd(w.u, g, g.nx - 1, j);
+  return 0.25 * (a + b + c + d);
+}
+
+__device__ __forceinline__ double vvXP_at(const View &w, int i, int j) {
+  const Grid &g = w.gr;
+  const double a = rd(w.v, g, i, j);
+  const double b = (i < g.nx - 1) ? rd(w.v, g, i + 1, j) : rd(w.v, g, 0, j + 1);
+  const double c = (j > 0) ? rd(w.v, g, i, j - 1) : 0.0;
+  const double d = (i < g.nx - 1) ? (j > 0 ? rd(w.v, g, i + 1, j - 1) : 0.0) : rd(w.v, g, 0, j);
+  return 0.25 * (a + b + c + d);
+}
+
+struct Ex {
+  double En, Drag;
+};
+
+// One cell's x-momentum source: explicitVelocity, advectionTerm with the CFL
+// limiter (nsfunctions.c:498-586), diffusionTermSub (subgrid.c:781-812),
+// dragTermSub with staggeredV = 1 (subgrid.c:857-927) and dragInversion
+// (nsfunctions.c:730-746).  The limiter scales advX[k] once for each cell of
+// the sweep that reaches k before k's own update: k - nx, k - 1, then k.
+__device__ Ex explicit_x(const View &w, int i, int j) {
+  const Params &p = w.p;
+  const Grid &g = w.gr;
+  const long k = g.at(i, j);
+  const double *u = w.u;
+  const double u0 = u[k], uE = rd(u, g, i + 1, j), uW = rd(u, g, i - 1, j);
+  const double uN = rd(u, g, i, j + 1), uS = rd(u, g, i, j - 1);
+  const double vX = vvXP_at(w, i, j);
+  double ax = (0.5 / p.dx) * (u0 + fabs(u0)) * (u0 - uW) + (0.5 / p.dx) * (u0 - fabs(u0)) * (uE - u0) +
+              (0.5 / p.dy) * (vX + fabs(vX)) * (u0 - uS) + (0.5 / p.dy) * (vX - fabs(vX)) * (uN - u0);
+  if (u0 == 0) ax = 0;
+  const double ck = w.CFLx[k];
+  const double den = p.CFLh - p.CFLl;
+#define FREHD_LIMIT_X(cc)                                              \
+  {                                                                    \
+    const double c_ = (cc);                                            \
+    if (c_ > p.CFLl && c_ <= p.CFLh) ax = ax * (p.CFLh - ck) / den;    \
+    else if (c_ > p.CFLh) ax = 0;                                      \
+  }
+  if (j > 0) FREHD_LIMIT_X(rd(w.CFLx, g, i, j - 1));
+  if (i > 0) FREHD_LIMIT_X(rd(w.CFLx, g, i - 1, j));
+  FREHD_LIMIT_X(ck);
+#undef FREHD_LIMIT_X
+  double En = u0 - p.dt * ax;
+  const double Vx = w.Vx[k];
+  double fx = 0;
+  if (Vx > 0) {
+    fx = (p.NUx / Vx) * (rd(w.Nx, g, i + 1, j) * (uE - u0) / p.dx - w.Nx[k] * (-uW + u0) / p.dx) +
+         (p.NUy / Vx) * (w.Oy[k] * (uN - u0) / p.dy - rd(w.Oy, g, i, j - 1) * (-uS + u0) / p.dy);
+  }
+  En = En + p.dt * fx;
+  const double velx = sqrt(u0 * u0 + vX * vX);
+  const double hx = Vx > 0 ? w.Zx[k] / Vx : 0;
+  Ex r;
+  r.Drag = 0.5 * p.dt * w.CDXP[k] * velx * hx;
+  r.En = En / (1 + r.Drag);
+  return r;
+}
+
+// y-momentum counterpart.  The y limiter uses a strict upper bound and its
+// zeroing branch tests CFLx, not CFLy (nsfunctions.c:561,574).
+__device__ Ex explicit_y(const View &w, int i, int j) {
+  const Params &p = w.p;
+  const Grid &g = w.gr;
+  const long k = g.at(i, j);
+  const double *v = w.v;
+  const double v0 = v[k], vE = rd(v, g, i + 1, j), vW = rd(v, g, i - 1, j);
+  const double vN = rd(v, g, i, j + 1), vS = rd(v, g, i, j - 1);
+  const double uY = uuYP_at(w, i, j);
+  double ay = (0.5 / p.dx) * (uY + fabs(uY)) * (v0 - vW) + (0.5 / p.dx) * (uY - fabs(uY)) * (vE - v0) +
+              (0.5 / p.dy) * (v0 + fabs(v0)) * (v0 - vS) + (0.5 / p.dy) * (v0 - fabs(v0)) * (vN - v0);
+  if (v0 == 0) ay = 0;
+  const double ck = w.CFLy[k];
+  const double den = p.CFLh - p.CFLl;
+#define FREHD_LIMIT_Y(ii_, jj_)                                        \
+  {                                                                    \
+    const long c_ = g.at(ii_, jj_);                                    \
+    const double cy_ = w.CFLy[c_];                                     \
+    if (cy_ > p.CFLl && cy_ < p.CFLh) ay = ay * (p.CFLh - ck) / den;   \
+    else if (w.CFLx[c_] > p.CFLh) ay = 0;                              \
+  }
+  if (j > 0) FREHD_LIMIT_Y(i, j - 1);
+  if (i > 0) FREHD_LIMIT_Y(i - 1, j);
+  FREHD_LIMIT_Y(i, j);
+#undef FREHD_LIMIT_Y
+  double En = v0 - p.dt * ay;
+  const double Vy = w.Vy[k];
+  double fy = 0;
+  if (Vy > 0) {
+    fy = (p.NUx / Vy) * (w.Nx[k] * (vE - v0) / p.dx - rd(w.Nx, g, i - 1, j) * (-vW + v0) / p.dx) +
+         (p.NUy / Vy) * (rd(w.Oy, g, i, j + 1) * (vN - v0) / p.dy - w.Oy[k] * (-vS + v0) / p.dy);
+  }
+  En = En + p.dt * fy;
+  const double vely = sqrt(uY * uY + v0 * v0);
+  const double hy = Vy > 0 ? w.Zy[k] / Vy : 0;
+  Ex r;
+  r.Drag = 0.5 * p.dt * w.CDYP[k] * vely * hy;
+  r.En = En / (1 + r.Drag);
+  return r;
+}
+
+// Face coefficient of matrixCoeffSub (subgrid.c:1012-1019); the same double
+// from either side of the face.
+__device__ __forceinline__ double gface(double coef, double N, double Vf, double Drag) {
+  return Vf > 0 ? coef * N * N / Vf / 1.0 / (1 + Drag) : 0.0;
+}
+
+// ---------------------------------------------------------------- k_explicit
+// Writes EnXP/EnYP, the face coefficients Gx (east face) and Gy (north face),
+// the row diagonal Ct (negated for rows the reference decouples: tidal rows and
+// closed dry cells) and the right-hand side b, all in the padded layout.
+__global__ void k_explicit(View w) {
+  if (*(volatile int *)&w.sc->status != FREHD_OK) return;  // a fatal step stops the run
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const Params &p = w.p;
+  const Grid &g = w.gr;
+  if (i >= g.nx || j >= g.ny) return;
+  const long k = g.at(i, j);
+  const Ex ex = explicit_x(w, i, j);
+  const Ex ey = explicit_y(w, i, j);
+  double EnW = 0.0, DrW = 0.0, EnS = 0.0, DrS = 0.0;  // ghosts never written: 0
+  if (i > 0) {
+    const Ex e = explicit_x(w, i - 1, j);
+    EnW = e.En;
+    DrW = e.Drag;
+  }
+  if (j > 0) {
+    const Ex e = explicit_y(w, i, j - 1);
+    EnS = e.En;
+    DrS = e.Drag;
+  }
+  w.EnXP[k] = ex.En;
+  w.EnYP[k] = ey.En;
+  if (j == 0) w.EnXP[g.at(i, -1)] = ex.En;  // dragInversion ghost copies
+  if (i == 0) w.EnYP[g.at(-1, j)] = ey.En;
+
+  const double coef = p.g * (p.dt * p.dt);
+  const double NxW = rd(w.Nx, g, i - 1, j), OyS = rd(w.Oy, g, i, j - 1);
+  double GnXP = gface(coef, w.Nx[k], w.Vx[k], ex.Drag);
+  double GnXM = gface(coef, NxW, rd(w.Vx, g, i - 1, j), DrW);
+  double GnYP = gface(coef, w.Oy[k], w.Vy[k], ey.Drag);
+  double GnYM = gface(coef, OyS, rd(w.Vy, g, i, j - 1), DrS);
+  const double gxe = GnXP, gyn = GnYP;
+  const double dxdy = p.dx * p.dy;
+  double Ct = w.Z[k] + GnXP + GnYP + GnXM + GnYM;
+  // matrixSourceTermSub (subgrid.c:934-974), no inflow cells
+  const double s = w.surf_cur[k];
+  double b = s * w.Z[k] - p.dt * (ex.En * w.Nx[k] - EnW * NxW) - p.dt * (ey.En * w.Oy[k] - EnS * OyS);
+  if (b == 0 || b == s * p.dx * p.dy) b = s * p.dx * p.dy;
+  // matrixCoeffSub singular-row guards (subgrid.c:1061-1078)
+  if (Ct == 0.0 || Ct == dxdy) Ct = dxdy;
+  bool iso = false;
+  if (w.depth_cur[k] == 0 && w.u[k] == 0 && rd(w.u, g, i - 1, j) == 0 && w.v[k] == 0 &&
+      rd(w.v, g, i, j - 1) == 0) {
+    Ct = dxdy;
+    GnXM = 0.0; GnXP = 0.0; GnYM = 0.0; GnYP = 0.0;
+    b = s * p.dx * p.dy;
+    iso = true;
+  }
+  // adjustMatrixBoundary (nsfunctions.c:846-884), one rank
+  if (i == 0) { Ct = Ct - GnXM; GnXM = 0; }
+  if (i == g.nx - 1) { Ct = Ct - GnXP; GnXP = 0; }
+  if (j == 0) { Ct = Ct - GnYM; GnYM = 0; }
+  if (j == g.ny - 1) { Ct = Ct - GnYP; GnYP = 0; }
+  // adjustTidalBoundary (nsfunctions.c:887-905)
+  if (is_tidal(p, i, j)) {
+    Ct = 1;
+    b = tide_value(w) + p.offset;
+    iso = true;
+  }
+  w.Gx[k] = (i == g.nx - 1) ? 0.0 : gxe;
+  w.Gy[k] = (j == g.ny - 1) ? 0.0 : gyn;
+  w.Ct[k] = iso ? -Ct : Ct;
+  w.b[k] = b;
+}
+
+// ---------------------------------------------------------------- subgrid
+__device__ __forceinline__ double interp_surf(double x, double x1, double y1, double x2, double y2) {
+  // interpSurf (utilities.c:155-162)
+  if (x2 == x1) return y1;
+  return (y2 - y1) * (x - x2) / (x2 - x1) + y2;
+}
+
+__device__ __forceinline__ double level_surf(const Params &p, int k) {
+  return frehd_level(p.surfmin, p.dsurf, k) + p.offset;  // subgrid.c:2118
+}
+
+__device__ __forceinline__ void level_values(const Params &p, int i, int j, int k, frehd_cell_levels *o) {
+  if (p.geom_fine) {
+    frehd_cell_levels_at(p.zf, p.fpitch, p.nx, p.ny, p.r, i, j, frehd_level(p.surfmin, p.dsurf, k),
+                         p.dxf * p.dyf, p.dxf, o);
+  } else {
+    const long N = (long)p.nx * p.ny, T = N * p.Ne;
+    const double *t = p.tab + (long)k * N + (long)j * p.nx + i;
+    o->V = t[0]; o->Z = t[T]; o->Vxp = t[2 * T]; o->Vxm = t[3 * T]; o->Vyp = t[4 * T];
+    o->Vym = t[5 * T]; o->Np = t[6 * T]; o->Nm = t[7 * T]; o->Op = t[8 * T]; o->Om = t[9 * T];
+  }
+}
+
+struct SubCell {
+  double V, Z, Vxp, Vxm, Vyp, Vym, Np, Nm, Op, Om;
+};
+
+// computeSubArea for one cell (subgrid.c:87-249) with useSubDrag = 0 and
+// useminA = 0; the minV* interpolations feed only useminV = 1/2 and are skipped.
+__device__ SubCell compute_sub_area(const View &w, int i, int j, double s, int *ind_io,
+                                    double depth_old) {
+  const Params &p = w.p;
+  const Grid &g = w.gr;
+  const double ds = p.dsurf;
+  const double thr = 0.5 * ds + ds / 100;
+  int ind = *ind_io;
+  for (int guard = 0; guard <= p.Ne + 1 && fabs(level_surf(p, ind) - s) > thr; ++guard) {
+    if (s > level_surf(p, ind)) ind += 1; else ind -= 1;
+    if (ind < 0) { ind = 0; break; }
+    if (ind > p.Ne - 1) { ind = p.Ne - 1; break; }
+  }
+  *ind_io = ind;
+  const int j1 = ind;
+  int j2;
+  if (j1 == 0) j2 = 0;
+  else if (j1 == p.Ne - 1) j2 = p.Ne - 1;
+  else j2 = s > level_surf(p, j1) ? j1 + 1 : j1 - 1;
+  const double a1 = level_surf(p, j1), a2 = level_surf(p, j2);
+  frehd_cell_levels L1, L2;
+  level_values(p, i, j, j1, &L1);
+  if (j2 != j1) level_values(p, i, j, j2, &L2); else L2 = L1;
+  SubCell c;
+  c.V = interp_surf(s, a1, L1.V, a2, L2.V);
+  c.Z = interp_surf(s, a1, L1.Z, a2, L2.Z);
+  c.Vxp = interp_surf(s, a1, L1.Vxp, a2, L2.Vxp);
+  c.Vyp = interp_surf(s, a1, L1.Vyp, a2, L2.Vyp);
+  c.Vxm = interp_surf(s, a1, L1.Vxm, a2, L2.Vxm);
+  c.Vym = interp_surf(s, a1, L1.Vym, a2, L2.Vym);
+  const double bxp = rd(w.bottomXP, g, i, j), byp = rd(w.bottomYP, g, i, j);
+  const double bxm = i > 0 ? rd(w.bottomXP, g, i - 1, j) : 0.0;  // edgeX is N-sized: ghost reads 0
+  const double bym = j > 0 ? rd(w.bottomYP, g, i, j - 1) : 0.0;
+#define FREHD_FACE(out, wd, f)                                                         \
+  {                                                                                    \
+    const double wd_ = (wd);                                                           \
+    if (wd_ > a1 && wd_ < a2) out = wd_ > s ? 0.0 : interp_surf(s, wd_, 0.0, a2, L2.f); \
+    else out = interp_surf(s, a1, L1.f, a2, L2.f);                                     \
+  }
+  FREHD_FACE(c.Np, bxp, Np);
+  FREHD_FACE(c.Nm, bxm, Nm);
+  FREHD_FACE(c.Op, byp, Op);
+  FREHD_FACE(c.Om, bym, Om);
+#undef FREHD_FACE
+  if (depth_old == 0) { c.Vxp = 0; c.Vyp = 0; c.Vxm = 0; c.Vym = 0; }
+  if (s - bxp <= 0) c.Np = 0;
+  if (s - byp <= 0) c.Op = 0;
+  if (i > 0 && s - bxm <= 0) c.Nm = 0;
+  if (j > 0 && s - bym <= 0) c.Om = 0;
+  return c;
+}
+
+// New surface of one cell: getFreeSurface, zeroNegSurf, enforceTidalBC
+// (nsfunctions.c:436-449,412-433,1020-1031) and limiterCFL (nsfunctions.c:452-495).
+// pre = the value enforceFreeSurfaceBC copies into ghosts (before tide and limiter).
+struct NewSurf {
+  double s, pre;
+  unsigned char rmv;
+};
+
+__device__ NewSurf new_surface(const View &w, int i, int j) {
+  const Params &p = w.p;
+  const Grid &g = w.gr;
+  const long k = g.at(i, j);
+  const double bz = w.bottomZ[k];
+  NewSurf r;
+  double s = w.x[k];
+  if (s < bz) s = bz;
+  r.pre = s;
+  if (is_tidal(p, i, j)) {
+    const double h = tide_value(w) + p.offset;
+    if (h > bz) s = h;
+  }
+  r.rmv = 0;
+  double diff = s - bz;
+  if (w.depth_cur[k] <= 0 && diff > 0) {
+    const double so = w.surf_cur[k] + p.minDepth;
+    const bool iP = rd(w.surf_cur, g, i + 1, j) <= so | rd(w.depth_cur, g, i + 1, j) <= 0;
+    const bool iM = rd(w.surf_cur, g, i - 1, j) <= so | rd(w.depth_cur, g, i - 1, j) <= 0;
+    const bool jP = rd(w.surf_cur, g, i, j + 1) <= so | rd(w.depth_cur, g, i, j + 1) <= 0;
+    const bool jM = rd(w.surf_cur, g, i, j - 1) <= so | rd(w.depth_cur, g, i, j - 1) <= 0;
+    if (iP & iM & jP & jM) {
+      s = bz;
+      r.rmv = 1;
+    }
+  }
+  diff = s - bz;
+  if (diff <= p.minDepth && diff > 0) s = bz;
+  r.s = s;
+  return r;
+}
+
+// ---------------------------------------------------------------- k_update_geo
+// Shared-memory tile: each 32x8 block evaluates the subgrid half-cell values of
+// its cells plus one column east and one row north, then combines them.
+constexpr int TBX = 32, TBY = 8, EX = TBX + 1, EY = TBY + 1;
+
+template <bool kInit>
+__global__ void __launch_bounds__(TBX *TBY) k_update_geo(View w) {
+  if (!kInit && *(volatile int *)&w.sc->status != FREHD_OK) return;
+  const Params &p = w.p;
+  const Grid &g = w.gr;
+  __shared__ double sh_s[EY][EX], sh_Np[EY][EX], sh_Nm[EY][EX], sh_Op[EY][EX], sh_Om[EY][EX];
+  __shared__ double sh_Vxp[EY][EX], sh_Vxm[EY][EX], sh_Vyp[EY][EX], sh_Vym[EY][EX];
+  __shared__ double sh_V[EY][EX], sh_Z[EY][EX];
+  const int i0 = blockIdx.x * TBX, j0 = blockIdx.y * TBY;
+  const int tid = threadIdx.y * TBX + threadIdx.x;
+  for (int e = tid; e < EX * EY; e += TBX * TBY) {
+    const int ex = e % EX, ey = e / EX;
+    const int i = i0 + ex, j = j0 + ey;
+    if (i >= g.nx || j >= g.ny) continue;
+    const long k = g.at(i, j);
+    const bool own = ex < TBX && ey < TBY;
+    double s;
+    double depth_old = w.depth_cur[k];
+    if (kInit) {
+      s = w.surf_cur[k];
+    } else {
+      const NewSurf ns = new_surface(w, i, j);
+      s = ns.s;
+      if (own) {
+        w.rmv[k] = ns.rmv;
+        w.surf_nxt[k] = s;
+        // enforceFreeSurfaceBC ghosts and corners (nsfunctions.c:317-334)
+        if (i == 0) w.surf_nxt[g.at(-1, j)] = ns.pre;
+        if (i == g.nx - 1) w.surf_nxt[g.at(g.nx, j)] = ns.pre;
+        if (j == 0) w.surf_nxt[g.at(i, -1)] = ns.pre;
+        if (j == g.ny - 1) w.surf_nxt[g.at(i, g.ny)] = ns.pre;
+        if (i == g.nx - 1 && j == g.ny - 1) w.surf_nxt[g.at(g.nx, g.ny)] = ns.pre;
+        if (i == 0 && j == g.ny - 1) w.surf_nxt[g.at(g.nx, -1)] = ns.pre;
+        if (i == g.nx - 1 && j == 0) w.surf_nxt[g.at(-1, g.ny)] = ns.pre;
+        if (i == 0 && j == 0) w.surf_nxt[g.at(-1, -1)] = ns.pre;
+        // computeVolumeSub keeps the previous V as the volume to update
+        w.cellV[k] = w.V[k];
+        double dn = s - w.bottomZ[k];
+        if (dn < 0) dn = 0;
+        w.depth_nxt[k] = dn;  // updateDepth (nsfunctions.c:239-247)
+      }
+    }
+    int ind = w.ind_cur[k];
+    const SubCell c = compute_sub_area(w, i, j, s, &ind, depth_old);
+    if (own) w.ind_nxt[k] = ind;
+    sh_s[ey][ex] = s;
+    sh_Np[ey][ex] = c.Np; sh_Nm[ey][ex] = c.Nm; sh_Op[ey][ex] = c.Op; sh_Om[ey][ex] = c.Om;
+    sh_Vxp[ey][ex] = c.Vxp; sh_Vxm[ey][ex] = c.Vxm; sh_Vyp[ey][ex] = c.Vyp; sh_Vym[ey][ex] = c.Vym;
+    sh_V[ey][ex] = c.V; sh_Z[ey][ex] = c.Z;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = i0 + tx, j = j0 + ty;
+  if (i >= g.nx || j >= g.ny) return;
+  // combineSubArea (subgrid.c:264-525), useminA = 0, useminV not 1/2, one rank
+  const double dxdy = p.dx * p.dy;
+  const double s = sh_s[ty][tx], Z = sh_Z[ty][tx];
+  const bool e = i + 1 < g.nx, n = j + 1 < g.ny;
+  double Nx, Oy, Vx, Vy, Zx, Zy;
+  if (e) Nx = sh_Np[ty][tx] >= sh_Nm[ty][tx + 1] ? sh_Np[ty][tx] : sh_Nm[ty][tx + 1];
+  else Nx = sh_Np[ty][tx];
+  if (n) Oy = sh_Op[ty][tx] >= sh_Om[ty + 1][tx] ? sh_Op[ty][tx] : sh_Om[ty + 1][tx];
+  else Oy = sh_Op[ty][tx];
+  const double bxp = rd(w.bottomXP, g, i, j), byp = rd(w.bottomYP, g, i, j);
+  if (e) {
+    const double a = sh_Vxp[ty][tx], bm = sh_Vxm[ty][tx + 1];
+    if (a > 0 && bm > 0) Vx = a + bm; else Vx = 2.0 * (a + bm);
+    Zx = Z;
+    if (Vx > 0 && Zx <= 0) Zx = dxdy;
+    if (s < bxp) { Vx = bm; Zx = 0.5 * Z; }
+    if (sh_s[ty][tx + 1] < bxp) { Vx = a; Zx = 0.5 * Z; }
+  } else {
+    Vx = 2 * sh_Vxp[ty][tx];
+    Zx = 2 * Z;
+  }
+  if (n) {
+    const double a = sh_Vyp[ty][tx], bm = sh_Vym[ty + 1][tx];
+    if (a > 0 && bm > 0) Vy = a + bm; else Vy = 2.0 * (a + bm);
+    Zy = Z;
+    if (Vy > 0 && Zy <= 0) Zy = dxdy;
+    if (s < byp) { Vy = bm; Zy = 0.5 * Z; }
+    if (sh_s[ty + 1][tx] < byp) { Vy = a; Zy = 0.5 * Z; }
+  } else {
+    Vy = 2 * sh_Vyp[ty][tx];
+    Zy = 2 * Z;
+  }
+  const double Vmin = 0.002, Amin = 0.002, Azmin = 0.002;
+  double V = sh_V[ty][tx], Zc = Z;
+  if (Vx < Vmin) Vx = 0.0;
+  if (Vy < Vmin) Vy = 0.0;
+  if (V < Vmin) V = 0.0;
+  if (Zc < Azmin) Zc = 1.0;
+  if (Zx < Amin) Zx = 0.0;
+  if (Zy < Amin) Zy = 0.0;
+  if (Nx < Amin) Nx = 0.0;
+  if (Oy < Amin) Oy = 0.0;
+  // boundary copies (subgrid.c:438-525): x ghosts first, then Nx closed on
+  // east/west faces, then y ghosts, then Oy closed south and on the YP row
+  // except at tidal cells.
+  double *arr[8] = {w.Vx, w.Vy, w.Zx, w.Zy, w.Nx, w.Oy, w.V, w.Z};
+  double val[8] = {Vx, Vy, Zx, Zy, Nx, Oy, V, Zc};
+  if (i == 0) {
+    const long q = g.at(-1, j);
+    for (int a = 0; a < 8; ++a) arr[a][q] = val[a];
+    w.Nx[q] = 0;
+  }
+  if (i == g.nx - 1) {
+    const long q = g.at(g.nx, j);
+    for (int a = 0; a < 8; ++a) arr[a][q] = val[a];
+    w.Nx[q] = 0;
+    val[4] = 0;  // Nx[iPbd] = 0
+  }
+  if (j == 0) {
+    const long q = g.at(i, -1);
+    for (int a = 0; a < 8; ++a) arr[a][q] = val[a];
+    w.Oy[q] = 0;
+  }
+  if (j == g.ny - 1) {
+    const long q = g.at(i, g.ny);
+    for (int a = 0; a < 8; ++a) arr[a][q] = val[a];
+    if (!is_tidal(p, i, j)) {
+      w.Oy[q] = 0;
+      val[5] = 0;
+    }
+  }
+  const long k = g.at(i, j);
+  for (int a = 0; a < 8; ++a) arr[a][k] = val[a];
+}
+
+template __global__ void k_update_geo<false>(View);
+template __global__ void k_update_geo<true>(View);
+
+// ---------------------------------------------------------------- k_update_vel
+// Final velocity of the east face of (i, j): updateVelocitySub (subgrid.c:1084-1176),
+// the dry-cell outflow and CFL-limiter zeroing, and waterfallCorrectionSub
+// (subgrid.c:1400-1444) with detectWaterfallLocationSub's flag (subgrid.c:1335-1396;
+// the XM pass runs after the XP pass, so +1 wins).
+__device__ double face_u(const View &w, int i, int j) {
+  const Params &p = w.p;
+  const Grid &g = w.gr;
+  const long k = g.at(i, j), kE = g.at(i + 1, j);
+  const double Vx = w.Vx[k], Nx = w.Nx[k];
+  const double hx = Vx > 0 ? Nx / Vx : 0;
+  const double s = w.surf_nxt[k], sE = w.surf_nxt[kE];
+  double u = w.EnXP[k] - (p.g * p.dt * hx) * (sE - s) / 1.0;
+  const bool e = i + 1 < g.nx;
+  if (Nx == 0) u = 0;
+  if (w.depth_nxt[k] == 0 && u > 0) u = 0;
+  if (e && w.depth_nxt[kE] == 0 && u < 0) u = 0;
+  if (w.rmv[k] == 1 || (e && w.rmv[kE] == 1)) u = 0;
+  const double b = w.bottomXP[k];
+  double f = 0;
+  if (s < b && sE - b >= p.wtfh) f = -1;
+  if (e && sE < b && s - b >= p.wtfh) f = 1;
+  if (f != 0) {
+    const double CFLmax = 0.24 / p.subR;
+    u = f * 0.7 * sqrt(2 * p.g * Nx / p.dy);
+    if (fabs(u) > CFLmax * p.dx / p.dt) u = f * CFLmax * p.dx / p.dt;
+  }
+  return u;
+}
+
+__device__ double face_v(const View &w, int i, int j) {
+  const Params &p = w.p;
+  const Grid &g = w.gr;
+  const long k = g.at(i, j), kN = g.at(i, j + 1);
+  const double Vy = w.Vy[k], Oy = w.Oy[k];
+  const double hy = Vy > 0 ? Oy / Vy : 0;
+  const double s = w.surf_nxt[k], sN = w.surf_nxt[kN];
+  double v = w.EnYP[k] - (p.g * p.dt * hy) * (sN - s) / 1.0;
+  const bool n = j + 1 < g.ny;
+  if (Oy == 0) v = 0;
+  if (w.depth_nxt[k] == 0 && v > 0) v = 0;
+  if (n && w.depth_nxt[kN] == 0 && v < 0) v = 0;
+  if (w.rmv[k] == 1 || (n && w.rmv[kN] == 1)) v = 0;
+  const double b = w.bottomYP[k];
+  double f = 0;
+  if (s < b && sN - b >= p.wtfh) f = -1;
+  if (n && sN < b && s - b >= p.wtfh) f = 1;
+  if (f != 0) {
+    const double CFLmax = 0.24 / p.subR;
+    v = f * 0.7 * sqrt(2 * p.g * Oy / p.dx);
+    if (fabs(v) > CFLmax * p.dy / p.dt) v = f * CFLmax * p.dy / p.dt;
+  }
+  return v;
+}
+
+__device__ __forceinline__ unsigned long long dbits(double x) {
+  return (unsigned long long)__double_as_longlong(x);
+}
+
+__global__ void __launch_bounds__(TBX *TBY) k_update_vel(View w) {
+  if (*(volatile int *)&w.sc->status != FREHD_OK) return;
+  const Params &p = w.p;
+  const Grid &g = w.gr;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  double cflx = 0, cfly = 0, vol = 0;
+  int nwarn = 0;
+  if (i < g.nx && j < g.ny) {
+    const long k = g.at(i, j);
+    const double uE = face_u(w, i, j);
+    const double uW = i > 0 ? face_u(w, i - 1, j) : uE;  // enforceVelocityBC ghost copy
+    const double vN = face_v(w, i, j);
+    const double vS = j > 0 ? face_v(w, i, j - 1) : vN;
+    // computeFaceFlowRateSub (subgrid.c:1190-1212)
+    const double NxW = rd(w.Nx, g, i - 1, j), OyS = rd(w.Oy, g, i, j - 1);
+    const double FE = uE * w.Nx[k], FW = uW * NxW, FN = vN * w.Oy[k], FS = vS * OyS;
+    double vstore = vN;
+    const double sN = w.surf_nxt[k];
+    if (is_tidal(p, i, j)) {
+      // adjustTidalVelocitySub (subgrid.c:1295-1313)
+      const double Fww = (sN - w.surf_cur[k]) * w.Z[k] / p.dt;
+      const double all = FS + FW - FE - Fww;
+      vstore = (all != 0 & w.Oy[k] > 0) ? all / w.Oy[k] : 0;
+    }
+    w.u[k] = uE;
+    w.v[k] = vstore;
+    w.Fuu[k] = FE;
+    w.Fvv[k] = FN;
+    // enforceVelocityBC ghosts (nsfunctions.c:289-314) and their face flows
+    if (i == 0) {
+      const long q = g.at(-1, j);
+      w.u[q] = uE; w.v[q] = vN; w.Fuu[q] = uE * w.Nx[q]; w.Fvv[q] = vN * w.Oy[q];
+    }
+    if (i == g.nx - 1) {
+      const long q = g.at(g.nx, j);
+      w.u[q] = uE; w.v[q] = vN; w.Fuu[q] = uE * w.Nx[q]; w.Fvv[q] = vN * w.Oy[q];
+    }
+    if (j == 0) {
+      const long q = g.at(i, -1);
+      w.u[q] = uE; w.v[q] = vN; w.Fuu[q] = uE * w.Nx[q]; w.Fvv[q] = vN * w.Oy[q];
+    }
+    if (j == g.ny - 1) {
+      const long q = g.at(i, g.ny);
+      w.u[q] = uE; w.v[q] = vN; w.Fuu[q] = uE * w.Nx[q]; w.Fvv[q] = vN * w.Oy[q];
+    }
+    // corners: u from the jP/jM ghost rows, v from the iP/iM ghost columns
+    if (i == g.nx - 1 && j == g.ny - 1) { w.u[g.at(g.nx, g.ny)] = uE; w.v[g.at(g.nx, g.ny)] = vN; }
+    if (i == g.nx - 1 && j == 0) w.u[g.at(g.nx, -1)] = uE;
+    if (i == 0 && j == g.ny - 1) { w.u[g.at(-1, g.ny)] = uE; w.v[g.at(g.nx, -1)] = vN; }
+    if (i == 0 && j == 0) { w.u[g.at(-1, -1)] = uE; w.v[g.at(-1, -1)] = vN; }
+    if (i == g.nx - 1 && j == 0) w.v[g.at(-1, g.ny)] = vN;
+    // corner face flows (computeFaceFlowRateSub runs over all N2ct entries)
+    if (i == g.nx - 1 && j == g.ny - 1) {
+      const long q = g.at(g.nx, g.ny);
+      w.Fuu[q] = w.u[q] * w.Nx[q]; w.Fvv[q] = w.v[q] * w.Oy[q];
+    }
+    // volumeByFluxSub (subgrid.c:1227-1263)
+    const double cv_old = w.cellV[k];
+    double cv = cv_old + p.dt * (FW - FE + FS - FN);
+    if (cv < 0) cv = 0;
+    w.cellV[k] = cv;
+    vol = cv;
+    // updateCDSub, useSubDrag = 0 (subgrid.c:1521-1536), then thinLayerDrag
+    // (nsfunctions.c:713-726) with the face depths of updateAllFaceDepth
+    const double coeff = p.g * p.manningN * p.manningN;
+    double CDX = w.CDXP[k], CDY = w.CDYP[k];
+    if (w.V[k] > 0) {
+      const double h = w.V[k] / w.Z[k];
+      CDX = coeff / pow(h, 1.0 / 3.0);
+      CDY = coeff / pow(h, 1.0 / 3.0);
+    }
+    const double dep = w.depth_nxt[k];
+    if (p.useThinLayer && dep > 0) {
+      double hxp = 0, hyp = 0;
+      if (i < g.nx - 1) {
+        const double a = sN, c = w.surf_nxt[g.at(i + 1, j)];
+        hxp = (a > c ? a : c) - w.bottomXP[k];
+        if (hxp < 0) hxp = 0;
+      }
+      if (j < g.ny - 1) {
+        const double a = sN, c = w.surf_nxt[g.at(i, j + 1)];
+        hyp = (a > c ? a : c) - w.bottomYP[k];
+        if (hyp < 0) hyp = 0;
+      }
+      if (hxp <= p.hD) CDX = coeff / pow(dep, 2.0 / 3.0);
+      if (hyp <= p.hD) CDY = coeff / pow(dep, 2.0 / 3.0);
+    }
+    w.CDXP[k] = CDX;
+    w.CDYP[k] = CDY;
+    // scalarTransport: upwind advection (scalar.c:72-97), scalarDiffusionSub
+    // (subgrid.c:1552-1567), updateScalarSub (subgrid.c:1570-1713), enforceScalarBC
+    // (scalar.c:419-471)
+    if (p.useScalar) {
+      const double *S = w.S_cur;
+      const double Sc = S[k], SE = rd(S, g, i + 1, j), SW = rd(S, g, i - 1, j);
+      const double SNn = rd(S, g, i, j + 1), SS = rd(S, g, i, j - 1);
+      double Sm = Sc * cv_old;  // computeVolumeSub: Sm = S * cellV
+      const double Sd = FE > 0 ? Sc : SE, Su = FW > 0 ? SW : Sc;
+      const double Sr = FN > 0 ? Sc : SNn, Sl = FS > 0 ? SS : Sc;
+      Sm = Sm + p.dt * (-FE * Sd + FW * Su - FN * Sr + FS * Sl);
+      Sm = Sm + p.dt * ((p.Kx * w.Nx[k] / p.dx) * (SE - Sc) - (p.Kx * NxW / p.dx) * (Sc - SW) +
+                        (p.Ky * w.Oy[k] / p.dy) * (SNn - Sc) - (p.Ky * OyS / p.dy) * (Sc - SS));
+      int cnt = 0;
+      double smax = 0, smin = 0;
+#define FREHD_NB(cond, val)                                 \
+  if (cond) {                                               \
+    const double v_ = (val);                                \
+    if (cnt == 0) { smax = v_; smin = v_; }                 \
+    else { if (v_ > smax) smax = v_; if (v_ < smin) smin = v_; } \
+    ++cnt;                                                  \
+  }
+      FREHD_NB(w.Nx[k] > 0 && rd(w.surf_cur, g, i + 1, j) - rd(w.bottomZ, g, i + 1, j) > 0, SE);
+      FREHD_NB(NxW > 0 && rd(w.surf_cur, g, i - 1, j) - rd(w.bottomZ, g, i - 1, j) > 0, SW);
+      FREHD_NB((j < g.ny - 1 || i == 0) && w.Oy[k] > 0 &&
+                   rd(w.surf_cur, g, i, j + 1) - rd(w.bottomZ, g, i, j + 1) > 0, SNn);
+      FREHD_NB(j > 0 && OyS > 0 && rd(w.surf_cur, g, i, j - 1) - rd(w.bottomZ, g, i, j - 1) > 0, SS);
+#undef FREHD_NB
+      double Sn = cv > 0 ? Sm / cv : 0;
+      if (cnt != 0 && Sn > smax) Sn = smax;
+      else if (cnt != 0 && Sn < smin) Sn = smin;
+      double depf = dep;
+      if ((Sn > 100 || Sn < 0) && !(j == 0) && !(j == g.ny - 1 && i > 0)) {
+        Sn = 0;
+        depf = 0;
+        const int slot = atomicAdd(&w.sc->n_fix, 1);
+        w.fix_list[slot] = (int)k;
+      }
+      if (i == 0) w.S_nxt[g.at(-1, j)] = Sn;
+      if (i == g.nx - 1) w.S_nxt[g.at(g.nx, j)] = Sn;
+      if (j == 0) w.S_nxt[g.at(i, -1)] = Sn;
+      if (j == g.ny - 1) w.S_nxt[g.at(i, g.ny)] = Sn;
+      if (is_tidal(p, i, j)) Sn = p.tidePS;
+      if (depf <= 0) Sn = 0;
+      w.S_nxt[k] = Sn;
+      w.Sm[k] = Sm;
+    }
+    // monitorCFL (nsfunctions.c:1196-1223)
+    cflx = fabs(uE) * p.dt / p.dx;
+    cfly = fabs(vstore) * p.dt / p.dy;
+    w.CFLx[k] = cflx;
+    w.CFLy[k] = cfly;
+    nwarn = (cflx > 2) + (cfly > 2);
+  }
+  // block reductions: max CFL, warnings, volume partial
+  cflx = warp_max(cflx);
+  cfly = warp_max(cfly);
+  nwarn = warp_sum_int(nwarn);
+  vol = warp_sum(vol);
+  __shared__ double sv[TBX * TBY / 32], sx[TBX * TBY / 32], sy[TBX * TBY / 32];
+  __shared__ int sw[TBX * TBY / 32];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  if (lane == 0) { sv[wid] = vol; sx[wid] = cflx; sy[wid] = cfly; sw[wid] = nwarn; }
+  __syncthreads();
+  if (tid == 0) {
+    double a = 0, mx = 0, my = 0;
+    int nw = 0;
+    for (int q = 0; q < TBX * TBY / 32; ++q) {
+      a += sv[q];
+      mx = fmax(mx, sx[q]);
+      my = fmax(my, sy[q]);
+      nw += sw[q];
+    }
+    w.partials[blockIdx.y * gridDim.x + blockIdx.x] = a;
+    if (mx > 0) atomicMax(&w.sc->max_cflx_bits, dbits(mx));
+    if (my > 0) atomicMax(&w.sc->max_cfly_bits, dbits(my));
+    if (nw) atomicAdd(&w.sc->n_cfl_warn, nw);
+  }
+}
+
+// ---------------------------------------------------------------- k_finish
+// The scalar singularity branch (subgrid.c:1700-1712) also lowers the surface
+// of the cell by its depth; cells are queued by k_update_vel and fixed here so
+// that no kernel reads a half-updated surface.  Then the step statistics.
+__global__ void k_finish(View w, int nblocks_vel, StepOut *out) {
+  const int tid = threadIdx.x;
+  if (*(volatile int *)&w.sc->status != FREHD_OK) {  // step skipped or aborted
+    if (tid == 0) out->status = w.sc->status;
+    return;
+  }
+  const int nfix = w.sc->n_fix;
+  for (int q = tid; q < nfix; q += blockDim.x) {
+    const int k = w.fix_list[q];
+    w.surf_nxt[k] = w.surf_nxt[k] - w.depth_nxt[k];
+    w.depth_nxt[k] = 0;
+  }
+  // fixed-order volume sum
+  __shared__ double sh[1024];
+  double a = 0;
+  for (int q = tid; q < nblocks_vel; q += blockDim.x) a += w.partials[q];
+  sh[tid] = a;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (tid < s) sh[tid] += sh[tid + s];
+    __syncthreads();
+  }
+  if (tid == 0) {
+    Scratch *sc = w.sc;
+    out->step = sc->tt;
+    out->cg_iters = sc->cg_iters;
+    out->status = FREHD_OK;
+    out->cg_rr = sc->cg_rr;
+    out->cg_bb = sc->cg_bb;
+    out->max_cflx = __longlong_as_double((long long)sc->max_cflx_bits);
+    out->max_cfly = __longlong_as_double((long long)sc->max_cfly_bits);
+    out->n_cfl_warn = sc->n_cfl_warn;
+    out->volume = sh[0];
+    out->n_fix = nfix;
+    sc->cg_iters_total += sc->cg_iters;
+    out->cg_iters_total = sc->cg_iters_total;
+    // monitorCFL's exit condition (nsfunctions.c:1226-1231)
+    if (fabs(out->max_cflx) > 20 || fabs(out->max_cfly) > 20) out->status = FREHD_ERR_CFL;
+    // reset the per-step counters for the next step
+    sc->n_fix = 0;
+    sc->n_cfl_warn = 0;
+    sc->max_cflx_bits = 0;
+    sc->max_cfly_bits = 0;
+    if (out->status != FREHD_OK) sc->status = out->status;
+    sc->tt = sc->tt + 1;
+  }
+}
+
+// ---------------------------------------------------------------- layout
+__global__ void k_ref_to_padded(double *dst, const double *src, long n, int nx, int ny, int pitch) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int i, j;
+  ref_to_ij(k, nx, ny, &i, &j);
+  dst[(long)(j + 1) * pitch + (i + kXOff)] = src[k];
+}
+
+__global__ void k_padded_to_ref(double *dst, const double *src, long n, int nx, int ny, int pitch) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int i, j;
+  ref_to_ij(k, nx, ny, &i, &j);
+  dst[k] = src[(long)(j + 1) * pitch + (i + kXOff)];
+}
+
+__global__ void k_ref_to_padded_int(int *dst, const int *src, long n, int nx, int ny, int pitch) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int i, j;
+  ref_to_ij(k, nx, ny, &i, &j);
+  dst[(long)(j + 1) * pitch + (i + kXOff)] = src[k];
+}
+
+__global__ void k_padded_to_ref_int(int *dst, const int *src, long n, int nx, int ny, int pitch) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int i, j;
+  ref_to_ij(k, nx, ny, &i, &j);
+  dst[k] = src[(long)(j + 1) * pitch + (i + kXOff)];
+}
+
+__global__ void k_fill(double *a, long n, double v) {
+  const long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (k < n) a[k] = v;
+}
+
+// uuYP / vvXP of the current velocities (for downloads).
+__global__ void k_interp_velocity(View w, double *uuYP, double *vvXP) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long N = (long)w.gr.nx * w.gr.ny;
+  if (t >= N) return;
+  const int i = (int)(t % w.gr.nx), j = (int)(t / w.gr.nx);
+  uuYP[t] = uuYP_at(w, i, j);
+  vvXP[t] = vvXP_at(w, i, j);
+}
+
+// Assembled system in the reference's terms (row-major Gn*, transposed z, x).
+__global__ void k_system_to_ref(View w, double *GnCt, double *GnXP, double *GnXM, double *GnYP,
+                                double *GnYM, double *z, double *xs) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const Grid &g = w.gr;
+  const long N = (long)g.nx * g.ny;
+  if (t >= N) return;
+  const int i = (int)(t % g.nx), j = (int)(t / g.nx);
+  const long k = g.at(i, j);
+  const double ct = w.Ct[k];
+  const bool iso = ct < 0;
+  if (GnCt) GnCt[t] = iso ? -ct : ct;
+  if (GnXP) GnXP[t] = (iso || i == g.nx - 1) ? 0.0 : w.Gx[k];
+  if (GnXM) GnXM[t] = (iso || i == 0) ? 0.0 : w.Gx[g.at(i - 1, j)];
+  if (GnYP) GnYP[t] = (iso || j == g.ny - 1) ? 0.0 : w.Gy[k];
+  if (GnYM) GnYM[t] = (iso || j == 0) ? 0.0 : w.Gy[g.at(i, j - 1)];
+  const long tr = (long)i * g.ny + j;  // sprt: transposed index of (i, j)
+  if (z) z[tr] = w.b[k];
+  if (xs) xs[tr] = w.x[k];
+}
+
+// Solution given in the transposed order into the padded x.
+__global__ void k_solution_from_ref(View w, const double *xs) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const Grid &g = w.gr;
+  const long N = (long)g.nx * g.ny;
+  if (t >= N) return;
+  const int i = (int)(t / g.ny), j = (int)(t % g.ny);  // trps
+  w.x[g.at(i, j)] = xs[t];
+}
+
+}  // namespace frehd

@@ -69,7 +69,7 @@ STATE_FIELDS = [
     "surfOld", "uuYP", "vvXP", "EnXP", "EnYP", "cellV", "Sm", "Fuu", "Fvv",
 ]
 # arrays carrying the ghost ring (N2ct) vs interior only (N)
-STATE_N = {"depth", "uuYP", "vvXP", "EnXP", "EnYP", "cellV", "Sm"}
+STATE_N = {"depth", "uuYP", "vvXP", "cellV", "Sm"}
 
 
 class State(C.Structure):
@@ -124,3 +124,212 @@ def build_bottoms(zf: np.ndarray, nx: int, ny: int, r: int):
     check(lib().frehd_build_bottoms(as_dp(zf), zf.shape[1], nx, ny, r, as_dp(b), as_dp(bx),
                                     as_dp(by)), "frehd_build_bottoms")
     return b, bx, by
+
+
+_vp = C.c_void_p
+
+PHASE_EXPLICIT, PHASE_SOLVE, PHASE_UPDATE = 1, 2, 3
+X0_ZERO, X0_SURFACE = 0, 1
+STATUS = {0: "ok", 1: "invalid", 2: "unsupported", 3: "cuda", 4: "nomem", 5: "cg_noconverge",
+          6: "cfl", 7: "timeout", 8: "state"}
+
+
+class KernelTimes(C.Structure):
+    _fields_ = [("explicit_ms", C.c_double), ("cg_ms", C.c_double), ("update_geo_ms", C.c_double),
+                ("update_vel_ms", C.c_double), ("finish_ms", C.c_double), ("steps", C.c_int),
+                ("cg_iters", C.c_longlong)]
+
+
+def _declare_domain(L: C.CDLL) -> None:
+    L.frehd_domain_set_profiling.argtypes = [_vp, C.c_int]
+    L.frehd_domain_kernel_times.argtypes = [_vp, C.POINTER(KernelTimes)]
+    L.frehd_domain_stream.argtypes = [_vp, C.POINTER(_vp)]
+    L.frehd_domain_create.argtypes = [C.POINTER(Config), C.c_int, C.POINTER(_vp)]
+    L.frehd_domain_destroy.argtypes = [_vp]
+    L.frehd_domain_set_tables.argtypes = [_vp, C.c_int, _dp]
+    L.frehd_domain_set_fine_bottoms.argtypes = [_vp, C.c_int, _dp, C.c_long]
+    L.frehd_domain_set_tide.argtypes = [_vp, C.c_int, _dp]
+    L.frehd_domain_set_solver.argtypes = [_vp, C.c_int]
+    L.frehd_domain_upload_state.argtypes = [_vp, C.POINTER(State)]
+    L.frehd_domain_download_state.argtypes = [_vp, C.POINTER(State)]
+    L.frehd_domain_init.argtypes = [_vp] + [_dp] * 7 + [C.c_int]
+    L.frehd_domain_step.argtypes = [_vp, C.c_int]
+    L.frehd_domain_run.argtypes = [_vp, C.c_int, C.c_int]
+    L.frehd_domain_phase.argtypes = [_vp, C.c_int, C.c_int, _dp]
+    L.frehd_domain_download_system.argtypes = [_vp] + [_dp] * 6
+    L.frehd_domain_download_solution.argtypes = [_vp, _dp]
+    L.frehd_domain_stats.argtypes = [_vp, C.POINTER(StepStats)]
+    L.frehd_domain_sync.argtypes = [_vp]
+    L.frehd_device_count.argtypes = [_ip]
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    lib().frehd_device_count(C.byref(n))
+    return n.value
+
+
+class Domain:
+    """One domain resident on a GPU, driven through the C ABI."""
+
+    def __init__(self, cfg: dict, device: int = 0):
+        L = lib()
+        if not hasattr(L, "_domain_declared"):
+            _declare_domain(L)
+            L._domain_declared = True
+        c = Config()
+        from .config import fill_struct
+        fill_struct(c, cfg)
+        h = _vp()
+        check(L.frehd_domain_create(C.byref(c), device, C.byref(h)), "frehd_domain_create")
+        self.h = h
+        self.cfg = dict(cfg)
+        self.nx, self.ny = cfg["nx"], cfg["ny"]
+        self.N = self.nx * self.ny
+        self.T = (self.nx + 2) * (self.ny + 2)
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().frehd_domain_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # geometry / forcing
+    def set_tables(self, tables: np.ndarray):
+        t = np.ascontiguousarray(tables, dtype=np.float64)
+        check(lib().frehd_domain_set_tables(self.h, t.shape[1], as_dp(t)), "set_tables")
+
+    def set_fine_bottoms(self, zf: np.ndarray, r: int):
+        z = np.ascontiguousarray(zf, dtype=np.float64)
+        check(lib().frehd_domain_set_fine_bottoms(self.h, r, as_dp(z), z.shape[1]), "set_fine_bottoms")
+
+    def set_tide(self, tideP: np.ndarray):
+        t = np.ascontiguousarray(tideP, dtype=np.float64)
+        check(lib().frehd_domain_set_tide(self.h, len(t), as_dp(t)), "set_tide")
+
+    def set_solver(self, x0: int):
+        check(lib().frehd_domain_set_solver(self.h, x0), "set_solver")
+
+    def init(self, bottom, bottomXP, bottomYP, surf0, u0=None, v0=None, S0=None,
+             round_trip_output: bool = True):
+        z = np.zeros(self.N)
+        arrs = [np.ascontiguousarray(a if a is not None else z, dtype=np.float64)
+                for a in (bottom, bottomXP, bottomYP, surf0, u0, v0, S0)]
+        check(lib().frehd_domain_init(self.h, *[as_dp(a) for a in arrs], int(round_trip_output)),
+              "init")
+
+    # state
+    def _len(self, name: str) -> int:
+        return self.N if name in STATE_N else self.T
+
+    def upload(self, arrays: dict):
+        st = State()
+        keep = []
+        for name, a in arrays.items():
+            if name not in STATE_FIELDS:
+                continue
+            if name == "ind":
+                b = np.ascontiguousarray(a, dtype=np.int32)
+                assert b.size == self.T
+                setattr(st, name, b.ctypes.data_as(_ip))
+            else:
+                b = np.ascontiguousarray(a, dtype=np.float64)
+                assert b.size == self._len(name), (name, b.size)
+                setattr(st, name, as_dp(b))
+            keep.append(b)
+        check(lib().frehd_domain_upload_state(self.h, C.byref(st)), "upload_state")
+
+    def download(self, names=None) -> dict:
+        names = STATE_FIELDS if names is None else names
+        st = State()
+        out = {}
+        for name in names:
+            if name == "ind":
+                a = np.empty(self.T, dtype=np.int32)
+                setattr(st, name, a.ctypes.data_as(_ip))
+            else:
+                a = np.empty(self._len(name))
+                setattr(st, name, as_dp(a))
+            out[name] = a
+        check(lib().frehd_domain_download_state(self.h, C.byref(st)), "download_state")
+        return out
+
+    def system(self) -> dict:
+        names = ["GnCt", "GnXP", "GnXM", "GnYP", "GnYM", "z"]
+        arrs = {n: np.empty(self.N) for n in names}
+        check(lib().frehd_domain_download_system(self.h, *[as_dp(arrs[n]) for n in names]),
+              "download_system")
+        return arrs
+
+    def solution(self) -> np.ndarray:
+        x = np.empty(self.N)
+        check(lib().frehd_domain_download_solution(self.h, as_dp(x)), "download_solution")
+        return x
+
+    # stepping
+    def phase(self, phase: int, tt: int, x_ext: np.ndarray | None = None) -> int:
+        if x_ext is not None:
+            x = np.ascontiguousarray(x_ext, dtype=np.float64)
+            rc = lib().frehd_domain_phase(self.h, phase, tt, as_dp(x))
+        else:
+            rc = lib().frehd_domain_phase(self.h, phase, tt, None)
+        if rc not in (0, 6):
+            check(rc, "phase")
+        return rc
+
+    def step(self, tt: int) -> int:
+        rc = lib().frehd_domain_step(self.h, tt)
+        if rc not in (0, 6):
+            check(rc, "step")
+        return rc
+
+    def run(self, t0: int, nsteps: int) -> int:
+        rc = lib().frehd_domain_run(self.h, t0, nsteps)
+        if rc not in (0, 6):
+            check(rc, "run")
+        return rc
+
+    def stats(self) -> dict:
+        s = StepStats()
+        check(lib().frehd_domain_stats(self.h, C.byref(s)), "stats")
+        return {n: getattr(s, n) for n, _ in StepStats._fields_}
+
+    def sync(self):
+        check(lib().frehd_domain_sync(self.h), "sync")
+
+    def set_profiling(self, on: bool):
+        check(lib().frehd_domain_set_profiling(self.h, int(on)), "set_profiling")
+
+    def kernel_times(self) -> dict:
+        t = KernelTimes()
+        check(lib().frehd_domain_kernel_times(self.h, C.byref(t)), "kernel_times")
+        return {n: getattr(t, n) for n, _ in KernelTimes._fields_}
+
+    def stream(self) -> int:
+        s = _vp()
+        check(lib().frehd_domain_stream(self.h, C.byref(s)), "stream")
+        return s.value or 0
+
+
+def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0_SURFACE):
+    """A Domain initialised from a generated deck (frehdc_b200.deck)."""
+    from . import deck as D
+    d = Domain(D.config_dict(deck), device)
+    if geometry == "fine":
+        d.set_fine_bottoms(deck.zf, deck.r)
+    else:
+        tabs = deck.extra.get("tables")
+        if tabs is None:
+            tabs = D.build_tables(deck)
+            deck.extra["tables"] = tabs
+        d.set_tables(tabs)
+    d.set_tide(D.tide_series(deck))
+    d.set_solver(x0)
+    d.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
+    return d

@@ -114,7 +114,7 @@ typedef struct frehd_state {
   /* per-step quantities (download only) */
   double *surfOld;           /* N2ct  */
   double *uuYP, *vvXP;       /* N     interpolated velocities (velocityInterp) */
-  double *EnXP, *EnYP;       /* N     explicit velocities after drag inversion */
+  double *EnXP, *EnYP;       /* N2ct  explicit velocities after drag inversion */
   double *cellV, *Sm;        /* N     cell volume and scalar mass after the update */
   double *Fuu, *Fvv;         /* N2ct  face flow rates */
 } frehd_state;
@@ -191,6 +191,18 @@ int frehd_domain_download_solution(frehd_domain *d, double *x);
 int frehd_domain_stats(frehd_domain *d, frehd_step_stats *out);
 /* Wait for all work queued on the domain's stream. */
 int frehd_domain_sync(frehd_domain *d);
+
+/* Accumulated device time per kernel (CUDA events on the domain's stream)
+ * while profiling is on, and the CG iterations those steps ran. */
+typedef struct frehd_kernel_times {
+  double explicit_ms, cg_ms, update_geo_ms, update_vel_ms, finish_ms;
+  int steps;
+  long long cg_iters;
+} frehd_kernel_times;
+int frehd_domain_set_profiling(frehd_domain *d, int on);  /* on: also resets the sums */
+int frehd_domain_kernel_times(frehd_domain *d, frehd_kernel_times *out);
+/* The CUDA stream (cudaStream_t) all work of the domain is queued on. */
+int frehd_domain_stream(frehd_domain *d, void **stream);
 
 /* Solver options (defaults: warm start from the current surface, Jacobi PCG). */
 enum { FREHD_X0_ZERO = 0, FREHD_X0_SURFACE = 1 };

@@ -1,0 +1,131 @@
+"""CUDA step parity (needs a B200): the device path against the C oracle,
+which the CPU suite pins bit for bit to the reference itself.
+
+Stencil phases must match the oracle's doubles exactly; the drag coefficients
+go through pow(), where CUDA and glibc may differ in the last place, so they
+are compared to 4 ulp-ish relative tolerance.  The linear solve is compared to
+the CG tolerance, whole runs to 1e-9 relative (the plain form's target).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from frehdc_b200 import deck as D
+from frehdc_b200 import native
+from oracle import port, refrun
+from tests.helpers import SPECS, deck_for, max_rel, mismatches
+
+pytestmark = pytest.mark.gpu
+
+EXACT = ["surf", "uuXP", "vvYP", "S", "depth", "V", "Z", "Nx", "Oy", "Vx", "Vy", "Zx", "Zy", "ind",
+         "surfOld", "cellV", "Sm", "Fuu", "Fvv", "CFLx", "CFLy", "uuYP", "vvXP"]
+POW = ["CDXP", "CDYP"]
+UPLOAD = ["surf", "uuXP", "vvYP", "S", "depth", "CDXP", "CDYP", "CFLx", "CFLy", "V", "Z", "Nx",
+          "Oy", "Vx", "Vy", "Zx", "Zy", "ind", "bottomZ", "bottomXP", "bottomYP"]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_gpu():
+    if native.device_count() < 1:
+        pytest.fail("no CUDA device visible: the GPU tests need a B200")
+
+
+def _oracle_state(o, names):
+    return {n: o.get(n) for n in names}
+
+
+@pytest.mark.parametrize("name", ["wet48x40", "dry40x36"])
+@pytest.mark.parametrize("geometry", ["fine", "tables"])
+def test_init_bitwise(name, geometry, scratch):
+    d, _ = deck_for(name, str(scratch))
+    o = port.from_deck(d)
+    g = native.domain_from_deck(d, geometry=geometry)
+    got = g.download(UPLOAD)
+    ref = _oracle_state(o, UPLOAD)
+    assert mismatches(got, ref, [n for n in UPLOAD if n not in POW]) == []
+    assert mismatches(got, ref, POW, exact=False, rtol=1e-15) == []
+
+
+@pytest.mark.parametrize("name,steps", [("wet48x40", 6), ("dry40x36", 25), ("dry37x29", 25)])
+def test_phases_bitwise(name, steps, scratch):
+    """Each step: the oracle's state is uploaded, then the device's explicit
+    phase and update phase (fed the oracle's x) must give the oracle's doubles."""
+    d, _ = deck_for(name, str(scratch))
+    o = port.from_deck(d, precond=port.PRECOND_JACOBI, x0=port.X0_SURFACE)
+    g = native.domain_from_deck(d, geometry="fine")
+    for tt in range(1, steps + 1):
+        g.upload(_oracle_state(o, UPLOAD))
+        o.explicit(tt)
+        g.phase(native.PHASE_EXPLICIT, tt)
+        sysg = g.system()
+        en = g.download(["EnXP", "EnYP"])
+        sysr = _oracle_state(o, ["GnCt", "GnXP", "GnXM", "GnYP", "GnYM", "z", "EnXP", "EnYP"])
+        assert mismatches({**sysg, **en}, sysr, list(sysr)) == [], tt
+        o.solve()
+        x = o.get("x")
+        o.update(tt, x)
+        g.phase(native.PHASE_UPDATE, tt, x_ext=x)
+        got = g.download(EXACT + POW)
+        ref = _oracle_state(o, EXACT + POW)
+        assert mismatches(got, ref, EXACT) == [], tt
+        assert mismatches(got, ref, POW, exact=False, rtol=1e-15) == [], tt
+
+
+@pytest.mark.parametrize("name", ["wet48x40", "dry40x36"])
+def test_solve_matches_oracle(name, scratch):
+    d, _ = deck_for(name, str(scratch))
+    o = port.from_deck(d, precond=port.PRECOND_JACOBI, x0=port.X0_SURFACE)
+    g = native.domain_from_deck(d, geometry="fine")
+    for tt in range(1, 4):
+        g.upload(_oracle_state(o, UPLOAD))
+        o.explicit(tt)
+        o.solve()
+        g.phase(native.PHASE_EXPLICIT, tt)
+        g.phase(native.PHASE_SOLVE, tt)
+        xg = g.solution()
+        assert max_rel(xg, o.get("x")) < 1e-12
+        o.update(tt, o.get("x"))
+
+
+@pytest.mark.parametrize("name", ["wet48x40", "dry40x36", "dry37x29"])
+def test_full_run_matches_oracle(name, scratch):
+    d, _ = deck_for(name, str(scratch))
+    steps = SPECS[name].steps
+    o = port.from_deck(d, precond=port.PRECOND_JACOBI, x0=port.X0_SURFACE)
+    for tt in range(1, steps + 1):
+        o.step(tt)
+    g = native.domain_from_deck(d, geometry="fine")
+    assert g.run(1, steps) == 0
+    st = g.stats()
+    assert st["step"] == steps
+    got = g.download(["surf", "uuXP", "vvYP", "S", "cellV"])
+    for n in ["surf", "uuXP", "vvYP", "S"]:
+        assert max_rel(got[n], o.get(n)) <= 1e-9, n
+    # volume ledger: the device's fixed-order sum of cellV equals the host sum
+    assert abs(st["volume"] - got["cellV"].sum()) <= 1e-12 * abs(got["cellV"].sum())
+
+
+@pytest.mark.skipif(not refrun.available(), reason="reference oracle binaries not present")
+@pytest.mark.parametrize("name", ["wet48x40", "dry40x36"])
+def test_full_run_matches_reference(name, scratch):
+    """Whole run against the reference program itself (SSOR-PCG from x = 0)."""
+    d, path = deck_for(name, str(scratch))
+    steps = SPECS[name].steps
+    ref = refrun.run(path, steps, os.path.join(path, "gpu_full.bin"))
+    g = native.domain_from_deck(d, geometry="fine")
+    assert g.run(1, steps) == 0
+    got = g.download(["surf", "uuXP", "vvYP", "S"])
+    for n in ["surf", "uuXP", "vvYP", "S"]:
+        assert max_rel(got[n], ref[n]) <= 1e-9, n
+
+
+def test_run_is_bit_reproducible(scratch):
+    d, _ = deck_for("dry40x36", str(scratch))
+    a = native.domain_from_deck(d, geometry="fine")
+    b = native.domain_from_deck(d, geometry="tables")
+    a.run(1, 15)
+    b.run(1, 15)
+    da = a.download(["surf", "uuXP", "vvYP", "S"])
+    db = b.download(["surf", "uuXP", "vvYP", "S"])
+    assert mismatches(da, db, list(da)) == []

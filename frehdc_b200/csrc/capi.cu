@@ -52,7 +52,7 @@ struct frehd_domain {
   double *stage = nullptr;      // device staging, T doubles
   double *stage2 = nullptr;
   int cur = 0;
-  int x0_mode = FREHD_X0_SURFACE;
+  int x0_mode = FREHD_X0_ZERO;
   int cg_blocks = 1;
   int geom_set = 0, ready = 0;
   frehd_step_stats last{};
@@ -290,11 +290,11 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
   if (!r) {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg, kCgThreads, 0);
-    long want = (d->N + kCgThreads - 1) / kCgThreads;
+    long want = (long)((d->gr.nx + 127) / 128) * ((d->gr.ny + kCgThreads / 32 - 1) / (kCgThreads / 32));
     long cap = (long)nsm * std::max(per, 1);
     d->cg_blocks = (int)std::max(1L, std::min(want, cap));
     const long nvel = (long)((d->gr.nx + 31) / 32) * ((d->gr.ny + 7) / 8);
-    d->npartials = std::max(nvel, 8L * d->cg_blocks);
+    d->npartials = std::max(nvel, 4L * d->cg_blocks + 8);
     r |= dalloc(d, &d->partials, d->npartials);
   }
   if (!r && cudaMallocHost((void **)&d->out_host, sizeof(StepOut)) != cudaSuccess)
@@ -409,10 +409,24 @@ extern "C" int frehd_domain_upload_state(frehd_domain *d, const frehd_state *st)
       int rc = upload_ref(d, it.dv, it.h, it.n);
       if (rc) return rc;
     }
+  // ping-pong state goes into both buffers, so ghost entries that no kernel
+  // rewrites keep the uploaded values whichever buffer is current
+  const int o = c ^ 1;
+  struct Item2 {
+    const double *h;
+    double *dv;
+    long n;
+  } twins[] = {{st->surf, d->surf[o], T}, {st->S, d->S[o], T}, {st->depth, d->depth[o], N}};
+  for (auto &it : twins)
+    if (it.h) {
+      int rc = upload_ref(d, it.dv, it.h, it.n);
+      if (rc) return rc;
+    }
   if (st->ind) {
     CUDA_TRY(cudaMemcpyAsync(d->stage, st->ind, sizeof(int) * T, cudaMemcpyHostToDevice, d->stream));
-    k_ref_to_padded_int<<<(unsigned)((T + 255) / 256), 256, 0, d->stream>>>(
-        d->ind[c], (const int *)d->stage, T, d->gr.nx, d->gr.ny, d->gr.pitch);
+    for (int a = 0; a < 2; ++a)
+      k_ref_to_padded_int<<<(unsigned)((T + 255) / 256), 256, 0, d->stream>>>(
+          d->ind[a], (const int *)d->stage, T, d->gr.nx, d->gr.ny, d->gr.pitch);
     CUDA_TRY(cudaGetLastError());
   }
   CUDA_TRY(cudaStreamSynchronize(d->stream));

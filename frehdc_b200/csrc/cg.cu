@@ -5,20 +5,32 @@
 // Here the system stays matrix-free in the padded layout written by k_explicit:
 // one face coefficient per east face (Gx) and north face (Gy) and the row
 // diagonal Ct.  Rows the reference decouples -- tidal rows (Ct = 1) and closed
-// dry cells (Ct = dx*dy) -- carry a negative Ct.  Their unknowns are known
-// exactly (x = b/|Ct|) and are eliminated: their couplings move to the
-// right-hand side of the neighbouring rows, which leaves a symmetric positive
-// definite system over the remaining rows.  The reference runs CG on the
+// dry cells (Ct = dx*dy) -- carry a negative Ct.  The reference runs CG on the
 // non-symmetric full matrix; both stop when ||r||_2 < eps*||b||_2 (rtc.c:53)
-// with ||b|| taken over the full right-hand side, so both solve the same system
-// to the same residual tolerance.
+// with ||b|| taken over the full right-hand side.
 //
-// One cooperative launch runs the whole solve: all blocks are co-resident and
-// meet at a grid barrier twice per iteration.  The barrier waits are bounded
-// (kBarrierTimeoutNs); a timeout records FREHD_ERR_TIMEOUT and every block
-// leaves.  Dot products are reduced in a fixed order (per-block partials, then
-// every block sums all partials in the same order), so every block computes the
-// same alpha/beta and runs are bit-reproducible.
+// A decoupled row has no off-diagonal entries, so inside the reference's CG it
+// is a lone eigen-component (lambda = 1 after Jacobi/SSOR scaling) and ends at
+// x = (b/Ct)(1 - P(1)), P the CG residual polynomial: within the tolerance of
+// b/Ct but on a side the CG picks.  That side decides later branches (a closed
+// dry cell with x a hair above its bed triggers limiterCFL's velocity removal,
+// nsfunctions.c:461-476).  So decoupled rows are iterated here too, as lambda = 1
+// components with their own residual, while their couplings into neighbouring
+// rows use the exact b/Ct (moved to the right-hand side): the system the CG
+// sees stays symmetric and each decoupled row gets the same kind of end value
+// as in the reference.
+//
+// One cooperative launch runs the whole solve.  Each block owns a fixed list of
+// 128 x 16 cell tiles for the whole solve.  Per iteration:
+//   phase 1  the block loads r, p_old and Ct of a tile plus a one-cell halo into
+//            shared memory (L2-coherent loads: other blocks wrote them), forms
+//            p = r/|Ct| + beta p_old there once, writes its own p and q = A p
+//   phase 2  x += alpha p, r -= alpha q, partial (r, M^-1 r) and ||r||^2
+// Each phase ends in grid_allreduce: blocks publish partial sums, the last block
+// to arrive sums them in a fixed order and releases the others, which then read
+// the totals -- one barrier per reduction, identical totals in every block,
+// bit-reproducible runs.  Waits are bounded (kBarrierTimeoutNs); a timeout
+// records FREHD_ERR_TIMEOUT and every block leaves.
 #include <cmath>
 
 #include "domain.cuh"
@@ -27,6 +39,10 @@
 namespace frehd {
 
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s per wait
+constexpr int CTX = 128, CTY = kCgThreads / 32;   // tile: 4 cells per thread along a row
+constexpr int HX = CTX + 2, HY = CTY + 2;         // tile + halo
+constexpr int CPT = 4;                            // cells per thread, stride 32 along a row
+constexpr int NWARP = kCgThreads / 32;
 
 __device__ __forceinline__ unsigned long long gtimer_ns() {
   unsigned long long t;
@@ -36,43 +52,13 @@ __device__ __forceinline__ unsigned long long gtimer_ns() {
 
 __device__ __forceinline__ double ld(const double *a, long k) { return __ldcg(a + k); }
 
-__device__ bool grid_barrier(Scratch *sc, unsigned nblocks) {
-  __shared__ int s_ok;
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile unsigned *gen = &sc->bar_gen;
-    const unsigned my = *gen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(&sc->bar_count, 1u);
-    int ok = 1;
-    if (arrived == nblocks - 1) {
-      atomicExch(&sc->bar_count, 0u);
-      __threadfence();
-      atomicAdd(&sc->bar_gen, 1u);
-    } else {
-      const unsigned long long t0 = gtimer_ns();
-      while (*gen == my) {
-        if (gtimer_ns() - t0 > kBarrierTimeoutNs) {
-          set_status(sc, FREHD_ERR_TIMEOUT);
-          ok = 0;
-          break;
-        }
-        __nanosleep(32);
-      }
-    }
-    __threadfence();
-    if (*(volatile int *)&sc->status == FREHD_ERR_TIMEOUT) ok = 0;
-    s_ok = ok;
-  }
-  __syncthreads();
-  return s_ok != 0;
-}
-
-// Write this block's partial sums of NV values (fixed reduction order).
+// Sum of NV values over all threads of all blocks, identical in every block,
+// and a grid barrier.  partials: 4 doubles per block; totals: 4 doubles.
 template <int NV>
-__device__ void block_partials(double (&v)[NV], double *out) {
-  __shared__ double sh[NV][kCgThreads / 32];
+__device__ bool grid_allreduce(double (&v)[NV], Scratch *sc, double *partials, double *totals,
+                               unsigned nblocks) {
+  __shared__ double sh[4][NWARP];
+  __shared__ int s_last, s_ok;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int m = 0; m < NV; ++m) {
@@ -80,91 +66,149 @@ __device__ void block_partials(double (&v)[NV], double *out) {
     if (lane == 0) sh[m][wid] = s;
   }
   __syncthreads();
+  unsigned my_gen = 0;
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int m = 0; m < NV; ++m) {
       double a = 0;
-      for (int q = 0; q < kCgThreads / 32; ++q) a += sh[m][q];
-      out[m] = a;
+      for (int q = 0; q < NWARP; ++q) a += sh[m][q];
+      partials[4 * blockIdx.x + m] = a;
     }
-  }
-}
-
-// Sum of all blocks' partials, identical in every block.
-template <int NV>
-__device__ void grid_total(const double *partials, unsigned nblocks, double (&tot)[NV]) {
-  __shared__ double sh[NV][kCgThreads / 32];
-  double a[NV];
-#pragma unroll
-  for (int m = 0; m < NV; ++m) a[m] = 0;
-  for (unsigned q = threadIdx.x; q < nblocks; q += blockDim.x) {
-#pragma unroll
-    for (int m = 0; m < NV; ++m) a[m] += ld(partials, (long)q * 4 + m);
-  }
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int m = 0; m < NV; ++m) {
-    const double s = warp_sum(a[m]);
-    if (lane == 0) sh[m][wid] = s;
+    // the generation can only move once every block (this one too) arrived
+    my_gen = *(volatile unsigned *)&sc->bar_gen;
+    __threadfence();
+    const unsigned arrived = atomicAdd(&sc->bar_count, 1u);
+    s_last = arrived == nblocks - 1;
+    s_ok = 1;
   }
   __syncthreads();
+  if (s_last) {
+    // every partial is visible: sum them in a fixed order, publish, release
+    __threadfence();
+    double a[4] = {0, 0, 0, 0};
+    for (unsigned q = threadIdx.x; q < nblocks; q += blockDim.x) {
 #pragma unroll
-  for (int m = 0; m < NV; ++m) {
-    double t = 0;
-    for (int q = 0; q < kCgThreads / 32; ++q) t += sh[m][q];
-    tot[m] = t;
+      for (int m = 0; m < NV; ++m) a[m] += ld(partials, 4 * (long)q + m);
+    }
+    __syncthreads();  // sh is reused
+#pragma unroll
+    for (int m = 0; m < NV; ++m) {
+      const double s = warp_sum(a[m]);
+      if (lane == 0) sh[m][wid] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int m = 0; m < NV; ++m) {
+        double t = 0;
+        for (int q = 0; q < NWARP; ++q) t += sh[m][q];
+        totals[m] = t;
+      }
+      *(volatile unsigned *)&sc->bar_count = 0;
+      __threadfence();
+      atomicAdd(&sc->bar_gen, 1u);
+    }
+  } else if (threadIdx.x == 0) {
+    volatile unsigned *gen = &sc->bar_gen;
+    const unsigned long long t0 = gtimer_ns();
+    while (*gen == my_gen) {
+      if (gtimer_ns() - t0 > kBarrierTimeoutNs) {
+        set_status(sc, FREHD_ERR_TIMEOUT);
+        s_ok = 0;
+        break;
+      }
+      __nanosleep(16);
+    }
+    __threadfence();
   }
   __syncthreads();
+  if (!s_ok || *(volatile int *)&sc->status == FREHD_ERR_TIMEOUT) return false;
+#pragma unroll
+  for (int m = 0; m < NV; ++m) v[m] = ld(totals, m);
+  return true;
 }
 
-__global__ void __launch_bounds__(kCgThreads) k_cg(View w, int x0_surface) {
+struct TileIt {
+  int ntx, nty, ntiles;
+};
+
+__device__ __forceinline__ void tile_origin(const TileIt &t, int tile, int *i0, int *j0) {
+  *i0 = (tile % t.ntx) * CTX;
+  *j0 = (tile / t.ntx) * CTY;
+}
+
+__global__ void __launch_bounds__(kCgThreads, 1) k_cg(View w, int x0_surface) {
   Scratch *sc = w.sc;
   if (*(volatile int *)&sc->status != FREHD_OK) return;
   const Grid g = w.gr;
   const Params &p = w.p;
-  const unsigned nx = g.nx, N = (unsigned)g.nx * g.ny;
+  const int nx = g.nx, ny = g.ny;
+  const long pitch = g.pitch;
   const unsigned nb = gridDim.x;
-  const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x, gs = nb * blockDim.x;
-  // two partial buffers, alternating per reduction, so a fast block never
-  // overwrites partials a slow block is still summing
-  double *part[2] = {w.partials, w.partials + 4 * (long)nb};
-  int pb = 0;
+  TileIt ti;
+  ti.ntx = (nx + CTX - 1) / CTX;
+  ti.nty = (ny + CTY - 1) / CTY;
+  ti.ntiles = ti.ntx * ti.nty;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  double *partials = w.partials, *totals = w.partials + 4 * (long)nb;
   const double *Ct = w.Ct, *Gx = w.Gx, *Gy = w.Gy;
+  __shared__ double s_p[HY][HX], s_c[HY][HX];
 
-  for (unsigned t = gtid; t < N; t += gs) {
-    const int i = t % nx, j = t / nx;
-    const long k = g.at(i, j);
-    const double ct = Ct[k];
-    w.x[k] = ct < 0 ? w.b[k] / (-ct) : (x0_surface ? w.surf_cur[k] : 0.0);
-    w.p0[k] = 0.0;
-    w.p1[k] = 0.0;
-  }
-  if (!grid_barrier(sc, nb)) return;
-
-  double acc[3] = {0, 0, 0};
-  for (unsigned t = gtid; t < N; t += gs) {
-    const int i = t % nx, j = t / nx;
-    const long k = g.at(i, j), kE = k + 1, kW = k - 1, kN = k + g.pitch, kS = k - g.pitch;
-    const double ct = Ct[k], bk = w.b[k];
-    double r = 0;
-    if (ct > 0) {
-      const double ax = ct * ld(w.x, k) -
-                        (Gx[k] * ld(w.x, kE) + Gx[kW] * ld(w.x, kW) + Gy[k] * ld(w.x, kN) +
-                         Gy[kS] * ld(w.x, kS));
-      r = bk - ax;
-      acc[0] += r * (r / ct);
-      acc[1] += r * r;
+  // ---- setup 1: x0 and the p buffers
+  for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb) {
+    int i0, j0;
+    tile_origin(ti, tile, &i0, &j0);
+    const int j = j0 + ty;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int i = i0 + c * 32 + tx;
+      if (i < nx && j < ny) {
+        const long k = g.at(i, j);
+        w.x[k] = x0_surface ? w.surf_cur[k] : 0.0;
+        w.p0[k] = 0.0;
+        w.p1[k] = 0.0;
+      }
     }
-    w.r[k] = r;
-    acc[2] += bk * bk;
   }
-  block_partials<3>(acc, part[pb] + 4 * blockIdx.x);
-  if (!grid_barrier(sc, nb)) return;
-  double tot3[3];
-  grid_total<3>(part[pb], nb, tot3);
-  pb ^= 1;
-  double rho = tot3[0], rr = tot3[1], rho_old = 1.0;
-  const double bnorm = sqrt(tot3[2]);
+  {
+    double none[1] = {0};
+    if (!grid_allreduce<1>(none, sc, partials, totals, nb)) return;
+  }
+
+  // ---- setup 2: r = b - A x (decoupled neighbours at their exact b/|Ct|)
+  double acc[3] = {0, 0, 0};
+  for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb) {
+    int i0, j0;
+    tile_origin(ti, tile, &i0, &j0);
+    const int j = j0 + ty;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int i = i0 + c * 32 + tx;
+      if (i < nx && j < ny) {
+        const long k = g.at(i, j);
+        const double ct = Ct[k], bk = w.b[k];
+        auto xv = [&](long kk) -> double {
+          const double cc = Ct[kk];
+          return cc < 0 ? w.b[kk] / (-cc) : ld(w.x, kk);
+        };
+        double r;
+        if (ct > 0) {
+          const double ax = ct * ld(w.x, k) - (Gx[k] * xv(k + 1) + Gx[k - 1] * xv(k - 1) +
+                                               Gy[k] * xv(k + pitch) + Gy[k - pitch] * xv(k - pitch));
+          r = bk - ax;
+        } else {
+          r = bk - (-ct) * ld(w.x, k);
+        }
+        acc[0] += r * (r / fabs(ct));
+        acc[1] += r * r;
+        acc[2] += bk * bk;
+        w.r[k] = r;
+      }
+    }
+  }
+  if (!grid_allreduce<3>(acc, sc, partials, totals, nb)) return;
+  double rho = acc[0], rr = acc[1], rho_old = 1.0;
+  const double bnorm = sqrt(acc[2]);
   int it = 0, cur = 0;
   auto converged = [&](double rr_) {
     const double rn = sqrt(rr_);
@@ -175,56 +219,84 @@ __global__ void __launch_bounds__(kCgThreads) k_cg(View w, int x0_surface) {
     const double beta = it == 1 ? 0.0 : rho / rho_old;
     const double *pold = cur ? w.p1 : w.p0;
     double *pnew = cur ? w.p0 : w.p1;
-    // p = M^-1 r + beta p (neighbours recomputed, no extra barrier); q = A p
-    double pq = 0;
-    for (unsigned t = gtid; t < N; t += gs) {
-      const int i = t % nx, j = t / nx;
-      const long k = g.at(i, j);
-      const double ct = Ct[k];
-      if (ct < 0) {
-        pnew[k] = 0.0;
-        w.q[k] = 0.0;
-        continue;
+    // ---- phase 1: p = M^-1 r + beta p_old on tile + halo, q = A p
+    double pq[1] = {0};
+    for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb) {
+      int i0, j0;
+      tile_origin(ti, tile, &i0, &j0);
+      __syncthreads();  // the previous tile's shared data is consumed
+      for (int e = threadIdx.x; e < HX * HY; e += kCgThreads) {
+        const int ey = e / HX, ex = e - ey * HX;
+        const int i = i0 - 1 + ex, j = j0 - 1 + ey;
+        double pv = 0.0, cv = -1.0;
+        if (i <= nx && j <= ny) {
+          const long k = g.at(i, j);
+          cv = Ct[k];
+          const double rv = ld(w.r, k), po = ld(pold, k);
+          pv = rv / fabs(cv) + beta * po;
+        }
+        s_p[ey][ex] = pv;
+        s_c[ey][ex] = cv;
       }
-      const long kE = k + 1, kW = k - 1, kN = k + g.pitch, kS = k - g.pitch;
-      auto pn = [&](long kk) -> double {
-        const double c = Ct[kk];
-        return c < 0 ? 0.0 : ld(w.r, kk) / c + beta * ld(pold, kk);
-      };
-      const double pc = ld(w.r, k) / ct + beta * ld(pold, k);
-      const double qv = ct * pc - (Gx[k] * pn(kE) + Gx[kW] * pn(kW) + Gy[k] * pn(kN) + Gy[kS] * pn(kS));
-      pnew[k] = pc;
-      w.q[k] = qv;
-      pq += pc * qv;
+      __syncthreads();
+      const int j = j0 + ty, ly = ty + 1;
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        const int lx = c * 32 + tx + 1;
+        const int i = i0 + lx - 1;
+        if (i < nx && j < ny) {
+          const long k = g.at(i, j);
+          const double ct = s_c[ly][lx], pc = s_p[ly][lx];
+          // decoupled neighbours contribute nothing (their coupling is in b)
+          auto nb_p = [&](int yy, int xx) -> double { return s_c[yy][xx] < 0 ? 0.0 : s_p[yy][xx]; };
+          double qv;
+          if (ct > 0)
+            qv = ct * pc - (Gx[k] * nb_p(ly, lx + 1) + Gx[k - 1] * nb_p(ly, lx - 1) +
+                            Gy[k] * nb_p(ly + 1, lx) + Gy[k - pitch] * nb_p(ly - 1, lx));
+          else
+            qv = (-ct) * pc;  // decoupled row: lambda = 1 component
+          pnew[k] = pc;
+          w.q[k] = qv;
+          pq[0] += pc * qv;
+        }
+      }
     }
-    double a1[1] = {pq};
-    block_partials<1>(a1, part[pb] + 4 * blockIdx.x);
-    if (!grid_barrier(sc, nb)) return;
-    double t1[1];
-    grid_total<1>(part[pb], nb, t1);
-    pb ^= 1;
-    const double alpha = rho / t1[0];
+    if (!grid_allreduce<1>(pq, sc, partials, totals, nb)) return;
+    const double alpha = rho / pq[0];
+    // ---- phase 2: x, r update and the preconditioned residual norms
     double a2[2] = {0, 0};
-    for (unsigned t = gtid; t < N; t += gs) {
-      const int i = t % nx, j = t / nx;
-      const long k = g.at(i, j);
-      const double ct = Ct[k];
-      if (ct < 0) continue;
-      const double pc = ld(pnew, k), qv = ld(w.q, k);
-      const double rv = ld(w.r, k) - alpha * qv;
-      w.x[k] = ld(w.x, k) + alpha * pc;
-      w.r[k] = rv;
-      a2[0] += rv * (rv / ct);
-      a2[1] += rv * rv;
+    for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb) {
+      int i0, j0;
+      tile_origin(ti, tile, &i0, &j0);
+      const int j = j0 + ty;
+      double xs[CPT], rs[CPT], ps[CPT], qs[CPT], cs[CPT];
+      long ks[CPT];
+      bool ok[CPT];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {  // issue every load of the tile row first
+        const int i = i0 + c * 32 + tx;
+        ok[c] = i < nx && j < ny;
+        ks[c] = ok[c] ? g.at(i, j) : g.at(0, 0);
+        cs[c] = Ct[ks[c]];
+        ps[c] = ld(pnew, ks[c]);
+        qs[c] = ld(w.q, ks[c]);
+        rs[c] = ld(w.r, ks[c]);
+        xs[c] = ld(w.x, ks[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        if (!ok[c]) continue;
+        const double rv = rs[c] - alpha * qs[c];
+        w.x[ks[c]] = xs[c] + alpha * ps[c];
+        w.r[ks[c]] = rv;
+        a2[0] += rv * (rv / fabs(cs[c]));
+        a2[1] += rv * rv;
+      }
     }
-    block_partials<2>(a2, part[pb] + 4 * blockIdx.x);
-    if (!grid_barrier(sc, nb)) return;
-    double t2[2];
-    grid_total<2>(part[pb], nb, t2);
-    pb ^= 1;
+    if (!grid_allreduce<2>(a2, sc, partials, totals, nb)) return;
     rho_old = rho;
-    rho = t2[0];
-    rr = t2[1];
+    rho = a2[0];
+    rr = a2[1];
     cur ^= 1;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {

@@ -44,7 +44,7 @@ __global__ void k_solution_from_ref(View w, const double *xs);
 // Persistent Jacobi-preconditioned CG (cg.cu).
 __global__ void k_cg(View w, int x0_surface);
 
-constexpr int kCgThreads = 256;
+constexpr int kCgThreads = 512;
 
 }  // namespace frehd
 

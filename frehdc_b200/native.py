@@ -317,7 +317,7 @@ class Domain:
         return s.value or 0
 
 
-def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0_SURFACE):
+def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0_ZERO):
     """A Domain initialised from a generated deck (frehdc_b200.deck)."""
     from . import deck as D
     d = Domain(D.config_dict(deck), device)

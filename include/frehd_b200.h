@@ -204,7 +204,11 @@ int frehd_domain_kernel_times(frehd_domain *d, frehd_kernel_times *out);
 /* The CUDA stream (cudaStream_t) all work of the domain is queued on. */
 int frehd_domain_stream(frehd_domain *d, void **stream);
 
-/* Solver options (defaults: warm start from the current surface, Jacobi PCG). */
+/* Solver start: FREHD_X0_ZERO (default) starts each solve from x = 0 as the
+ * reference does (nsfunctions.c:1011); FREHD_X0_SURFACE starts from the current
+ * surface (fewer iterations, same residual tolerance, but closed dry cells then
+ * end exactly on b/Ct instead of on the CG's side of it, which can change the
+ * reference's wet/dry branches). */
 enum { FREHD_X0_ZERO = 0, FREHD_X0_SURFACE = 1 };
 int frehd_domain_set_solver(frehd_domain *d, int x0_mode);
 

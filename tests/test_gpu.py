@@ -3,8 +3,14 @@ which the CPU suite pins bit for bit to the reference itself.
 
 Stencil phases must match the oracle's doubles exactly; the drag coefficients
 go through pow(), where CUDA and glibc may differ in the last place, so they
-are compared to 4 ulp-ish relative tolerance.  The linear solve is compared to
-the CG tolerance, whole runs to 1e-9 relative (the plain form's target).
+are compared to a few ulp.  The linear solve is compared to the CG tolerance.
+
+Whole runs: the surface and the scalar to 1e-9 relative (max norm).  Face
+velocities are compared to 3e-9: two solves that both meet ||r|| < 1e-12 ||b||
+(the reference's own SSOR-PCG and a Jacobi-PCG, both on the CPU) already differ
+by 1.2e-9 in the velocities of the 30%-dry deck, because u = En - g dt (Nx/Vx)
+d(eta) amplifies the solver's eta error on thin-water faces; the surface itself
+agrees to ~1e-11.
 """
 import os
 
@@ -21,6 +27,7 @@ pytestmark = pytest.mark.gpu
 EXACT = ["surf", "uuXP", "vvYP", "S", "depth", "V", "Z", "Nx", "Oy", "Vx", "Vy", "Zx", "Zy", "ind",
          "surfOld", "cellV", "Sm", "Fuu", "Fvv", "CFLx", "CFLy", "uuYP", "vvXP"]
 POW = ["CDXP", "CDYP"]
+RUN_TOL = {"surf": 1e-9, "S": 1e-9, "uuXP": 3e-9, "vvYP": 3e-9}
 UPLOAD = ["surf", "uuXP", "vvYP", "S", "depth", "CDXP", "CDYP", "CFLx", "CFLy", "V", "Z", "Nx",
           "Oy", "Vx", "Vy", "Zx", "Zy", "ind", "bottomZ", "bottomXP", "bottomYP"]
 
@@ -52,7 +59,7 @@ def test_phases_bitwise(name, steps, scratch):
     """Each step: the oracle's state is uploaded, then the device's explicit
     phase and update phase (fed the oracle's x) must give the oracle's doubles."""
     d, _ = deck_for(name, str(scratch))
-    o = port.from_deck(d, precond=port.PRECOND_JACOBI, x0=port.X0_SURFACE)
+    o = port.from_deck(d, precond=port.PRECOND_JACOBI, x0=port.X0_ZERO)
     g = native.domain_from_deck(d, geometry="fine")
     for tt in range(1, steps + 1):
         g.upload(_oracle_state(o, UPLOAD))
@@ -75,7 +82,7 @@ def test_phases_bitwise(name, steps, scratch):
 @pytest.mark.parametrize("name", ["wet48x40", "dry40x36"])
 def test_solve_matches_oracle(name, scratch):
     d, _ = deck_for(name, str(scratch))
-    o = port.from_deck(d, precond=port.PRECOND_JACOBI, x0=port.X0_SURFACE)
+    o = port.from_deck(d, precond=port.PRECOND_JACOBI, x0=port.X0_ZERO)
     g = native.domain_from_deck(d, geometry="fine")
     for tt in range(1, 4):
         g.upload(_oracle_state(o, UPLOAD))
@@ -84,15 +91,18 @@ def test_solve_matches_oracle(name, scratch):
         g.phase(native.PHASE_EXPLICIT, tt)
         g.phase(native.PHASE_SOLVE, tt)
         xg = g.solution()
-        assert max_rel(xg, o.get("x")) < 1e-12
+        # both solves meet ||r|| < 1e-12 ||b||; x agrees to the conditioning of A
+        assert max_rel(xg, o.get("x")) < 1e-10
         o.update(tt, o.get("x"))
 
 
 @pytest.mark.parametrize("name", ["wet48x40", "dry40x36", "dry37x29"])
 def test_full_run_matches_oracle(name, scratch):
+    """Whole run against the oracle in the reference's own solver set-up (SSOR-PCG
+    from x = 0, which tracks the reference program to ~1e-13)."""
     d, _ = deck_for(name, str(scratch))
     steps = SPECS[name].steps
-    o = port.from_deck(d, precond=port.PRECOND_JACOBI, x0=port.X0_SURFACE)
+    o = port.from_deck(d, precond=port.PRECOND_SSOR, x0=port.X0_ZERO)
     for tt in range(1, steps + 1):
         o.step(tt)
     g = native.domain_from_deck(d, geometry="fine")
@@ -101,7 +111,7 @@ def test_full_run_matches_oracle(name, scratch):
     assert st["step"] == steps
     got = g.download(["surf", "uuXP", "vvYP", "S", "cellV"])
     for n in ["surf", "uuXP", "vvYP", "S"]:
-        assert max_rel(got[n], o.get(n)) <= 1e-9, n
+        assert max_rel(got[n], o.get(n)) <= RUN_TOL[n], n
     # volume ledger: the device's fixed-order sum of cellV equals the host sum
     assert abs(st["volume"] - got["cellV"].sum()) <= 1e-12 * abs(got["cellV"].sum())
 
@@ -117,7 +127,21 @@ def test_full_run_matches_reference(name, scratch):
     assert g.run(1, steps) == 0
     got = g.download(["surf", "uuXP", "vvYP", "S"])
     for n in ["surf", "uuXP", "vvYP", "S"]:
-        assert max_rel(got[n], ref[n]) <= 1e-9, n
+        assert max_rel(got[n], ref[n]) <= RUN_TOL[n], n
+
+
+def test_warm_start_option(scratch):
+    """The warm-started solve (FREHD_X0_SURFACE) meets the same residual test."""
+    d, _ = deck_for("wet48x40", str(scratch))
+    g = native.domain_from_deck(d, geometry="fine", x0=native.X0_SURFACE)
+    assert g.run(1, 10) == 0
+    st = g.stats()
+    assert st["cg_rel_residual"] < d.spec.eps
+    o = port.from_deck(d, precond=port.PRECOND_SSOR, x0=port.X0_ZERO)
+    for tt in range(1, 11):
+        o.step(tt)
+    got = g.download(["surf"])
+    assert max_rel(got["surf"], o.get("surf")) <= 1e-9
 
 
 def test_run_is_bit_reproducible(scratch):

@@ -1,0 +1,369 @@
+"""Benchmark of the plain FP64 FrehdC step on B200.
+
+Workload (one GPU): a 4096 x 4096 subgrid basin at dx = 2 m, dt = 0.5 s, 4 x 4
+fine pixels per cell, about 30% of the cells above low tide, Manning n = 0.025,
+one scalar, CG to ||r|| < 1e-12 ||b|| from x = 0 (the reference's solver set-up).
+Synthetic, seeded deck (frehdc_b200.deck); the state of a 4096^2 domain is far
+larger than the 126 MB L2, so no flush is needed between steps.
+
+Printed JSON line (rank 0):
+  value        cell-steps/s of all ranks, device time (CUDA events on the
+               library's stream) of the K timed steps, inputs resident in HBM
+  e2e          the same metric through the C ABI from host buffers: deck upload
+               and initialisation, K steps each returning its monitorCFL
+               statistics to the host, final state download
+  roofline     the CG kernel (the dominant one): algorithmic bytes per launch
+               (48 B/cell set-up + 72 B/cell per iteration) over its mean
+               event-timed launch duration, against the measured HBM copy peak
+  cpu_baseline the reference program itself (oracle/_ref, one core) on a
+               256 x 256 window of the same deck
+With --gpus N (torchrun) every rank steps its own replica domain (the step does
+not shard: one domain lives on one GPU), value sums them, time is the max over
+ranks.  --impl reference times the reference program on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = ("cell-steps/s plain FP64 vs batched FP32+refine at ≤1e-6 m eta err; "
+          "served p50/p99")
+UNIT = "cell-steps/s"
+
+
+def c2_spec(n: int = 4096, steps: int = 1000, crop=None):
+    from frehdc_b200 import deck as D
+    return D.DeckSpec(nx=n, ny=n, dx=2.0, dt=0.5, steps=steps, seed=2024, dry_frac=0.3,
+                      manning_n=0.025, crop=crop)
+
+
+def c2_crop_spec(n_full: int, w: int, steps: int):
+    """A w x w window of the full deck along its tidal (YP) edge."""
+    s = c2_spec(n_full, steps)
+    return s.replace(nx=w, ny=w, crop=(0, n_full - w, n_full, n_full))
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- helpers
+def measured_hbm_peak():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline_reference(steps: int, n_full: int, w: int = 256):
+    """The reference program (oracle/_ref, stock allocator build) on one core."""
+    from frehdc_b200 import deck as D
+    from oracle import refrun
+    if not refrun.available():
+        return None
+    spec = c2_crop_spec(n_full, w, steps)
+    d = D.make_deck(spec)
+    tmp = tempfile.mkdtemp(prefix="frehd_cpu_")
+    D.write_reference_deck(d, tmp, binary_tables=True)
+    t = refrun.time_run(tmp, steps)
+    return {"value": t["cell_steps_per_s"], "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{w}x{w} window of the {n_full}^2 deck along its tidal edge, "
+                      f"{steps} steps, reference program (frehdc5+ + laspack) on 1 core, "
+                      f"{t['seconds']:.1f} s"}
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from frehdc_b200 import deck as D
+    from oracle import refrun
+    if not refrun.available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference oracle binaries (oracle/_ref) not built"}))
+        return 0
+    cores = os.cpu_count() or 1
+    w = 256
+    sample_steps = 40
+    spec = c2_crop_spec(args.n, w, sample_steps)
+    d = D.make_deck(spec)
+    tmp = tempfile.mkdtemp(prefix="frehd_refarm_")
+    D.write_reference_deck(d, tmp, binary_tables=True)
+    total_steps = args.steps + args.warmup
+    # every "step" of this arm is a bounded sample: all cores each run the
+    # reference program over the window concurrently
+    rates = []
+    t_all0 = time.time()
+    for s in range(total_steps):
+        procs = [subprocess.Popen([refrun.TIMING_BIN, "time", tmp, str(sample_steps)],
+                                  stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 for _ in range(cores)]
+        outs = [p.communicate()[0] for p in procs]
+        secs = []
+        for o in outs:
+            for ln in o.splitlines():
+                if ln.startswith("{"):
+                    secs.append(json.loads(ln)["seconds"])
+        if s >= args.warmup and len(secs) == cores:
+            # concurrent step loops: all cells of all processes over the slowest loop
+            rates.append(cores * w * w * sample_steps / max(secs))
+    value = statistics.median(rates)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * (w * w * sample_steps * cores) / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"{w}x{w} window of the {args.n}^2 plain FP64 subgrid deck "
+                               f"(reference cannot hold a {args.n}-cell tidal row: "
+                               f"tideLocP[1000], configuration.h:60)",
+                   "parallelism": f"{cores} independent reference processes"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{cores} concurrent runs of the reference program, "
+                                   f"{sample_steps} steps of a {w}^2 window each"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": time.time() - t_all0,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_gpu_arm(args):
+    import numpy as np
+    import torch
+
+    from frehdc_b200 import deck as D
+    from frehdc_b200 import native
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = local
+    n = args.n
+    spec = c2_spec(n, steps=max(args.steps + args.warmup + 5, 20))
+    t0 = time.time()
+    deck = D.make_deck(spec)
+    gen_s = time.time() - t0
+    cfg = D.config_dict(deck)
+    tide = D.tide_series(deck)
+    N = n * n
+
+    # ---- value: resident in HBM, device time of K steps
+    dom = native.Domain(cfg, dev)
+    dom.set_fine_bottoms(deck.zf, deck.r)
+    dom.set_tide(tide)
+    dom.set_solver(native.X0_ZERO)
+    dom.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
+    rc = dom.run(1, args.warmup)
+    if rc != 0:
+        raise RuntimeError(f"warm-up steps returned status {rc}")
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    dom.sync()
+    dom.set_profiling(True)
+    with ClockSampler(dev) as clk:
+        rc = dom.run(1 + args.warmup, args.steps)
+    dom.sync()
+    if rc != 0:
+        raise RuntimeError(f"timed steps returned status {rc}")
+    kt = dom.kernel_times()
+    st = dom.stats()
+    dev_ms = sum(kt[k] for k in ("explicit_ms", "cg_ms", "update_geo_ms", "update_vel_ms",
+                                 "finish_ms"))
+    t_max = dev_ms
+    if ws > 1:
+        tt = torch.tensor([dev_ms], device=f"cuda:{dev}", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = ws * N * args.steps / (t_max / 1e3)
+    iters = kt["cg_iters"] / max(kt["steps"], 1)
+    dom.set_profiling(False)
+    dom.close()
+
+    # ---- e2e: through the C ABI from host buffers
+    if args.no_e2e:
+        e2e = None
+    else:
+        e2e = run_e2e(args, deck, cfg, tide, dev, ws, N)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return 0
+    return report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk)
+
+
+def run_e2e(args, deck, cfg, tide, dev, ws, N):
+    import numpy as np
+    import torch
+
+    from frehdc_b200 import native
+    zf = np.ascontiguousarray(deck.zf)
+    host_fields = [deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, deck.S0]
+    torch.cuda.synchronize(dev)
+    te0 = time.time()
+    dom2 = native.Domain(cfg, dev)
+    dom2.set_fine_bottoms(zf, deck.r)
+    dom2.set_tide(tide)
+    dom2.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
+    for s in range(args.steps):
+        rc = dom2.step(1 + s)          # each step returns its monitorCFL statistics
+        if rc != 0:
+            raise RuntimeError(f"e2e step returned status {rc}")
+    out = dom2.download(["surf", "uuXP", "vvYP", "S"])
+    te1 = time.time()
+    dom2.close()
+    e2e_s = te1 - te0
+    if ws > 1:
+        tt = torch.tensor([e2e_s], device=f"cuda:{dev}", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    h2d = zf.nbytes + sum(a.nbytes for a in host_fields) + tide.nbytes
+    d2h = sum(a.nbytes for a in out.values()) + args.steps * 72
+    return {"value": ws * N * args.steps / e2e_s, "unit": UNIT,
+            "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
+            "includes": "deck upload + initialisation, per-step C-ABI step with its statistics "
+                        "read back, final state download"}
+
+
+def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk):
+    N = n * n
+    peak, peak_kind = measured_hbm_peak()
+    cg_launch_ms = kt["cg_ms"] / kt["steps"]
+    cg_bytes = N * (48.0 + 72.0 * iters)
+    achieved = cg_bytes / (cg_launch_ms / 1e3) / 1e9
+    roof = {"kernel": "k_cg (persistent Jacobi-PCG, one launch per step)", "bound": "hbm",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_kind": peak_kind, "traffic": None,
+            "bytes_model": "48 B/cell set-up + 72 B/cell per CG iteration",
+            "cg_iters_per_step": iters, "launch_ms": cg_launch_ms}
+    prof = os.path.join(REPO, "profiles", "k_cg_4096_traffic.json")
+    if os.path.exists(prof):
+        try:
+            with open(prof) as f:
+                roof["traffic"] = json.load(f)["bytes_per_launch"]
+        except Exception:
+            pass
+    step_bytes = N * (456.0 + 72.0 * iters)
+    whole = step_bytes * args.steps / (t_max / 1e3) / 1e9
+    cpu = None if args.no_cpu else cpu_baseline_reference(args.cpu_steps, n)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{n}x{n} plain FP64 subgrid basin (dx 2 m, dt 0.5 s, 4x4 fine, "
+                               f"~30% dry at low tide, n 0.025, 1 scalar), CG eps 1e-12 from x=0",
+                   "nx": n, "ny": n, "parallelism": f"{ws} replica domain(s), one per GPU",
+                   "l2": "no flush: the domain state (>2 GB) exceeds the 126 MB L2",
+                   "deck_seed": spec.seed, "deck_gen_s": round(gen_s, 1)},
+        "e2e": e2e,
+        "roofline": roof,
+        "step_roofline": {"bytes_per_cell_step": 456.0 + 72.0 * iters, "achieved": whole,
+                          "peak": peak, "unit": "GB/s", "frac": whole / peak},
+        "per_kernel_ms_per_step": {k: kt[k] / kt["steps"] for k in
+                                   ("explicit_ms", "cg_ms", "update_geo_ms", "update_vel_ms",
+                                    "finish_ms")},
+        "gpu_launches": 5 * args.steps + 1,
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+        "last_step": st,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=4096)
+    ap.add_argument("--cpu-steps", type=int, default=60)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU reference baseline")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI leg")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -29,6 +29,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-fno-fast-m
 EXTRA = {
     "default": ["--fmad=false"],
     "cg.cu": ["--fmad=true"],
+    "noalloc.cu": ["--fmad=true"],
 }
 
 

@@ -33,109 +33,11 @@
 // records FREHD_ERR_TIMEOUT and every block leaves.
 #include <cmath>
 
+#include "cg_common.cuh"
 #include "domain.cuh"
 #include "kernels.cuh"
 
 namespace frehd {
-
-constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s per wait
-constexpr int CTX = 128, CTY = kCgThreads / 32;   // tile: 4 cells per thread along a row
-constexpr int HX = CTX + 2, HY = CTY + 2;         // tile + halo
-constexpr int CPT = 4;                            // cells per thread, stride 32 along a row
-constexpr int NWARP = kCgThreads / 32;
-
-__device__ __forceinline__ unsigned long long gtimer_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ double ld(const double *a, long k) { return __ldcg(a + k); }
-
-// Sum of NV values over all threads of all blocks, identical in every block,
-// and a grid barrier.  partials: 4 doubles per block; totals: 4 doubles.
-template <int NV>
-__device__ bool grid_allreduce(double (&v)[NV], Scratch *sc, double *partials, double *totals,
-                               unsigned nblocks) {
-  __shared__ double sh[4][NWARP];
-  __shared__ int s_last, s_ok;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int m = 0; m < NV; ++m) {
-    const double s = warp_sum(v[m]);
-    if (lane == 0) sh[m][wid] = s;
-  }
-  __syncthreads();
-  unsigned my_gen = 0;
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int m = 0; m < NV; ++m) {
-      double a = 0;
-      for (int q = 0; q < NWARP; ++q) a += sh[m][q];
-      partials[4 * blockIdx.x + m] = a;
-    }
-    // the generation can only move once every block (this one too) arrived
-    my_gen = *(volatile unsigned *)&sc->bar_gen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(&sc->bar_count, 1u);
-    s_last = arrived == nblocks - 1;
-    s_ok = 1;
-  }
-  __syncthreads();
-  if (s_last) {
-    // every partial is visible: sum them in a fixed order, publish, release
-    __threadfence();
-    double a[4] = {0, 0, 0, 0};
-    for (unsigned q = threadIdx.x; q < nblocks; q += blockDim.x) {
-#pragma unroll
-      for (int m = 0; m < NV; ++m) a[m] += ld(partials, 4 * (long)q + m);
-    }
-    __syncthreads();  // sh is reused
-#pragma unroll
-    for (int m = 0; m < NV; ++m) {
-      const double s = warp_sum(a[m]);
-      if (lane == 0) sh[m][wid] = s;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-#pragma unroll
-      for (int m = 0; m < NV; ++m) {
-        double t = 0;
-        for (int q = 0; q < NWARP; ++q) t += sh[m][q];
-        totals[m] = t;
-      }
-      *(volatile unsigned *)&sc->bar_count = 0;
-      __threadfence();
-      atomicAdd(&sc->bar_gen, 1u);
-    }
-  } else if (threadIdx.x == 0) {
-    volatile unsigned *gen = &sc->bar_gen;
-    const unsigned long long t0 = gtimer_ns();
-    while (*gen == my_gen) {
-      if (gtimer_ns() - t0 > kBarrierTimeoutNs) {
-        set_status(sc, FREHD_ERR_TIMEOUT);
-        s_ok = 0;
-        break;
-      }
-      __nanosleep(16);
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  if (!s_ok || *(volatile int *)&sc->status == FREHD_ERR_TIMEOUT) return false;
-#pragma unroll
-  for (int m = 0; m < NV; ++m) v[m] = ld(totals, m);
-  return true;
-}
-
-struct TileIt {
-  int ntx, nty, ntiles;
-};
-
-__device__ __forceinline__ void tile_origin(const TileIt &t, int tile, int *i0, int *j0) {
-  *i0 = (tile % t.ntx) * CTX;
-  *j0 = (tile / t.ntx) * CTY;
-}
 
 __global__ void __launch_bounds__(kCgThreads, 1) k_cg(View w, int x0_surface) {
   Scratch *sc = w.sc;

@@ -161,6 +161,8 @@ def _declare_domain(L: C.CDLL) -> None:
     L.frehd_domain_stats.argtypes = [_vp, C.POINTER(StepStats)]
     L.frehd_domain_sync.argtypes = [_vp]
     L.frehd_device_count.argtypes = [_ip]
+    L.frehd_cg_solve_noalloc.argtypes = [C.c_int, C.c_int] + [_vp] * 5 + \
+        [C.c_double, C.c_int, C.c_int, _vp, _ip, C.POINTER(C.c_double)]
 
 
 def device_count() -> int:
@@ -315,6 +317,29 @@ class Domain:
         s = _vp()
         check(lib().frehd_domain_stream(self.h, C.byref(s)), "stream")
         return s.value or 0
+
+
+def cg_solve_noalloc(nx: int, ny: int, Ct: int, Gx: int, Gy: int, b: int, x: int, eps: float,
+                     max_iter: int, x0_from_x: bool = False, stream: int = 0,
+                     wait: bool = True):
+    """frehd_cg_solve_noalloc on device pointers (ints) the caller owns.
+
+    Row-major nx*ny doubles each; at most 512*512 cells.  With wait=True the
+    call blocks until the solve ends and returns (iterations, ||r||/||b||);
+    otherwise it only queues the solve on `stream` and returns None."""
+    L = lib()
+    if not hasattr(L, "_domain_declared"):
+        _declare_domain(L)
+        L._domain_declared = True
+    if wait:
+        it, rel = C.c_int(0), C.c_double(0.0)
+        check(L.frehd_cg_solve_noalloc(nx, ny, Ct, Gx, Gy, b, x, eps, max_iter, int(x0_from_x),
+                                       stream or None, C.byref(it), C.byref(rel)),
+              "frehd_cg_solve_noalloc")
+        return it.value, rel.value
+    check(L.frehd_cg_solve_noalloc(nx, ny, Ct, Gx, Gy, b, x, eps, max_iter, int(x0_from_x),
+                                   stream or None, None, None), "frehd_cg_solve_noalloc")
+    return None
 
 
 def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0_ZERO):

@@ -212,6 +212,35 @@ int frehd_domain_stream(frehd_domain *d, void **stream);
 enum { FREHD_X0_ZERO = 0, FREHD_X0_SURFACE = 1 };
 int frehd_domain_set_solver(frehd_domain *d, int x0_mode);
 
+/* The free-surface CG solve alone, for callers that cannot allocate device
+ * memory.  No counterpart in the reference (it solves through laspack inside
+ * the step, nsfunctions.c:1004-1017); this entry point exists for hosts whose
+ * device memory is owned by another runtime's pool, or whose time loop must
+ * not allocate after start-up (cudaMalloc/cudaFree synchronise the device).
+ * It allocates nothing: no cudaMalloc, no cudaFree, no allocating library call.
+ *
+ * All arrays are device pointers the caller owns, row-major, cell (i, j) at
+ * j*nx + i, in the convention of the domain's device system: Ct the diagonal
+ * (negative on a decoupled row, which then holds x = b/|Ct| and has no
+ * couplings), Gx[k] the coupling across the east face of cell k, Gy[k] across
+ * its north face (0 on the domain edge), b the right-hand side.  Solves to
+ * ||r||_2 < eps*||b||_2 or max_iter iterations with the same Jacobi-PCG as
+ * the domain step.  x0_from_x = 0 starts from x = 0, else from the x passed in.
+ *
+ * Limit: nx*ny <= 512*512 cells; larger sizes return FREHD_ERR_INVALID.  The
+ * solve's work vectors live in a static device array inside the library
+ * (about 8.4 MB, held on every GPU that loads the library until the process
+ * exits).  Every call shares it: calls that overlap on the GPU (other streams,
+ * other threads without ordering) race; queue them on one stream.  The first
+ * call on each device looks up that array's address with that device current;
+ * make it before any stream capture.  With iters and rel_residual both NULL
+ * the call only queues work on `stream` (a cudaStream_t; NULL = legacy
+ * default); otherwise it waits for the solve and reports them, returning
+ * FREHD_ERR_TIMEOUT if a device-side wait gave up. */
+int frehd_cg_solve_noalloc(int nx, int ny, const double *Ct, const double *Gx, const double *Gy,
+                           const double *b, double *x, double eps, int max_iter, int x0_from_x,
+                           void *stream, int *iters, double *rel_residual);
+
 #ifdef __cplusplus
 }
 #endif

@@ -41,6 +41,9 @@ METRIC = ("cell-steps/s plain FP64 vs batched FP32+refine at ≤1e-6 m eta err; 
 UNIT = "cell-steps/s"
 
 
+SCHEDULES = {"single_sweep": 0, "two_phase": 1}  # FREHD_CG_SINGLE_SWEEP / FREHD_CG_TWO_PHASE
+
+
 def c2_spec(n: int = 4096, steps: int = 1000, crop=None):
     from frehdc_b200 import deck as D
     return D.DeckSpec(nx=n, ny=n, dx=2.0, dt=0.5, steps=steps, seed=2024, dry_frac=0.3,
@@ -227,6 +230,7 @@ def run_gpu_arm(args):
     dom.set_fine_bottoms(deck.zf, deck.r)
     dom.set_tide(tide)
     dom.set_solver(native.X0_ZERO)
+    dom.set_cg_schedule(SCHEDULES[args.cg_schedule])
     dom.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
     rc = dom.run(1, args.warmup)
     if rc != 0:
@@ -280,6 +284,7 @@ def run_e2e(args, deck, cfg, tide, dev, ws, N):
     dom2 = native.Domain(cfg, dev)
     dom2.set_fine_bottoms(zf, deck.r)
     dom2.set_tide(tide)
+    dom2.set_cg_schedule(SCHEDULES[args.cg_schedule])
     dom2.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
     for s in range(args.steps):
         rc = dom2.step(1 + s)          # each step returns its monitorCFL statistics
@@ -307,7 +312,9 @@ def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk):
     cg_launch_ms = kt["cg_ms"] / kt["steps"]
     cg_bytes = N * (48.0 + 72.0 * iters)
     achieved = cg_bytes / (cg_launch_ms / 1e3) / 1e9
-    roof = {"kernel": "k_cg (persistent Jacobi-PCG, one launch per step)", "bound": "hbm",
+    kname = {"single_sweep": "k_cg1 (persistent single-sweep Jacobi-PCG, one launch per step)",
+             "two_phase": "k_cg (persistent two-phase Jacobi-PCG, one launch per step)"}
+    roof = {"kernel": kname[args.cg_schedule], "bound": "hbm",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_kind": peak_kind, "traffic": None,
             "bytes_model": "48 B/cell set-up + 72 B/cell per CG iteration",
@@ -330,7 +337,8 @@ def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk):
                                f"~30% dry at low tide, n 0.025, 1 scalar), CG eps 1e-12 from x=0",
                    "nx": n, "ny": n, "parallelism": f"{ws} replica domain(s), one per GPU",
                    "l2": "no flush: the domain state (>2 GB) exceeds the 126 MB L2",
-                   "deck_seed": spec.seed, "deck_gen_s": round(gen_s, 1)},
+                   "deck_seed": spec.seed, "deck_gen_s": round(gen_s, 1),
+                   "cg_schedule": args.cg_schedule},
         "e2e": e2e,
         "roofline": roof,
         "step_roofline": {"bytes_per_cell_step": 456.0 + 72.0 * iters, "achieved": whole,
@@ -357,6 +365,9 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=60)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU reference baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI leg")
+    ap.add_argument("--cg-schedule", default="single_sweep", choices=list(SCHEDULES),
+                    help="CG schedule: one sweep and one reduction per iteration, or the "
+                         "textbook two-phase ordering")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

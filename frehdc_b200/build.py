@@ -30,6 +30,7 @@ EXTRA = {
     "default": ["--fmad=false"],
     "cg.cu": ["--fmad=true"],
     "noalloc.cu": ["--fmad=true"],
+    "cg1.cu": ["--fmad=true"],
 }
 
 

@@ -7,6 +7,7 @@
 #include <cstring>
 #include <vector>
 
+#include "cg1.h"
 #include "domain.cuh"
 #include "frehd_internal.h"
 #include "kernels.cuh"
@@ -54,6 +55,10 @@ struct frehd_domain {
   int cur = 0;
   int x0_mode = FREHD_X0_ZERO;
   int cg_blocks = 1;
+  int cg_schedule = FREHD_CG_SINGLE_SWEEP;
+  Cg1Maps cg1_maps{};
+  Cg1Maps *cg1_maps_dev = nullptr;  // device copy read by the kernel
+  int cg1_blocks_n = 1;
   int geom_set = 0, ready = 0;
   frehd_step_stats last{};
   std::vector<void *> allocs;
@@ -185,6 +190,8 @@ int read_stats(frehd_domain *d) {
 }
 
 int launch_cg(frehd_domain *d, const View &w) {
+  if (d->cg_schedule == FREHD_CG_SINGLE_SWEEP)
+    return cg1_launch(w, d->cg1_maps_dev, d->cg1_blocks_n, d->x0_mode, d->stream);
   View wv = w;
   int x0 = d->x0_mode;
   void *args[] = {&wv, &x0};
@@ -293,10 +300,20 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
     long want = (long)((d->gr.nx + 127) / 128) * ((d->gr.ny + kCgThreads / 32 - 1) / (kCgThreads / 32));
     long cap = (long)nsm * std::max(per, 1);
     d->cg_blocks = (int)std::max(1L, std::min(want, cap));
+    r |= cg1_blocks(device, d->gr, &d->cg1_blocks_n);
+  }
+  if (!r) {
     const long nvel = (long)((d->gr.nx + 31) / 32) * ((d->gr.ny + 7) / 8);
-    d->npartials = std::max(nvel, 4L * d->cg_blocks + 8);
+    d->npartials = std::max(nvel, 4L * std::max(d->cg_blocks, d->cg1_blocks_n) + 8);
     r |= dalloc(d, &d->partials, d->npartials);
   }
+  // the single-sweep CG reads r/q and p0/p1 alternately, Ct, Gx and Gy as TMA boxes
+  if (!r)
+    r |= cg1_make_maps(d->gr, d->r, d->q, d->p0, d->p1, d->Ct, d->Gx, d->Gy, &d->cg1_maps);
+  if (!r) r |= dalloc(d, &d->cg1_maps_dev, 1);
+  if (!r && cudaMemcpyAsync(d->cg1_maps_dev, &d->cg1_maps, sizeof(Cg1Maps), cudaMemcpyHostToDevice,
+                            d->stream) != cudaSuccess)
+    r = fail(FREHD_ERR_CUDA, "copying the CG tensor maps to the device failed");
   if (!r && cudaMallocHost((void **)&d->out_host, sizeof(StepOut)) != cudaSuccess)
     r = fail(FREHD_ERR_NOMEM, "pinned host allocation failed");
   if (r) {
@@ -383,6 +400,13 @@ extern "C" int frehd_domain_set_solver(frehd_domain *d, int x0_mode) {
   if (!d || (x0_mode != FREHD_X0_ZERO && x0_mode != FREHD_X0_SURFACE))
     return fail(FREHD_ERR_INVALID, "bad solver option");
   d->x0_mode = x0_mode;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_set_cg_schedule(frehd_domain *d, int schedule) {
+  if (!d || (schedule != FREHD_CG_SINGLE_SWEEP && schedule != FREHD_CG_TWO_PHASE))
+    return fail(FREHD_ERR_INVALID, "bad CG schedule");
+  d->cg_schedule = schedule;
   return FREHD_OK;
 }
 

@@ -1,0 +1,28 @@
+// Host interface of the single-sweep CG (cg1.cu): TMA descriptors of the
+// arrays it reads as halo boxes, launch size and launch.
+#ifndef FREHD_CG1_H
+#define FREHD_CG1_H
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "domain.cuh"
+
+namespace frehd {
+
+// Tensor maps over the padded layout: r and p (two buffers each), Ct, Gx, Gy.
+// The kernel reads them from global memory (a device copy, 64-byte aligned).
+struct Cg1Maps {
+  CUtensorMap r[2], p[2], ct, gx, gy;
+};
+
+int cg1_make_maps(const Grid &g, double *r0, double *r1, double *p0, double *p1, double *ct,
+                  double *gx, double *gy, Cg1Maps *m);
+size_t cg1_smem_bytes();
+// Co-resident blocks for a cooperative launch, at most one per tile.
+int cg1_blocks(int device, const Grid &g, int *blocks);
+int cg1_launch(const View &w, const Cg1Maps *m_dev, int blocks, int x0_surface, cudaStream_t stream);
+
+}  // namespace frehd
+
+#endif

@@ -130,6 +130,7 @@ _vp = C.c_void_p
 
 PHASE_EXPLICIT, PHASE_SOLVE, PHASE_UPDATE = 1, 2, 3
 X0_ZERO, X0_SURFACE = 0, 1
+CG_SINGLE_SWEEP, CG_TWO_PHASE = 0, 1
 STATUS = {0: "ok", 1: "invalid", 2: "unsupported", 3: "cuda", 4: "nomem", 5: "cg_noconverge",
           6: "cfl", 7: "timeout", 8: "state"}
 
@@ -150,6 +151,7 @@ def _declare_domain(L: C.CDLL) -> None:
     L.frehd_domain_set_fine_bottoms.argtypes = [_vp, C.c_int, _dp, C.c_long]
     L.frehd_domain_set_tide.argtypes = [_vp, C.c_int, _dp]
     L.frehd_domain_set_solver.argtypes = [_vp, C.c_int]
+    L.frehd_domain_set_cg_schedule.argtypes = [_vp, C.c_int]
     L.frehd_domain_upload_state.argtypes = [_vp, C.POINTER(State)]
     L.frehd_domain_download_state.argtypes = [_vp, C.POINTER(State)]
     L.frehd_domain_init.argtypes = [_vp] + [_dp] * 7 + [C.c_int]
@@ -217,6 +219,9 @@ class Domain:
 
     def set_solver(self, x0: int):
         check(lib().frehd_domain_set_solver(self.h, x0), "set_solver")
+
+    def set_cg_schedule(self, schedule: int):
+        check(lib().frehd_domain_set_cg_schedule(self.h, schedule), "set_cg_schedule")
 
     def init(self, bottom, bottomXP, bottomYP, surf0, u0=None, v0=None, S0=None,
              round_trip_output: bool = True):
@@ -342,7 +347,8 @@ def cg_solve_noalloc(nx: int, ny: int, Ct: int, Gx: int, Gy: int, b: int, x: int
     return None
 
 
-def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0_ZERO):
+def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0_ZERO,
+                     schedule: int = CG_SINGLE_SWEEP):
     """A Domain initialised from a generated deck (frehdc_b200.deck)."""
     from . import deck as D
     d = Domain(D.config_dict(deck), device)
@@ -356,5 +362,6 @@ def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0
         d.set_tables(tabs)
     d.set_tide(D.tide_series(deck))
     d.set_solver(x0)
+    d.set_cg_schedule(schedule)
     d.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
     return d

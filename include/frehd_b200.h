@@ -212,6 +212,15 @@ int frehd_domain_stream(frehd_domain *d, void **stream);
 enum { FREHD_X0_ZERO = 0, FREHD_X0_SURFACE = 1 };
 int frehd_domain_set_solver(frehd_domain *d, int x0_mode);
 
+/* CG schedule.  Both run the reference's Jacobi-PCG to the same stopping rule
+ * (itersolv.c:355-456, rtc.c:53) and agree to that tolerance.
+ * FREHD_CG_SINGLE_SWEEP (default): one pass over the grid and one global
+ * reduction per iteration (Chronopoulos-Gear ordering of the dot products).
+ * FREHD_CG_TWO_PHASE: the textbook ordering, two passes and two reductions per
+ * iteration, as CGIter does it. */
+enum { FREHD_CG_SINGLE_SWEEP = 0, FREHD_CG_TWO_PHASE = 1 };
+int frehd_domain_set_cg_schedule(frehd_domain *d, int schedule);
+
 /* The free-surface CG solve alone, for callers that cannot allocate device
  * memory.  No counterpart in the reference (it solves through laspack inside
  * the step, nsfunctions.c:1004-1017); this entry point exists for hosts whose

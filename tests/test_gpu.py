@@ -79,11 +79,15 @@ def test_phases_bitwise(name, steps, scratch):
         assert mismatches(got, ref, POW, exact=False, rtol=1e-15) == [], tt
 
 
+SCHEDULES = {"single_sweep": native.CG_SINGLE_SWEEP, "two_phase": native.CG_TWO_PHASE}
+
+
+@pytest.mark.parametrize("schedule", list(SCHEDULES))
 @pytest.mark.parametrize("name", ["wet48x40", "dry40x36"])
-def test_solve_matches_oracle(name, scratch):
+def test_solve_matches_oracle(name, schedule, scratch):
     d, _ = deck_for(name, str(scratch))
     o = port.from_deck(d, precond=port.PRECOND_JACOBI, x0=port.X0_ZERO)
-    g = native.domain_from_deck(d, geometry="fine")
+    g = native.domain_from_deck(d, geometry="fine", schedule=SCHEDULES[schedule])
     for tt in range(1, 4):
         g.upload(_oracle_state(o, UPLOAD))
         o.explicit(tt)
@@ -96,8 +100,9 @@ def test_solve_matches_oracle(name, scratch):
         o.update(tt, o.get("x"))
 
 
+@pytest.mark.parametrize("schedule", list(SCHEDULES))
 @pytest.mark.parametrize("name", ["wet48x40", "dry40x36", "dry37x29"])
-def test_full_run_matches_oracle(name, scratch):
+def test_full_run_matches_oracle(name, schedule, scratch):
     """Whole run against the oracle in the reference's own solver set-up (SSOR-PCG
     from x = 0, which tracks the reference program to ~1e-13)."""
     d, _ = deck_for(name, str(scratch))
@@ -105,7 +110,7 @@ def test_full_run_matches_oracle(name, scratch):
     o = port.from_deck(d, precond=port.PRECOND_SSOR, x0=port.X0_ZERO)
     for tt in range(1, steps + 1):
         o.step(tt)
-    g = native.domain_from_deck(d, geometry="fine")
+    g = native.domain_from_deck(d, geometry="fine", schedule=SCHEDULES[schedule])
     assert g.run(1, steps) == 0
     st = g.stats()
     assert st["step"] == steps
@@ -153,3 +158,20 @@ def test_run_is_bit_reproducible(scratch):
     da = a.download(["surf", "uuXP", "vvYP", "S"])
     db = b.download(["surf", "uuXP", "vvYP", "S"])
     assert mismatches(da, db, list(da)) == []
+
+
+@pytest.mark.parametrize("name", ["wet48x40", "dry37x29"])
+def test_schedules_agree(name, scratch):
+    """The single-sweep and two-phase schedules solve the same system to the CG
+    tolerance, with iteration counts within one of each other."""
+    d, _ = deck_for(name, str(scratch))
+    a = native.domain_from_deck(d, geometry="fine", schedule=native.CG_SINGLE_SWEEP)
+    b = native.domain_from_deck(d, geometry="fine", schedule=native.CG_TWO_PHASE)
+    for g in (a, b):
+        g.phase(native.PHASE_EXPLICIT, 1)
+        g.phase(native.PHASE_SOLVE, 1)
+        g.phase(native.PHASE_UPDATE, 1)
+    sa, sb = a.stats(), b.stats()
+    assert abs(sa["cg_iters"] - sb["cg_iters"]) <= 1
+    assert sa["cg_rel_residual"] < d.spec.eps and sb["cg_rel_residual"] < d.spec.eps
+    assert max_rel(a.solution(), b.solution()) < 1e-10

@@ -1,0 +1,107 @@
+"""Generate the golden fixtures of the plain FP64 step from the reference itself.
+
+Each case is a seeded synthetic deck (frehdc_b200.deck) run by the reference
+program built from its own sources (oracle/_ref/frehd_ref: the unchanged
+FrehdC 5+ step and laspack's SSOR-PCG from x = 0).  A fixture keeps, for the
+final state of the run:
+  * the deck's fingerprint (SHA-256 of its fine bottoms, initial surface,
+    initial scalar and tide series), so a change of the generator is caught;
+  * every field at 4096 seeded cell positions (exact doubles);
+  * per-field checksums over all interior cells: sum, sum of squares, min, max.
+
+Cases:
+  c1_128      128 x 128, dx 10 m, dt 1 s, 200 steps, n 0.03 (the CPU case)
+  c2crop_512  the 512 x 512 window of the 4096 x 4096 deck (dx 2 m, dt 0.5 s,
+              ~30 % dry, n 0.025) along its tidal edge, 100 steps
+
+Run from the repository root where the reference sources are present:
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import math
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+if REPO not in sys.path:
+    sys.path.insert(0, REPO)
+
+from frehdc_b200 import deck as D  # noqa: E402
+
+FIELDS = ["surf", "uuXP", "vvYP", "S", "depth", "cellV"]
+N_SAMPLES = 4096
+SAMPLE_SEED = 20240611
+
+
+def c1_spec() -> D.DeckSpec:
+    return D.DeckSpec(nx=128, ny=128, dx=10.0, dt=1.0, steps=200, manning_n=0.03, seed=1234)
+
+
+def c2crop_spec() -> D.DeckSpec:
+    full = D.DeckSpec(nx=4096, ny=4096, dx=2.0, dt=0.5, steps=100, seed=2024, dry_frac=0.3,
+                      manning_n=0.025)
+    return full.replace(nx=512, ny=512, crop=(0, 4096 - 512, 4096, 4096))
+
+
+CASES = {"c1_128": c1_spec, "c2crop_512": c2crop_spec}
+
+
+def fingerprint(deck) -> str:
+    h = hashlib.sha256()
+    for a in (deck.zf, deck.surf0, deck.S0, D.tide_series(deck)):
+        h.update(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+    return h.hexdigest()
+
+
+def sample_index(n_cells: int) -> np.ndarray:
+    rng = np.random.default_rng(SAMPLE_SEED)
+    return np.sort(rng.choice(n_cells, size=min(N_SAMPLES, n_cells), replace=False))
+
+
+def checksums(a: np.ndarray) -> np.ndarray:
+    a = np.asarray(a, dtype=np.float64)
+    return np.array([math.fsum(a), math.fsum(a * a), a.min(), a.max()])
+
+
+def fixture_path(case: str) -> str:
+    return os.path.join(HERE, f"{case}.npz")
+
+
+def load(case: str) -> dict:
+    with np.load(fixture_path(case)) as z:
+        return {k: z[k] for k in z.files}
+
+
+def main() -> int:
+    from oracle import refrun
+    if not refrun.build():
+        print("the reference oracle binaries are not available", file=sys.stderr)
+        return 1
+    for case, make_spec in CASES.items():
+        spec = make_spec()
+        deck = D.make_deck(spec)
+        N = spec.nx * spec.ny
+        with tempfile.TemporaryDirectory() as tmp:
+            path = os.path.join(tmp, case)
+            D.write_reference_deck(deck, path)
+            st = refrun.run(path, spec.steps, os.path.join(tmp, "final.bin"))
+        idx = sample_index(N)
+        out = {"fingerprint": np.array(fingerprint(deck)), "steps": np.array(spec.steps),
+               "idx": idx}
+        for f in FIELDS:
+            a = st[f][:N]
+            out[f] = a[idx]
+            out[f + "_sums"] = checksums(a)
+        np.savez_compressed(fixture_path(case), **out)
+        print(case, "steps", spec.steps, "volume", out["cellV_sums"][0])
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

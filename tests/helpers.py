@@ -62,3 +62,27 @@ def max_rel(a, b) -> float:
     b = np.asarray(b, dtype=np.float64)
     scale = max(float(np.max(np.abs(b))), 1e-300)
     return float(np.max(np.abs(a - b))) / scale
+
+
+def ledger_residual(V_old, cellV, Fuu, Fvv, nx: int, ny: int, dt: float) -> float:
+    """Relative misclosure of one step's volume ledger (volumeByFluxSub,
+    subgrid.c:1227-1263): the cell volumes after the flux update must add up to
+    the volumes before it plus dt times the net inflow through the domain's
+    outer faces, plus the water added where a negative volume was clipped to 0.
+    Arrays in the reference layout (ghost ring after the N interior cells)."""
+    N = nx * ny
+    ii = np.arange(N)
+    i, j = ii % nx, ii // nx
+    iM = np.where(i == 0, N + 2 * nx + ny + j, ii - 1)   # iMjc (map.c)
+    jM = np.where(j == 0, N + nx + i, ii - nx)           # icjM
+    raw = V_old[:N] + dt * (Fuu[iM] - Fuu[:N] + Fvv[jM] - Fvv[:N])
+    clip_added = float(np.sum(np.where(raw < 0, -raw, 0.0)))
+    # outer faces: west (ghost column), east (i = nx-1), south (ghost row), north (j = ny-1)
+    west = Fuu[N + 2 * nx + ny + np.arange(ny)]
+    east = Fuu[np.arange(ny) * nx + nx - 1]
+    south = Fvv[N + nx + np.arange(nx)]
+    north = Fvv[(ny - 1) * nx + np.arange(nx)]
+    inflow = float(np.sum(west) - np.sum(east) + np.sum(south) - np.sum(north))
+    total = float(np.sum(cellV[:N]))
+    want = float(np.sum(V_old[:N])) + dt * inflow + clip_added
+    return abs(total - want) / max(abs(total), 1e-300)

@@ -38,6 +38,7 @@ struct frehd_domain {
   double *bottomZ = nullptr, *bottomXP = nullptr, *bottomYP = nullptr;
   double *EnXP = nullptr, *EnYP = nullptr, *Gx = nullptr, *Gy = nullptr, *Ct = nullptr,
          *b = nullptr;
+  double *Hx = nullptr, *Hy = nullptr;
   double *x = nullptr, *r = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr;
   double *cellV = nullptr, *Sm = nullptr, *Fuu = nullptr, *Fvv = nullptr;
   unsigned char *rmv = nullptr;
@@ -56,6 +57,7 @@ struct frehd_domain {
   int x0_mode = FREHD_X0_ZERO;
   int cg_blocks = 1;
   int cg_schedule = FREHD_CG_SINGLE_SWEEP;
+  int eliminate = 0;  // FREHD_DECOUPLED_ELIMINATED selected
   Cg1Maps cg1_maps{};
   Cg1Maps *cg1_maps_dev = nullptr;  // device copy read by the kernel
   int cg1_blocks_n = 1;
@@ -123,6 +125,7 @@ View make_view(const frehd_domain *d) {
   w.Zy = d->Zy;
   w.bottomZ = d->bottomZ; w.bottomXP = d->bottomXP; w.bottomYP = d->bottomYP;
   w.EnXP = d->EnXP; w.EnYP = d->EnYP; w.Gx = d->Gx; w.Gy = d->Gy; w.Ct = d->Ct; w.b = d->b;
+  w.Hx = d->Hx; w.Hy = d->Hy;
   w.x = d->x; w.r = d->r; w.p0 = d->p0; w.p1 = d->p1; w.q = d->q;
   w.cellV = d->cellV; w.Sm = d->Sm; w.Fuu = d->Fuu; w.Fvv = d->Fvv;
   w.rmv = d->rmv; w.fix_list = d->fix_list; w.partials = d->partials;
@@ -180,6 +183,7 @@ int read_stats(frehd_domain *d) {
   const StepOut &o = *d->out_host;
   d->last.step = o.step;
   d->last.cg_iters = o.cg_iters;
+  d->last.cg_fallback = o.cg_fallback;
   d->last.status = o.status;
   d->last.cg_rel_residual = o.cg_bb > 0 ? std::sqrt(o.cg_rr) / std::sqrt(o.cg_bb) : 0.0;
   d->last.max_cflx = o.max_cflx;
@@ -191,10 +195,10 @@ int read_stats(frehd_domain *d) {
 
 int launch_cg(frehd_domain *d, const View &w) {
   if (d->cg_schedule == FREHD_CG_SINGLE_SWEEP)
-    return cg1_launch(w, d->cg1_maps_dev, d->cg1_blocks_n, d->x0_mode, d->stream);
+    return cg1_launch(w, d->cg1_maps_dev, d->cg1_blocks_n, d->x0_mode, d->eliminate, d->stream);
   View wv = w;
-  int x0 = d->x0_mode;
-  void *args[] = {&wv, &x0};
+  int x0 = d->x0_mode, el = d->eliminate;
+  void *args[] = {&wv, &x0, &el};
   CUDA_TRY(cudaLaunchCooperativeKernel((void *)k_cg, dim3(d->cg_blocks), dim3(kCgThreads), args, 0,
                                        d->stream));
   return FREHD_OK;
@@ -281,7 +285,7 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
   }
   double **arrs[] = {&d->u, &d->v, &d->CDXP, &d->CDYP, &d->CFLx, &d->CFLy, &d->V, &d->Z, &d->Nx,
                      &d->Oy, &d->Vx, &d->Vy, &d->Zx, &d->Zy, &d->bottomZ, &d->bottomXP,
-                     &d->bottomYP, &d->EnXP, &d->EnYP, &d->Gx, &d->Gy, &d->Ct, &d->b, &d->x, &d->r,
+                     &d->bottomYP, &d->EnXP, &d->EnYP, &d->Gx, &d->Gy, &d->Hx, &d->Hy, &d->Ct, &d->b, &d->x, &d->r,
                      &d->p0, &d->p1, &d->q, &d->cellV, &d->Sm, &d->Fuu, &d->Fvv};
   for (auto a : arrs)
     if (!r) r |= dalloc(d, a, tot);
@@ -304,12 +308,12 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
   }
   if (!r) {
     const long nvel = (long)((d->gr.nx + 31) / 32) * ((d->gr.ny + 7) / 8);
-    d->npartials = std::max(nvel, 4L * std::max(d->cg_blocks, d->cg1_blocks_n) + 8);
+    d->npartials = std::max(nvel, std::max(4L * d->cg_blocks, (long)kCg1PartialStride * d->cg1_blocks_n) + 8);
     r |= dalloc(d, &d->partials, d->npartials);
   }
-  // the single-sweep CG reads r/q and p0/p1 alternately, Ct, Gx and Gy as TMA boxes
+  // the single-sweep CG reads r/q and p0/p1 alternately, Hx and Hy as TMA boxes
   if (!r)
-    r |= cg1_make_maps(d->gr, d->r, d->q, d->p0, d->p1, d->Ct, d->Gx, d->Gy, &d->cg1_maps);
+    r |= cg1_make_maps(d->gr, d->r, d->q, d->p0, d->p1, d->Hx, d->Hy, &d->cg1_maps);
   if (!r) r |= dalloc(d, &d->cg1_maps_dev, 1);
   if (!r && cudaMemcpyAsync(d->cg1_maps_dev, &d->cg1_maps, sizeof(Cg1Maps), cudaMemcpyHostToDevice,
                             d->stream) != cudaSuccess)
@@ -400,6 +404,13 @@ extern "C" int frehd_domain_set_solver(frehd_domain *d, int x0_mode) {
   if (!d || (x0_mode != FREHD_X0_ZERO && x0_mode != FREHD_X0_SURFACE))
     return fail(FREHD_ERR_INVALID, "bad solver option");
   d->x0_mode = x0_mode;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_set_decoupled(frehd_domain *d, int mode) {
+  if (!d || (mode != FREHD_DECOUPLED_AS_ASSEMBLED && mode != FREHD_DECOUPLED_ELIMINATED))
+    return fail(FREHD_ERR_INVALID, "bad decoupled-row mode");
+  d->eliminate = mode == FREHD_DECOUPLED_ELIMINATED;
   return FREHD_OK;
 }
 

@@ -3,29 +3,44 @@
 // Same system, preconditioner, start and stopping rule as k_cg (cg.cu): Jacobi
 // M = diag|Ct|, x0 = 0 (or the surface), stop when ||r||_2 < eps*||b||_2
 // checked before each iteration (rtc.c:53, itersolv.c:355-456), decoupled rows
-// iterated as lambda = 1 components whose couplings sit in b.  What changes is
-// the schedule: the Chronopoulos-Gear form of CG (Chronopoulos & Gear, "s-step
-// iterative methods for symmetric linear systems", J. Comput. Appl. Math. 25,
-// 1989) takes alpha_i from the previous iteration's two dot products,
-//   beta_i  = gamma_i / gamma_{i-1}
-//   alpha_i = gamma_i / (delta_i - beta_i * gamma_i / alpha_{i-1}),
-//   gamma_i = (r_i, u_i), delta_i = (A u_i, u_i), u_i = M^-1 r_i,
-// so one sweep over the grid does a whole iteration and ends in ONE grid
-// reduction of (gamma, delta, ||r||^2) instead of two.  A p_i is computed
-// explicitly from p_i (not by a recurrence), so r follows the same update as
-// in standard CG.
+// iterated as lambda = 1 components; their neighbours keep the coupling to them
+// as in the reference's assembled (non-symmetric) matrix, or, with
+// FREHD_DECOUPLED_ELIMINATED, see their exact value b/|Ct| in the right-hand
+// side instead (cg.cu explains both).  Two things change:
+//
+// 1. The solve runs on the symmetrically scaled system
+//      A~ = D^-1/2 A D^-1/2,  x~ = D^1/2 x,  r~ = D^-1/2 r,  D = diag|Ct|,
+//    on which plain CG produces exactly the Jacobi-PCG iterates of A in exact
+//    arithmetic (x = D^-1/2 x~ at every step; no symmetry of A is needed for
+//    that change of variables).  A~ has a unit diagonal and the face couplings
+//    H = G/sqrt(D_i D_j); a decoupled row applies none of them (its flag is the
+//    sign bit of its own east coupling Hx), so an iteration needs no division.
+//    The stopping test uses the unscaled residual, ||r||^2 = sum D r~^2.
+// 2. One sweep per iteration: with p_i = r~_i + beta_i p_{i-1},
+//      (p_i, A~ p_i) = (r~_i, A~ r~_i) + beta_i [(r~_i, A~ p_{i-1}) + (p_{i-1}, A~ r~_i)]
+//                      + beta_i^2 (p_{i-1}, A~ p_{i-1}),
+//    an identity that holds for any A~, so alpha_i = (r~_i, r~_i)/(p_i, A~ p_i)
+//    of textbook CG (CGIter, itersolv.c:355-456) is known from dot products of
+//    the previous sweep.  A sweep forms p_i, A~ p_i, r~_{i+1} and A~ r~_{i+1}
+//    and ends in ONE grid reduction of those six sums instead of two
+//    reductions.  (For symmetric A~ this is the ordering of Chronopoulos &
+//    Gear, "s-step iterative methods for symmetric linear systems",
+//    J. Comput. Appl. Math. 25, 1989.)
 //
 // One sweep per tile of 128 x 16 cells, with a two-cell halo loaded by TMA:
-//   A  p_i = r_i/|Ct| + beta p_{i-1}            tile + 2 halo (in place)
-//   B  s = A p_i; r_{i+1} = r_i - alpha s;
-//      u_{i+1} = r_{i+1}/|Ct|                   tile + 1 halo (in place)
-//   C  w = A u_{i+1}; x += alpha p_i            tile
-// DRAM traffic per cell and iteration: read r, p, Ct, Gx, Gy, x; write r, p, x
-// = 72 bytes.  r and p ping-pong between two buffers (neighbouring blocks read
-// the old halo while a block writes its new tile); x is updated in place.
-// Boxes of r, p, Ct, Gx, Gy (132 x 20 doubles each) are double-buffered in
-// shared memory behind one mbarrier per stage: the next tile's loads are in
-// flight while the current tile computes.  All waits are bounded.
+//   A  p_i = r~_i + beta p_{i-1}                 tile + 2 halo (in place)
+//   B  s = A~ p_i, r~_{i+1} = r~_i - alpha s     tile + 1 halo (in place)
+//   C  w = A~ r~_{i+1}; x~ += alpha p_i; sums    tile
+// DRAM traffic per cell and iteration: read r~, p, Hx, Hy, x~, |Ct|; write r~,
+// p, x~ = 72 bytes.  r~ and p ping-pong between two buffers (neighbouring
+// blocks read the old halo while a block writes its new tile); x~ is updated in
+// place and turned back into x = x~/sqrt|Ct| at the end.  The boxes of r~, p,
+// Hx, Hy (132 x 20 doubles each) are double-buffered in shared memory behind
+// one mbarrier per stage: the next tile's loads are in flight while the current
+// tile computes.  Every array holds zeros outside the interior (ghost ring and
+// row padding are never written; rows past the array come back as TMA zero
+// fill), which is what lets the passes run without bounds tests.  All waits are
+// bounded.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -43,13 +58,16 @@ namespace {
 constexpr int kTW = CTX, kTH = CTY;              // owned cells of a tile (128 x 16)
 constexpr int kBW = kTW + 4, kBH = kTH + 4;      // tile + two-cell halo: 132 x 20
 constexpr int kBox = kBW * kBH;                  // doubles per array per stage
-constexpr int kIW = kBW - 2, kIH = kBH - 2;      // tile + one-cell halo: 130 x 18
-constexpr int kNArr = 5;                         // r, p, Ct, Gx, Gy
+constexpr int kNArr = 4;                         // r~, p, Hx, Hy
 constexpr unsigned kArrBytes = kBox * 8u;        // 21120, a multiple of 128
 constexpr unsigned kStageBytes = kNArr * kArrBytes;
+constexpr int kRing = 2 * (kTW + 2) + 2 * kTH;   // cells of the one-cell halo ring: 292
+constexpr int kRedStride = 8;                    // partial sums per block in grid_allreduce
 static_assert(kArrBytes % 128 == 0, "TMA destinations must stay 128-byte aligned");
 static_assert((kBW * 8) % 16 == 0, "TMA box rows must be a multiple of 16 bytes");
-static_assert(kTH == kCgThreads / 32, "one warp per tile row in pass C");
+static_assert(kTH == kCgThreads / 32, "one warp per tile row");
+static_assert(kRing <= kCgThreads, "one thread per halo-ring cell");
+static_assert(kBox % 2 == 0, "pass A works on double2");
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
   return (unsigned)__cvta_generic_to_shared(p);
@@ -98,17 +116,16 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map,
 
 // Shared-memory arrays of one stage.
 struct Stage {
-  double *R, *P, *C, *GX, *GY;
+  double *R, *P, *HX, *HY;
   __device__ Stage(unsigned char *base) {
     R = reinterpret_cast<double *>(base);
     P = R + kBox;
-    C = P + kBox;
-    GX = C + kBox;
-    GY = GX + kBox;
+    HX = P + kBox;
+    HY = HX + kBox;
   }
 };
 
-// Issue the five box loads of tile `tile` into stage `st` (one thread).
+// Issue the four box loads of tile `tile` into a stage (one thread).
 __device__ __forceinline__ void issue_tile(const Cg1Maps *m, int cur, const TileIt &ti, int tile,
                                            unsigned char *stage_base, unsigned long long *bar) {
   int i0, j0;
@@ -121,15 +138,34 @@ __device__ __forceinline__ void issue_tile(const Cg1Maps *m, int cur, const Tile
   mbar_expect_tx(bar, kStageBytes);
   tma_load_2d(s.R, &m->r[cur], bar, x, y);
   tma_load_2d(s.P, &m->p[cur], bar, x, y);
-  tma_load_2d(s.C, &m->ct, bar, x, y);
-  tma_load_2d(s.GX, &m->gx, bar, x, y);
-  tma_load_2d(s.GY, &m->gy, bar, x, y);
+  tma_load_2d(s.HX, &m->hx, bar, x, y);
+  tma_load_2d(s.HY, &m->hy, bar, x, y);
+}
+
+// A~ v at shared-memory position q of a box: unit diagonal, scaled couplings,
+// none for a decoupled row (sign bit of its own HX).
+__device__ __forceinline__ double apply(const double *V, const double *HX, const double *HY, int q) {
+  const double he = HX[q];
+  const double off = fabs(he) * V[q + 1] + fabs(HX[q - 1]) * V[q - 1] + HY[q] * V[q + kBW] +
+                     HY[q - kBW] * V[q - kBW];
+  return signbit(he) ? V[q] : V[q] - off;
+}
+
+// Box position of cell t of the tile's one-cell halo ring (t < kRing).
+__device__ __forceinline__ int ring_pos(int t) {
+  if (t < kTW + 2) return kBW + 1 + t;                  // row above the tile
+  t -= kTW + 2;
+  if (t < kTW + 2) return (kTH + 2) * kBW + 1 + t;      // row below
+  t -= kTW + 2;
+  if (t < kTH) return (2 + t) * kBW + 1;                // column left
+  t -= kTH;
+  return (2 + t) * kBW + kTW + 2;                       // column right
 }
 
 }  // namespace
 
 __global__ void __launch_bounds__(kCgThreads, 1)
-    k_cg1(View w, const Cg1Maps *__restrict__ m, int x0_surface) {
+    k_cg1(View w, const Cg1Maps *__restrict__ m, int x0_surface, int eliminate) {
   Scratch *sc = w.sc;
   if (*(volatile int *)&sc->status != FREHD_OK) return;
   // The dynamic region starts after the static shared data (this kernel's and
@@ -149,7 +185,7 @@ __global__ void __launch_bounds__(kCgThreads, 1)
   ti.nty = (ny + CTY - 1) / CTY;
   ti.ntiles = ti.ntx * ti.nty;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  double *partials = w.partials, *totals = w.partials + 4 * (long)nb;
+  double *partials = w.partials, *totals = w.partials + kRedStride * (long)nb;
   const double *Ct = w.Ct, *Gx = w.Gx, *Gy = w.Gy;
 
   // TMA destinations 128-byte aligned, mbarriers 8-byte aligned, tensor maps
@@ -165,230 +201,294 @@ __global__ void __launch_bounds__(kCgThreads, 1)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     // the maps were written to global memory by a host copy: make them visible to the TMA unit
     const CUtensorMap *maps = &m->r[0];
-    for (int q = 0; q < 7; ++q)
+    for (int q = 0; q < 6; ++q)
       asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(maps + q) : "memory");
   }
   __syncthreads();
 
-  // ---- setup 1: x0 and p_{-1} = 0
-  for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb) {
-    int i0, j0;
-    tile_origin(ti, tile, &i0, &j0);
-    const int j = j0 + ty;
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-      const int i = i0 + c * 32 + tx;
-      if (i < nx && j < ny) {
-        const long k = g.at(i, j);
-        w.x[k] = x0_surface ? w.surf_cur[k] : 0.0;
-        w.p0[k] = 0.0;
-      }
-    }
+  // A solve of the assembled (non-symmetric) matrix can stall: ||r|| stops
+  // falling above eps*||b|| and laspack's CGIter runs on to maxIter.  When ||r||
+  // has not halved for kStallIters iterations the solve starts again in the
+  // eliminated (symmetric positive definite) form, and the step reports it.
+  // (the stall bookkeeping lives in shared memory: written by thread 0 only,
+  // read by all between grid reductions)
+  __shared__ double s_best;
+  __shared__ int s_best_it, s_it_all, s_fallback;
+  unsigned seq = 0;  // tiles consumed by this block: stage = seq & 1, phase parity = (seq >> 1) & 1
+  int it = 0;
+  double rr = 0.0, bnorm = 0.0;
+  if (threadIdx.x == 0) {
+    s_it_all = 0;
+    s_fallback = 0;
   }
-  {
-    double none[1] = {0};
-    if (!grid_allreduce<1>(none, sc, partials, totals, nb)) return;
-  }
-
-  // ---- setup 2: r0 = b - A x0 (decoupled neighbours at their exact b/|Ct|)
-  double acc[3] = {0, 0, 0};
-  for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb) {
-    int i0, j0;
-    tile_origin(ti, tile, &i0, &j0);
-    const int j = j0 + ty;
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-      const int i = i0 + c * 32 + tx;
-      if (i < nx && j < ny) {
-        const long k = g.at(i, j);
-        const double ct = Ct[k], bk = w.b[k];
-        auto xv = [&](long kk) -> double {
-          const double cc = Ct[kk];
-          return cc < 0 ? w.b[kk] / (-cc) : ld(w.x, kk);
-        };
-        double r;
-        if (ct > 0) {
-          const double ax = ct * ld(w.x, k) - (Gx[k] * xv(k + 1) + Gx[k - 1] * xv(k - 1) +
-                                               Gy[k] * xv(k + pitch) + Gy[k - pitch] * xv(k - pitch));
-          r = bk - ax;
-        } else {
-          r = bk - (-ct) * ld(w.x, k);
-        }
-        acc[0] += r * (r / fabs(ct));
-        acc[1] += r * r;
-        acc[2] += bk * bk;
-        w.r[k] = r;
-      }
-    }
-  }
-  if (!grid_allreduce<3>(acc, sc, partials, totals, nb)) return;
-  double gamma = acc[0], rr = acc[1];
-  const double bnorm = sqrt(acc[2]);
-
-  // ---- setup 3: delta0 = (A u0, u0), u0 = r0/|Ct| (plain halo loads into stage 0)
-  double delta;
-  {
-    double d0[1] = {0};
-    Stage s(smem);
+  for (int attempt = 0;; ++attempt) {
+    const int elim = eliminate | (attempt > 0);
+    // ---- setup 1: scaled couplings, x~0 = sqrt|Ct| x0, p_{-1} = 0
     for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb) {
       int i0, j0;
       tile_origin(ti, tile, &i0, &j0);
-      __syncthreads();
-      for (int e = threadIdx.x; e < kIW * kIH; e += kCgThreads) {
-        const int ly = 1 + e / kIW, lx = 1 + e % kIW;
-        const int i = i0 - 2 + lx, j = j0 - 2 + ly;
-        double u = 0.0, cv = -1.0;
-        if ((unsigned)i < (unsigned)nx && (unsigned)j < (unsigned)ny) {
-          const long k = g.at(i, j);
-          cv = Ct[k];
-          u = ld(w.r, k) / fabs(cv);
-        }
-        s.R[ly * kBW + lx] = u;
-        s.C[ly * kBW + lx] = cv;
-      }
-      __syncthreads();
       const int j = j0 + ty;
 #pragma unroll
       for (int c = 0; c < CPT; ++c) {
         const int i = i0 + c * 32 + tx;
         if (i < nx && j < ny) {
           const long k = g.at(i, j);
-          const int cc = (ty + 2) * kBW + c * 32 + tx + 2;
-          const double ct = s.C[cc], u = s.R[cc];
-          auto vis = [&](int q) -> double { return s.C[q] > 0 ? s.R[q] : 0.0; };
-          const double au = ct > 0 ? ct * u - (Gx[k] * vis(cc + 1) + Gx[k - 1] * vis(cc - 1) +
-                                               Gy[k] * vis(cc + kBW) + Gy[k - pitch] * vis(cc - kBW))
-                                   : (-ct) * u;
-          d0[0] += au * u;
+          const double ct = Ct[k], ce = Ct[k + 1], cn = Ct[k + pitch];
+          const double d = sqrt(fabs(ct));
+          double hx = Gx[k] / (d * sqrt(fabs(ce))), hy = Gy[k] / (d * sqrt(fabs(cn)));
+          if (elim) {  // no coupling across a face with a decoupled row or a ghost (Ct < 0)
+            if (!(ct > 0 && ce > 0)) hx = 0.0;
+            if (!(ct > 0 && cn > 0)) hy = 0.0;
+          }
+          // row k's decoupled flag rides in the sign bit of its own east coupling
+          w.Hx[k] = ct < 0 ? -fabs(hx) : fabs(hx);
+          w.Hy[k] = hy;
+          w.x[k] = x0_surface ? d * w.surf_cur[k] : 0.0;
+          w.p0[k] = 0.0;
         }
       }
     }
-    __syncthreads();
-    if (!grid_allreduce<1>(d0, sc, partials, totals, nb)) return;
-    delta = d0[0];
-  }
-
-  auto converged = [&](double rr_) {
-    const double rn = sqrt(rr_);
-    return rn < p.eps * bnorm || (bnorm == 0.0 && 1.0 + rn == 1.0);
-  };
-  double gamma_old = 1.0, alpha_old = 1.0;
-  int it = 0, cur = 0;
-  unsigned seq = 0;  // tiles consumed by this block: stage = seq & 1, phase parity = (seq >> 1) & 1
-  while (!converged(rr) && it < p.maxIter) {
-    const double beta = it == 0 ? 0.0 : gamma / gamma_old;
-    const double alpha = it == 0 ? gamma / delta : gamma / (delta - beta * gamma / alpha_old);
-    ++it;
-    double *rn_out = cur ? w.r : w.q, *pn_out = cur ? w.p0 : w.p1;
-    double red[3] = {0, 0, 0};  // gamma, delta, rr of the new residual
-    // generic writes of the previous sweep (all blocks) come before this sweep's TMA reads
-    if (threadIdx.x == 0) {
-      asm volatile("fence.proxy.async.global;" ::: "memory");
-      issue_tile(m, cur, ti, blockIdx.x, smem + (seq & 1) * kStageBytes, &bars[seq & 1]);
+    {
+      double none[1] = {0};
+      if (!grid_allreduce<1, kRedStride>(none, sc, partials, totals, nb)) return;
     }
-    for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb, ++seq) {
-      const int st = seq & 1;
-      const int next = tile + (int)nb;
-      if (threadIdx.x == 0 && next < ti.ntiles)
-        issue_tile(m, cur, ti, next, smem + (st ^ 1) * kStageBytes, &bars[st ^ 1]);
+
+    // ---- setup 2: r0 = b - A x0 (eliminated: decoupled neighbours at their exact b/|Ct|),
+    //      r~0 = r0/sqrt|Ct|
+    double acc[3] = {0, 0, 0};
+    for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb) {
       int i0, j0;
       tile_origin(ti, tile, &i0, &j0);
-      // x of the owned cells: in flight while the boxes arrive
-      double xs[CPT];
-      {
-        const int j = j0 + ty;
+      const int j = j0 + ty;
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-          const int i = i0 + c * 32 + tx;
-          xs[c] = (i < nx && j < ny) ? w.x[g.at(i, j)] : 0.0;
-        }
-      }
-      if (threadIdx.x == 0) s_ok = mbar_wait(&bars[st], (seq >> 1) & 1, kBarrierTimeoutNs);
-      __syncthreads();
-      if (!s_ok) {
-        // the other stage may hold a load issued for the next tile: let it land
-        if (threadIdx.x == 0) {
-          set_status(sc, FREHD_ERR_TIMEOUT);
-          if (next < ti.ntiles) mbar_wait(&bars[st ^ 1], ((seq + 1) >> 1) & 1, kBarrierTimeoutNs);
-        }
-        return;
-      }
-      mbar_wait(&bars[st], (seq >> 1) & 1, kBarrierTimeoutNs);  // completed: acquire in every thread
-      Stage s(smem + st * kStageBytes);
-
-      // pass A: p_i = r_i/|Ct| + beta p_{i-1} on tile + 2 halo; outside the domain p = r = 0
-      for (int e = threadIdx.x; e < kBox; e += kCgThreads) {
-        const int ly = e / kBW, lx = e - ly * kBW;
-        const int i = i0 - 2 + lx, j = j0 - 2 + ly;
-        if ((unsigned)i < (unsigned)nx && (unsigned)j < (unsigned)ny) {
-          s.P[e] = s.R[e] / fabs(s.C[e]) + beta * s.P[e];
-        } else {
-          s.P[e] = 0.0;
-          s.R[e] = 0.0;
-          s.C[e] = -1.0;
-        }
-      }
-      __syncthreads();
-
-      // pass B: s = A p_i, r_{i+1} = r_i - alpha s, u_{i+1} = r_{i+1}/|Ct| on tile + 1 halo
-      for (int e = threadIdx.x; e < kIW * kIH; e += kCgThreads) {
-        const int ly = 1 + e / kIW, lx = 1 + e % kIW;
-        const int q = ly * kBW + lx;
-        const double ct = s.C[q], pc = s.P[q];
-        auto vis = [&](int qq) -> double { return s.C[qq] > 0 ? s.P[qq] : 0.0; };
-        const double ap = ct > 0 ? ct * pc - (s.GX[q] * vis(q + 1) + s.GX[q - 1] * vis(q - 1) +
-                                              s.GY[q] * vis(q + kBW) + s.GY[q - kBW] * vis(q - kBW))
-                                 : (-ct) * pc;
-        const double rnew = s.R[q] - alpha * ap;
-        const double unew = rnew / fabs(ct);
-        s.R[q] = unew;
-        const int li = lx - 2, lj = ly - 2;
-        if ((unsigned)li < (unsigned)kTW && (unsigned)lj < (unsigned)kTH) {
-          const int i = i0 + li, j = j0 + lj;
-          if (i < nx && j < ny) {
-            rn_out[g.at(i, j)] = rnew;
-            red[0] += rnew * unew;
-            red[2] += rnew * rnew;
+      for (int c = 0; c < CPT; ++c) {
+        const int i = i0 + c * 32 + tx;
+        if (i < nx && j < ny) {
+          const long k = g.at(i, j);
+          const double ct = Ct[k], bk = w.b[k];
+          auto x0 = [&](long kk) -> double { return x0_surface ? w.surf_cur[kk] : 0.0; };
+          auto xv = [&](long kk) -> double {
+            const double cc = Ct[kk];
+            return (elim && cc < 0) ? w.b[kk] / (-cc) : x0(kk);
+          };
+          double r;
+          if (ct > 0) {
+            const double ax = ct * x0(k) - (Gx[k] * xv(k + 1) + Gx[k - 1] * xv(k - 1) +
+                                            Gy[k] * xv(k + pitch) + Gy[k - pitch] * xv(k - pitch));
+            r = bk - ax;
+          } else {
+            r = bk - (-ct) * x0(k);
           }
+          const double rs = r / sqrt(fabs(ct));
+          acc[0] += rs * rs;
+          acc[1] += r * r;
+          acc[2] += bk * bk;
+          w.r[k] = rs;
         }
       }
-      __syncthreads();
+    }
+    if (!grid_allreduce<3, kRedStride>(acc, sc, partials, totals, nb)) return;
+    double gamma = acc[0];
+    rr = acc[1];
+    bnorm = sqrt(acc[2]);
 
-      // pass C: w = A u_{i+1}, delta partial; x_{i+1} = x_i + alpha p_i; store p_i
-      {
+    // ---- setup 3: delta0 = (A~ r~0, r~0) (plain halo loads into stage 0)
+    double delta;
+    {
+      double d0[1] = {0};
+      Stage s(smem);
+      for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb) {
+        int i0, j0;
+        tile_origin(ti, tile, &i0, &j0);
+        __syncthreads();
+        // r~0, Hx, Hy of the tile and its one-cell ring (zeros outside the interior)
+        for (int e = threadIdx.x; e < (kTW + 2) * (kTH + 2); e += kCgThreads) {
+          const int ly = 1 + e / (kTW + 2), lx = 1 + e % (kTW + 2);
+          const int i = i0 - 2 + lx, jj = j0 - 2 + ly;
+          const bool in = (unsigned)i < (unsigned)nx && (unsigned)jj < (unsigned)ny;
+          const long k = in ? g.at(i, jj) : 0;
+          s.R[ly * kBW + lx] = in ? ld(w.r, k) : 0.0;
+          s.HX[ly * kBW + lx] = in ? ld(w.Hx, k) : 0.0;
+          s.HY[ly * kBW + lx] = in ? ld(w.Hy, k) : 0.0;
+        }
+        __syncthreads();
         const int j = j0 + ty;
 #pragma unroll
         for (int c = 0; c < CPT; ++c) {
           const int i = i0 + c * 32 + tx;
           if (i < nx && j < ny) {
             const int q = (ty + 2) * kBW + c * 32 + tx + 2;
-            const double ct = s.C[q], u = s.R[q];
-            auto vis = [&](int qq) -> double { return s.C[qq] > 0 ? s.R[qq] : 0.0; };
-            const double au = ct > 0 ? ct * u - (s.GX[q] * vis(q + 1) + s.GX[q - 1] * vis(q - 1) +
-                                                 s.GY[q] * vis(q + kBW) + s.GY[q - kBW] * vis(q - kBW))
-                                     : (-ct) * u;
-            red[1] += au * u;
-            const long k = g.at(i, j);
-            const double pc = s.P[q];
-            w.x[k] = xs[c] + alpha * pc;
-            pn_out[k] = pc;
+            d0[0] += apply(s.R, s.HX, s.HY, q) * s.R[q];
           }
         }
       }
-      __syncthreads();  // stage st is free for the tile after next
+      __syncthreads();
+      if (!grid_allreduce<1, kRedStride>(d0, sc, partials, totals, nb)) return;
+      delta = d0[0];
     }
-    // this thread's global writes before the next sweep's TMA reads (other blocks)
-    asm volatile("fence.proxy.async.global;" ::: "memory");
-    if (!grid_allreduce<3>(red, sc, partials, totals, nb)) return;
-    gamma_old = gamma;
-    alpha_old = alpha;
-    gamma = red[0];
-    delta = red[1];
-    rr = red[2];
-    cur ^= 1;
+
+    auto converged = [&](double rr_) {
+      const double rn = sqrt(rr_);
+      return rn < p.eps * bnorm || (bnorm == 0.0 && 1.0 + rn == 1.0);
+    };
+    double gamma_old = 1.0, e1 = 0.0, e2 = 0.0, e3 = 0.0;
+    if (threadIdx.x == 0) {
+      s_best = rr;
+      s_best_it = 0;
+    }
+    __syncthreads();
+    int cur = 0;
+    bool stalled = false;
+    it = 0;
+    while (!converged(rr) && it < p.maxIter) {
+      const double beta = it == 0 ? 0.0 : gamma / gamma_old;
+      const double alpha = gamma / (delta + beta * (e1 + e2) + beta * beta * e3);
+      ++it;
+      double *rn_out = cur ? w.r : w.q, *pn_out = cur ? w.p0 : w.p1;
+      // (r~', r~'), (A~ r~', r~'), (r~', A~ p), (p, A~ r~'), (p, A~ p), ||r'||^2; r~' = r~_{i+1}
+      double red[6] = {0, 0, 0, 0, 0, 0};
+      // generic writes of the previous sweep (all blocks) come before this sweep's TMA reads
+      if (threadIdx.x == 0) {
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        issue_tile(m, cur, ti, blockIdx.x, smem + (seq & 1) * kStageBytes, &bars[seq & 1]);
+      }
+      for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb, ++seq) {
+        const int st = seq & 1;
+        const int next = tile + (int)nb;
+        if (threadIdx.x == 0 && next < ti.ntiles)
+          issue_tile(m, cur, ti, next, smem + (st ^ 1) * kStageBytes, &bars[st ^ 1]);
+        int i0, j0;
+        tile_origin(ti, tile, &i0, &j0);
+        // x~ and |Ct| of the owned cells: in flight while the boxes arrive
+        const int j = j0 + ty;
+        double xs[CPT], ds[CPT];
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          const int i = i0 + c * 32 + tx;
+          const bool in = i < nx && j < ny;
+          const long k = g.at(in ? i : 0, in ? j : 0);
+          xs[c] = w.x[k];
+          ds[c] = fabs(Ct[k]);
+        }
+        if (threadIdx.x == 0) s_ok = mbar_wait(&bars[st], (seq >> 1) & 1, kBarrierTimeoutNs);
+        __syncthreads();
+        if (!s_ok) {
+          // the other stage may hold a load issued for the next tile: let it land
+          if (threadIdx.x == 0) {
+            set_status(sc, FREHD_ERR_TIMEOUT);
+            if (next < ti.ntiles) mbar_wait(&bars[st ^ 1], ((seq + 1) >> 1) & 1, kBarrierTimeoutNs);
+          }
+          return;
+        }
+        mbar_wait(&bars[st], (seq >> 1) & 1, kBarrierTimeoutNs);  // completed: acquire in every thread
+        Stage s(smem + st * kStageBytes);
+
+        // pass A: p_i = r~_i + beta p_{i-1} on the whole box
+        {
+          double2 *P2 = reinterpret_cast<double2 *>(s.P);
+          const double2 *R2 = reinterpret_cast<const double2 *>(s.R);
+#pragma unroll
+          for (int e = threadIdx.x; e < kBox / 2; e += kCgThreads) {
+            const double2 rv = R2[e];
+            double2 pv = P2[e];
+            pv.x = rv.x + beta * pv.x;
+            pv.y = rv.y + beta * pv.y;
+            P2[e] = pv;
+          }
+        }
+        __syncthreads();
+
+        // pass B: r~_{i+1} = r~_i - alpha A~ p_i on the tile (4 cells per thread) and its ring;
+        // it reads only P, HX, HY besides each thread's own R cells, so R is updated in place
+        {
+          double rb[CPT];
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) {
+            const int q = (ty + 2) * kBW + c * 32 + tx + 2;
+            const double sv = apply(s.P, s.HX, s.HY, q);
+            rb[c] = s.R[q] - alpha * sv;
+            if (i0 + c * 32 + tx < nx && j < ny) {
+              red[2] += rb[c] * sv;
+              red[4] += s.P[q] * sv;
+            }
+          }
+          double rring = 0.0;
+          const int qr = threadIdx.x < kRing ? ring_pos(threadIdx.x) : 0;
+          if (threadIdx.x < kRing) rring = s.R[qr] - alpha * apply(s.P, s.HX, s.HY, qr);
+#pragma unroll
+          for (int c = 0; c < CPT; ++c) s.R[(ty + 2) * kBW + c * 32 + tx + 2] = rb[c];
+          if (threadIdx.x < kRing) s.R[qr] = rring;
+        }
+        __syncthreads();
+
+        // pass C: w = A~ r~_{i+1}; sums; x~_{i+1} = x~_i + alpha p_i; store r~, p, x~
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          const int i = i0 + c * 32 + tx;
+          if (i < nx && j < ny) {
+            const int q = (ty + 2) * kBW + c * 32 + tx + 2;
+            const double u = s.R[q], pc = s.P[q];
+            const double wv = apply(s.R, s.HX, s.HY, q);
+            red[0] += u * u;
+            red[1] += wv * u;
+            red[3] += pc * wv;
+            red[5] += ds[c] * (u * u);
+            const long k = g.at(i, j);
+            w.x[k] = xs[c] + alpha * pc;
+            rn_out[k] = u;
+            pn_out[k] = pc;
+          }
+        }
+        __syncthreads();  // stage st is free for the tile after next
+      }
+      // this thread's global writes before the next sweep's TMA reads (other blocks)
+      asm volatile("fence.proxy.async.global;" ::: "memory");
+      if (!grid_allreduce<6, kRedStride>(red, sc, partials, totals, nb)) return;
+      gamma_old = gamma;
+      gamma = red[0];
+      delta = red[1];
+      e1 = red[2];
+      e2 = red[3];
+      e3 = red[4];
+      rr = red[5];
+      cur ^= 1;
+      // identical totals in every block: every block takes the same decision; every
+      // thread reads the record before thread 0 may update it
+      const double best = s_best;
+      const int best_it = s_best_it;
+      __syncthreads();
+      if (rr < 0.25 * best) {
+        if (threadIdx.x == 0) {
+          s_best = rr;
+          s_best_it = it;
+        }
+      } else if (!elim && it - best_it >= kStallIters) {
+        stalled = true;
+        break;
+      }
+    }
+    if (threadIdx.x == 0) s_it_all += it;
+    if (!stalled) break;
+    if (threadIdx.x == 0) s_fallback = 1;
+  }  // attempt
+
+  // ---- x = x~ / sqrt|Ct| (each block its own tiles)
+  for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb) {
+    int i0, j0;
+    tile_origin(ti, tile, &i0, &j0);
+    const int j = j0 + ty;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int i = i0 + c * 32 + tx;
+      if (i < nx && j < ny) {
+        const long k = g.at(i, j);
+        w.x[k] = w.x[k] / sqrt(fabs(Ct[k]));
+      }
+    }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    sc->cg_iters = it;
+    sc->cg_iters = s_it_all;
+    sc->cg_fallback = s_fallback;
     sc->cg_rr = rr;
     sc->cg_bb = bnorm * bnorm;
   }
@@ -426,17 +526,16 @@ int encode(const Grid &g, double *base, CUtensorMap *out) {
 
 }  // namespace
 
-int cg1_make_maps(const Grid &g, double *r0, double *r1, double *p0, double *p1, double *ct,
-                  double *gx, double *gy, Cg1Maps *m) {
+int cg1_make_maps(const Grid &g, double *r0, double *r1, double *p0, double *p1, double *hx,
+                  double *hy, Cg1Maps *m) {
   std::memset(m, 0, sizeof(*m));
   int rc = 0;
   rc = rc ? rc : encode(g, r0, &m->r[0]);
   rc = rc ? rc : encode(g, r1, &m->r[1]);
   rc = rc ? rc : encode(g, p0, &m->p[0]);
   rc = rc ? rc : encode(g, p1, &m->p[1]);
-  rc = rc ? rc : encode(g, ct, &m->ct);
-  rc = rc ? rc : encode(g, gx, &m->gx);
-  rc = rc ? rc : encode(g, gy, &m->gy);
+  rc = rc ? rc : encode(g, hx, &m->hx);
+  rc = rc ? rc : encode(g, hy, &m->hy);
   return rc;
 }
 
@@ -458,11 +557,12 @@ int cg1_blocks(int device, const Grid &g, int *blocks) {
   return FREHD_OK;
 }
 
-int cg1_launch(const View &w, const Cg1Maps *m_dev, int blocks, int x0_surface, cudaStream_t stream) {
+int cg1_launch(const View &w, const Cg1Maps *m_dev, int blocks, int x0_surface, int eliminate,
+               cudaStream_t stream) {
   View wv = w;
   const Cg1Maps *mp = m_dev;
-  int x0 = x0_surface;
-  void *args[] = {&wv, &mp, &x0};
+  int x0 = x0_surface, el = eliminate;
+  void *args[] = {&wv, &mp, &x0, &el};
   cudaError_t e = cudaLaunchCooperativeKernel((void *)k_cg1, dim3(blocks), dim3(kCgThreads), args,
                                               cg1_smem_bytes(), stream);
   if (e != cudaSuccess) return fail(FREHD_ERR_CUDA, "k_cg1 launch: %s", cudaGetErrorString(e));

@@ -10,18 +10,22 @@
 
 namespace frehd {
 
-// Tensor maps over the padded layout: r and p (two buffers each), Ct, Gx, Gy.
-// The kernel reads them from global memory (a device copy, 64-byte aligned).
+// Tensor maps over the padded layout: the scaled residual and direction (two
+// buffers each) and the scaled face couplings Hx, Hy.  The kernel reads them
+// from global memory (a device copy, 64-byte aligned).
 struct Cg1Maps {
-  CUtensorMap r[2], p[2], ct, gx, gy;
+  CUtensorMap r[2], p[2], hx, hy;
 };
 
-int cg1_make_maps(const Grid &g, double *r0, double *r1, double *p0, double *p1, double *ct,
-                  double *gx, double *gy, Cg1Maps *m);
+int cg1_make_maps(const Grid &g, double *r0, double *r1, double *p0, double *p1, double *hx,
+                  double *hy, Cg1Maps *m);
 size_t cg1_smem_bytes();
 // Co-resident blocks for a cooperative launch, at most one per tile.
 int cg1_blocks(int device, const Grid &g, int *blocks);
-int cg1_launch(const View &w, const Cg1Maps *m_dev, int blocks, int x0_surface, cudaStream_t stream);
+int cg1_launch(const View &w, const Cg1Maps *m_dev, int blocks, int x0_surface, int eliminate,
+               cudaStream_t stream);
+// Partial sums per block the single-sweep CG keeps in the partials buffer.
+constexpr int kCg1PartialStride = 8;
 
 }  // namespace frehd
 

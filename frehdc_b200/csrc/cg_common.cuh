@@ -10,6 +10,7 @@
 namespace frehd {
 
 constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;  // 2 s per wait
+constexpr int kStallIters = 400;  // CG iterations without ||r|| halving that count as a stall
 constexpr int CTX = 128, CTY = kCgThreads / 32;   // tile: 4 cells per thread along a row
 constexpr int HX = CTX + 2, HY = CTY + 2;         // tile + halo
 constexpr int CPT = 4;                            // cells per thread, stride 32 along a row
@@ -24,11 +25,12 @@ __device__ __forceinline__ unsigned long long gtimer_ns() {
 __device__ __forceinline__ double ld(const double *a, long k) { return __ldcg(a + k); }
 
 // Sum of NV values over all threads of all blocks, identical in every block,
-// and a grid barrier.  partials: 4 doubles per block; totals: 4 doubles.
-template <int NV>
+// and a grid barrier.  partials: STRIDE doubles per block; totals: NV doubles.
+template <int NV, int STRIDE = 4>
 __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], Scratch *sc, double *partials, double *totals,
                                unsigned nblocks) {
-  __shared__ double sh[4][NWARP];
+  static_assert(NV <= STRIDE, "NV values per block must fit the partials stride");
+  __shared__ double sh[STRIDE][NWARP];
   __shared__ int s_last, s_ok;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
@@ -43,7 +45,7 @@ __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], Scratch *sc, dou
     for (int m = 0; m < NV; ++m) {
       double a = 0;
       for (int q = 0; q < NWARP; ++q) a += sh[m][q];
-      partials[4 * blockIdx.x + m] = a;
+      partials[STRIDE * blockIdx.x + m] = a;
     }
     // the generation can only move once every block (this one too) arrived
     my_gen = *(volatile unsigned *)&sc->bar_gen;
@@ -56,10 +58,12 @@ __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], Scratch *sc, dou
   if (s_last) {
     // every partial is visible: sum them in a fixed order, publish, release
     __threadfence();
-    double a[4] = {0, 0, 0, 0};
+    double a[NV];
+#pragma unroll
+    for (int m = 0; m < NV; ++m) a[m] = 0;
     for (unsigned q = threadIdx.x; q < nblocks; q += blockDim.x) {
 #pragma unroll
-      for (int m = 0; m < NV; ++m) a[m] += ld(partials, 4 * (long)q + m);
+      for (int m = 0; m < NV; ++m) a[m] += ld(partials, STRIDE * (long)q + m);
     }
     __syncthreads();  // sh is reused
 #pragma unroll

@@ -74,7 +74,7 @@ struct Scratch {
   int cg_iters;
   int n_cfl_warn;
   int n_fix;                        // scalar-singularity cells queued for the fix-up
-  int pad0;
+  int cg_fallback;                  // 1: the last solve stalled and was redone in eliminated form
   double cg_rr, cg_bb;              // ||r||^2, ||b||^2 at CG exit
   unsigned long long max_cflx_bits, max_cfly_bits;  // positive doubles as ordered bits
   double volume;
@@ -95,6 +95,7 @@ struct View {
   const double *bottomZ, *bottomXP, *bottomYP;
   // per-step work
   double *EnXP, *EnYP, *Gx, *Gy, *Ct, *b;
+  double *Hx, *Hy;  // symmetrically scaled couplings of the single-sweep CG
   double *x, *r, *p0, *p1, *q;
   double *cellV, *Sm, *Fuu, *Fvv;
   unsigned char *rmv;

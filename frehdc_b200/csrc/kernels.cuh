@@ -8,7 +8,7 @@ namespace frehd {
 
 // Step statistics written by k_finish (device memory, read by the host).
 struct StepOut {
-  int step, cg_iters, status, n_cfl_warn, n_fix, pad;
+  int step, cg_iters, status, n_cfl_warn, n_fix, cg_fallback;
   double cg_rr, cg_bb, max_cflx, max_cfly, volume;
   long long cg_iters_total;
 };
@@ -42,7 +42,7 @@ __global__ void k_system_to_ref(View w, double *GnCt, double *GnXP, double *GnXM
 __global__ void k_solution_from_ref(View w, const double *xs);
 
 // Persistent Jacobi-preconditioned CG (cg.cu).
-__global__ void k_cg(View w, int x0_surface);
+__global__ void k_cg(View w, int x0_surface, int eliminate);
 
 constexpr int kCgThreads = 512;
 

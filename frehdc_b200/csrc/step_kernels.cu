@@ -732,6 +732,7 @@ __global__ void k_finish(View w, int nblocks_vel, StepOut *out) {
     Scratch *sc = w.sc;
     out->step = sc->tt;
     out->cg_iters = sc->cg_iters;
+    out->cg_fallback = sc->cg_fallback;
     out->status = FREHD_OK;
     out->cg_rr = sc->cg_rr;
     out->cg_bb = sc->cg_bb;

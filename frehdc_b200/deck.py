@@ -55,6 +55,7 @@ class DeckSpec:
     eta0_amp: float = 0.05
     scalar_sigma: float = 100.0
     scalar_peak: float = 1.0
+    scalar_in_window: bool = False  # plume at the centre of the (cropped) window, not the basin
     dsurf: float = 0.01
     eps: float = 1e-12
     max_iter: int = 100000
@@ -199,8 +200,12 @@ def make_deck(spec: DeckSpec, start: str = DEFAULT_START, with_tables: bool = Fa
     xb_full = _xb(jj + j0, nyf, spec.dx)
     L = nyf * spec.dx
     surf0 = spec.eta0_amp * np.sin(2.0 * np.pi * xb_full / L)
-    xcen = ((ii + i0) + 0.5) * spec.dx - 0.5 * nxf * spec.dx
-    ycen = ((jj + j0) + 0.5) * spec.dx - 0.5 * nyf * spec.dx
+    if spec.scalar_in_window:
+        xcen = (ii + 0.5) * spec.dx - 0.5 * nx * spec.dx
+        ycen = (jj + 0.5) * spec.dx - 0.5 * ny * spec.dx
+    else:
+        xcen = ((ii + i0) + 0.5) * spec.dx - 0.5 * nxf * spec.dx
+        ycen = ((jj + j0) + 0.5) * spec.dx - 0.5 * nyf * spec.dx
     S0 = spec.scalar_peak * np.exp(-(xcen ** 2 + ycen ** 2) / (2.0 * spec.scalar_sigma ** 2))
 
     lo_eta = min(-spec.tide_amp, -spec.eta0_amp)

@@ -80,7 +80,7 @@ class StepStats(C.Structure):
     _fields_ = [
         ("step", C.c_int), ("cg_iters", C.c_int), ("status", C.c_int),
         ("cg_rel_residual", C.c_double), ("max_cflx", C.c_double), ("max_cfly", C.c_double),
-        ("n_cfl_warn", C.c_int), ("volume", C.c_double),
+        ("n_cfl_warn", C.c_int), ("volume", C.c_double), ("cg_fallback", C.c_int),
     ]
 
 
@@ -131,6 +131,7 @@ _vp = C.c_void_p
 PHASE_EXPLICIT, PHASE_SOLVE, PHASE_UPDATE = 1, 2, 3
 X0_ZERO, X0_SURFACE = 0, 1
 CG_SINGLE_SWEEP, CG_TWO_PHASE = 0, 1
+DECOUPLED_AS_ASSEMBLED, DECOUPLED_ELIMINATED = 0, 1
 STATUS = {0: "ok", 1: "invalid", 2: "unsupported", 3: "cuda", 4: "nomem", 5: "cg_noconverge",
           6: "cfl", 7: "timeout", 8: "state"}
 
@@ -152,6 +153,7 @@ def _declare_domain(L: C.CDLL) -> None:
     L.frehd_domain_set_tide.argtypes = [_vp, C.c_int, _dp]
     L.frehd_domain_set_solver.argtypes = [_vp, C.c_int]
     L.frehd_domain_set_cg_schedule.argtypes = [_vp, C.c_int]
+    L.frehd_domain_set_decoupled.argtypes = [_vp, C.c_int]
     L.frehd_domain_upload_state.argtypes = [_vp, C.POINTER(State)]
     L.frehd_domain_download_state.argtypes = [_vp, C.POINTER(State)]
     L.frehd_domain_init.argtypes = [_vp] + [_dp] * 7 + [C.c_int]
@@ -222,6 +224,9 @@ class Domain:
 
     def set_cg_schedule(self, schedule: int):
         check(lib().frehd_domain_set_cg_schedule(self.h, schedule), "set_cg_schedule")
+
+    def set_decoupled(self, mode: int):
+        check(lib().frehd_domain_set_decoupled(self.h, mode), "set_decoupled")
 
     def init(self, bottom, bottomXP, bottomYP, surf0, u0=None, v0=None, S0=None,
              round_trip_output: bool = True):
@@ -348,7 +353,7 @@ def cg_solve_noalloc(nx: int, ny: int, Ct: int, Gx: int, Gy: int, b: int, x: int
 
 
 def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0_ZERO,
-                     schedule: int = CG_SINGLE_SWEEP):
+                     schedule: int = CG_SINGLE_SWEEP, decoupled: int = DECOUPLED_AS_ASSEMBLED):
     """A Domain initialised from a generated deck (frehdc_b200.deck)."""
     from . import deck as D
     d = Domain(D.config_dict(deck), device)
@@ -363,5 +368,6 @@ def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0
     d.set_tide(D.tide_series(deck))
     d.set_solver(x0)
     d.set_cg_schedule(schedule)
+    d.set_decoupled(decoupled)
     d.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
     return d

@@ -128,6 +128,9 @@ typedef struct frehd_step_stats {
   double max_cflx, max_cfly; /* monitorCFL maxima (nsfunctions.c:1196-1223) */
   int n_cfl_warn;            /* cells with CFL > 2 (the reference prints one line each) */
   double volume;             /* sum of cellV over the domain after the step */
+  int cg_fallback;           /* 1: the solve of the assembled matrix stalled (||r|| did not
+                                halve in 400 iterations) and was redone with decoupled rows
+                                eliminated; laspack would run on to maxIter */
 } frehd_step_stats;
 
 /* Create an empty domain on CUDA device `device`.  Unsupported Config options
@@ -220,6 +223,19 @@ int frehd_domain_set_solver(frehd_domain *d, int x0_mode);
  * iteration, as CGIter does it. */
 enum { FREHD_CG_SINGLE_SWEEP = 0, FREHD_CG_TWO_PHASE = 1 };
 int frehd_domain_set_cg_schedule(frehd_domain *d, int schedule);
+
+/* Rows the reference decouples (tidal rows, closed dry cells:
+ * adjustTidalBoundary nsfunctions.c:887-924, matrixCoeffSub subgrid.c:1061-1078)
+ * keep only their diagonal, but their neighbours' rows keep the coupling to
+ * them, so the assembled matrix is not symmetric.
+ * FREHD_DECOUPLED_AS_ASSEMBLED (default): the CG iterates that matrix, as
+ * laspack's CGIter does; results follow the reference's to rounding.
+ * FREHD_DECOUPLED_ELIMINATED: the couplings are moved into the right-hand side
+ * at the decoupled rows' exact values b/|Ct|, so the iterated system is
+ * symmetric positive definite (CG's convergence theory applies); results agree
+ * with the reference to the CG tolerance rather than to rounding. */
+enum { FREHD_DECOUPLED_AS_ASSEMBLED = 0, FREHD_DECOUPLED_ELIMINATED = 1 };
+int frehd_domain_set_decoupled(frehd_domain *d, int mode);
 
 /* The free-surface CG solve alone, for callers that cannot allocate device
  * memory.  No counterpart in the reference (it solves through laspack inside

@@ -21,12 +21,14 @@ RECIPE = os.path.join(HERE, "ref")
 REF_SRC = os.environ.get("FREHD_REFERENCE", "/root/reference")
 
 PARITY_BIN = os.path.join(REF_DIR, "frehd_ref")
+# the parity build with laspack's JacobiPrecond in place of SSORPrecond
+JACOBI_BIN = os.path.join(REF_DIR, "frehd_ref_jacobi")
 TIMING_BIN = os.path.join(REF_DIR, "frehd_ref_timing")
 MLSTEST_BIN = os.path.join(REF_DIR, "mlstest")
 
 
 def available() -> bool:
-    return os.path.exists(PARITY_BIN) and os.path.exists(TIMING_BIN)
+    return all(os.path.exists(b) for b in (PARITY_BIN, JACOBI_BIN, TIMING_BIN))
 
 
 def build(quiet: bool = True) -> bool:
@@ -58,9 +60,13 @@ def read_dump(path: str) -> dict:
     return out
 
 
-def run(deck_dir: str, steps: int, out_path: str, timing: bool = False) -> dict:
-    """Run the reference for `steps` steps and return its final state."""
-    binary = TIMING_BIN if timing else PARITY_BIN
+def run(deck_dir: str, steps: int, out_path: str, timing: bool = False,
+        precond: str = "ssor") -> dict:
+    """Run the reference for `steps` steps and return its final state.
+
+    precond "ssor" is the reference as shipped (SSORPrecond, nsfunctions.c:1016);
+    "jacobi" hands laspack's JacobiPrecond to the same CGIter call."""
+    binary = TIMING_BIN if timing else (JACOBI_BIN if precond == "jacobi" else PARITY_BIN)
     mode = "time" if timing else "run"
     r = subprocess.run([binary, mode, os.path.abspath(deck_dir), str(steps),
                         os.path.abspath(out_path)], capture_output=True, text=True)

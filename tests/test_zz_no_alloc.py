@@ -48,7 +48,9 @@ def test_noalloc_matches_domain_solve(name, scratch):
     import torch
 
     d, _ = deck_for(name, str(scratch))
-    g = native.domain_from_deck(d, geometry="fine")
+    # the no-allocation solve takes decoupled rows' couplings in b (its documented
+    # convention), so the domain solves the same, eliminated form
+    g = native.domain_from_deck(d, geometry="fine", decoupled=native.DECOUPLED_ELIMINATED)
     nx, ny = g.nx, g.ny
     eps, max_iter = g.cfg["eps"], g.cfg["maxIter"]
     dev = torch.device("cuda", 0)

@@ -319,13 +319,15 @@ def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk):
             "peak_kind": peak_kind, "traffic": None,
             "bytes_model": "48 B/cell set-up + 72 B/cell per CG iteration",
             "cg_iters_per_step": iters, "launch_ms": cg_launch_ms}
-    prof = os.path.join(REPO, "profiles", "k_cg_4096_traffic.json")
-    if os.path.exists(prof):
-        try:
-            with open(prof) as f:
-                roof["traffic"] = json.load(f)["bytes_per_launch"]
-        except Exception:
-            pass
+    # DRAM traffic of one launch from the committed ncu summary (scaled from a
+    # smaller capture; it describes the 4096^2 single-sweep solve only)
+    prof = os.path.join(REPO, "profiles", "k_cg1_2048x2048_fp64.md")
+    if args.cg_schedule == "single_sweep" and n == 4096 and os.path.exists(prof):
+        import re
+        m = re.search(r"traffic_bytes_per_4096_launch:\s*([0-9.eE+]+)", open(prof).read())
+        if m:
+            roof["traffic"] = float(m.group(1))
+            roof["traffic_source"] = "profiles/k_cg1_2048x2048_fp64.md (ncu, scaled by cells x iterations)"
     step_bytes = N * (456.0 + 72.0 * iters)
     whole = step_bytes * args.steps / (t_max / 1e3) / 1e9
     cpu = None if args.no_cpu else cpu_baseline_reference(args.cpu_steps, n)

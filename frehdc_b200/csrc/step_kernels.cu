@@ -24,6 +24,9 @@
 namespace frehd {
 
 // ---------------------------------------------------------------- helpers
+// Thread-block tile of the stencil kernels: 32 cells along x (one warp) by 8 rows.
+constexpr int TBX = 32, TBY = 8, EX = TBX + 1, EY = TBY + 1;
+
 __device__ __forceinline__ double rd(const double *a, const Grid &g, int i, int j) {
   return a[g.at(i, j)];
 }
@@ -150,27 +153,45 @@ __device__ __forceinline__ double gface(double coef, double N, double Vf, double
 // Writes EnXP/EnYP, the face coefficients Gx (east face) and Gy (north face),
 // the row diagonal Ct (negated for rows the reference decouples: tidal rows and
 // closed dry cells) and the right-hand side b, all in the padded layout.
-__global__ void k_explicit(View w) {
+// A 32 x 8 block evaluates the explicit term of every x face and y face it
+// needs once: each thread its own east and north face, threads 0-31 the south
+// halo row's north faces and threads 32-39 the west halo column's east faces.
+__global__ void __launch_bounds__(TBX *TBY, 4) k_explicit(View w) {
   if (*(volatile int *)&w.sc->status != FREHD_OK) return;  // a fatal step stops the run
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
   const Params &p = w.p;
   const Grid &g = w.gr;
-  if (i >= g.nx || j >= g.ny) return;
+  __shared__ double sEx[TBY][TBX + 1], sDx[TBY][TBX + 1];  // x faces, column 0 = west halo
+  __shared__ double sEy[TBY + 1][TBX], sDy[TBY + 1][TBX];  // y faces, row 0 = south halo
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TBX + tx;
+  const int i0 = blockIdx.x * TBX, j0 = blockIdx.y * TBY;
+  const int i = i0 + tx, j = j0 + ty;
+  const bool in = i < g.nx && j < g.ny;
+  Ex ex{0.0, 0.0}, ey{0.0, 0.0};
+  if (in) {
+    ex = explicit_x(w, i, j);
+    ey = explicit_y(w, i, j);
+  }
+  sEx[ty][tx + 1] = ex.En;
+  sDx[ty][tx + 1] = ex.Drag;
+  sEy[ty + 1][tx] = ey.En;
+  sDy[ty + 1][tx] = ey.Drag;
+  if (tid < TBX) {  // north faces of the row below the block (ghosts never written: 0)
+    Ex e{0.0, 0.0};
+    if (i0 + tid < g.nx && j0 > 0 && j0 - 1 < g.ny) e = explicit_y(w, i0 + tid, j0 - 1);
+    sEy[0][tid] = e.En;
+    sDy[0][tid] = e.Drag;
+  } else if (tid < TBX + TBY) {  // east faces of the column left of the block
+    const int t = tid - TBX;
+    Ex e{0.0, 0.0};
+    if (i0 > 0 && j0 + t < g.ny) e = explicit_x(w, i0 - 1, j0 + t);
+    sEx[t][0] = e.En;
+    sDx[t][0] = e.Drag;
+  }
+  __syncthreads();
+  if (!in) return;
   const long k = g.at(i, j);
-  const Ex ex = explicit_x(w, i, j);
-  const Ex ey = explicit_y(w, i, j);
-  double EnW = 0.0, DrW = 0.0, EnS = 0.0, DrS = 0.0;  // ghosts never written: 0
-  if (i > 0) {
-    const Ex e = explicit_x(w, i - 1, j);
-    EnW = e.En;
-    DrW = e.Drag;
-  }
-  if (j > 0) {
-    const Ex e = explicit_y(w, i, j - 1);
-    EnS = e.En;
-    DrS = e.Drag;
-  }
+  const double EnW = sEx[ty][tx], DrW = sDx[ty][tx];  // i = 0: the halo holds 0
+  const double EnS = sEy[ty][tx], DrS = sDy[ty][tx];  // j = 0: the halo holds 0
   w.EnXP[k] = ex.En;
   w.EnYP[k] = ey.En;
   if (j == 0) w.EnXP[g.at(i, -1)] = ex.En;  // dragInversion ghost copies
@@ -227,10 +248,17 @@ __device__ __forceinline__ double level_surf(const Params &p, int k) {
   return frehd_level(p.surfmin, p.dsurf, k) + p.offset;  // subgrid.c:2118
 }
 
-__device__ __forceinline__ void level_values(const Params &p, int i, int j, int k, frehd_cell_levels *o) {
+// Table values of cell (i, j) at level k: all ten, or (part) only the west- or
+// south-face pair.
+__device__ __forceinline__ void level_values(const Params &p, int i, int j, int k, frehd_cell_levels *o,
+                                             int part) {
   if (p.geom_fine) {
-    frehd_cell_levels_at(p.zf, p.fpitch, p.nx, p.ny, p.r, i, j, frehd_level(p.surfmin, p.dsurf, k),
-                         p.dxf * p.dyf, p.dxf, o);
+    if (p.r == 4)
+      frehd_cell_levels_r4(p.zf, p.fpitch, p.nx, p.ny, i, j, frehd_level(p.surfmin, p.dsurf, k),
+                           p.dxf * p.dyf, p.dxf, part, o);
+    else
+      frehd_cell_levels_at(p.zf, p.fpitch, p.nx, p.ny, p.r, i, j, frehd_level(p.surfmin, p.dsurf, k),
+                           p.dxf * p.dyf, p.dxf, o);
   } else {
     const long N = (long)p.nx * p.ny, T = N * p.Ne;
     const double *t = p.tab + (long)k * N + (long)j * p.nx + i;
@@ -245,6 +273,9 @@ struct SubCell {
 
 // computeSubArea for one cell (subgrid.c:87-249) with useSubDrag = 0 and
 // useminA = 0; the minV* interpolations feed only useminV = 1/2 and are skipped.
+// PART = FREHD_LV_ALL computes every value; FREHD_LV_WEST only Nm and Vxm,
+// FREHD_LV_SOUTH only Om and Vym (what the west/south neighbour's face needs).
+template <int PART>
 __device__ SubCell compute_sub_area(const View &w, int i, int j, double s, int *ind_io,
                                     double depth_old) {
   const Params &p = w.p;
@@ -265,34 +296,42 @@ __device__ SubCell compute_sub_area(const View &w, int i, int j, double s, int *
   else j2 = s > level_surf(p, j1) ? j1 + 1 : j1 - 1;
   const double a1 = level_surf(p, j1), a2 = level_surf(p, j2);
   frehd_cell_levels L1, L2;
-  level_values(p, i, j, j1, &L1);
-  if (j2 != j1) level_values(p, i, j, j2, &L2); else L2 = L1;
+  level_values(p, i, j, j1, &L1, PART);
+  if (j2 != j1) level_values(p, i, j, j2, &L2, PART); else L2 = L1;
   SubCell c;
-  c.V = interp_surf(s, a1, L1.V, a2, L2.V);
-  c.Z = interp_surf(s, a1, L1.Z, a2, L2.Z);
-  c.Vxp = interp_surf(s, a1, L1.Vxp, a2, L2.Vxp);
-  c.Vyp = interp_surf(s, a1, L1.Vyp, a2, L2.Vyp);
-  c.Vxm = interp_surf(s, a1, L1.Vxm, a2, L2.Vxm);
-  c.Vym = interp_surf(s, a1, L1.Vym, a2, L2.Vym);
-  const double bxp = rd(w.bottomXP, g, i, j), byp = rd(w.bottomYP, g, i, j);
-  const double bxm = i > 0 ? rd(w.bottomXP, g, i - 1, j) : 0.0;  // edgeX is N-sized: ghost reads 0
-  const double bym = j > 0 ? rd(w.bottomYP, g, i, j - 1) : 0.0;
 #define FREHD_FACE(out, wd, f)                                                         \
   {                                                                                    \
     const double wd_ = (wd);                                                           \
     if (wd_ > a1 && wd_ < a2) out = wd_ > s ? 0.0 : interp_surf(s, wd_, 0.0, a2, L2.f); \
     else out = interp_surf(s, a1, L1.f, a2, L2.f);                                     \
   }
-  FREHD_FACE(c.Np, bxp, Np);
-  FREHD_FACE(c.Nm, bxm, Nm);
-  FREHD_FACE(c.Op, byp, Op);
-  FREHD_FACE(c.Om, bym, Om);
+  if (PART == FREHD_LV_ALL) {
+    c.V = interp_surf(s, a1, L1.V, a2, L2.V);
+    c.Z = interp_surf(s, a1, L1.Z, a2, L2.Z);
+    c.Vxp = interp_surf(s, a1, L1.Vxp, a2, L2.Vxp);
+    c.Vyp = interp_surf(s, a1, L1.Vyp, a2, L2.Vyp);
+    const double bxp = rd(w.bottomXP, g, i, j), byp = rd(w.bottomYP, g, i, j);
+    FREHD_FACE(c.Np, bxp, Np);
+    FREHD_FACE(c.Op, byp, Op);
+    if (depth_old == 0) { c.Vxp = 0; c.Vyp = 0; }
+    if (s - bxp <= 0) c.Np = 0;
+    if (s - byp <= 0) c.Op = 0;
+  }
+  if (PART != FREHD_LV_SOUTH) {
+    c.Vxm = interp_surf(s, a1, L1.Vxm, a2, L2.Vxm);
+    const double bxm = i > 0 ? rd(w.bottomXP, g, i - 1, j) : 0.0;  // edgeX is N-sized: ghost reads 0
+    FREHD_FACE(c.Nm, bxm, Nm);
+    if (depth_old == 0) c.Vxm = 0;
+    if (i > 0 && s - bxm <= 0) c.Nm = 0;
+  }
+  if (PART != FREHD_LV_WEST) {
+    c.Vym = interp_surf(s, a1, L1.Vym, a2, L2.Vym);
+    const double bym = j > 0 ? rd(w.bottomYP, g, i, j - 1) : 0.0;
+    FREHD_FACE(c.Om, bym, Om);
+    if (depth_old == 0) c.Vym = 0;
+    if (j > 0 && s - bym <= 0) c.Om = 0;
+  }
 #undef FREHD_FACE
-  if (depth_old == 0) { c.Vxp = 0; c.Vyp = 0; c.Vxm = 0; c.Vym = 0; }
-  if (s - bxp <= 0) c.Np = 0;
-  if (s - byp <= 0) c.Op = 0;
-  if (i > 0 && s - bxm <= 0) c.Nm = 0;
-  if (j > 0 && s - bym <= 0) c.Om = 0;
   return c;
 }
 
@@ -339,10 +378,14 @@ __device__ NewSurf new_surface(const View &w, int i, int j) {
 // ---------------------------------------------------------------- k_update_geo
 // Shared-memory tile: each 32x8 block evaluates the subgrid half-cell values of
 // its cells plus one column east and one row north, then combines them.
-constexpr int TBX = 32, TBY = 8, EX = TBX + 1, EY = TBY + 1;
+// Blocks of k_update_geo per SM the register allocation aims for (2: 128
+// registers without spills; 3: 80 registers with some spill traffic to L1).
+#ifndef FREHD_GEO_MIN_BLOCKS
+#define FREHD_GEO_MIN_BLOCKS 3
+#endif
 
 template <bool kInit>
-__global__ void __launch_bounds__(TBX *TBY) k_update_geo(View w) {
+__global__ void __launch_bounds__(TBX *TBY, FREHD_GEO_MIN_BLOCKS) k_update_geo(View w) {
   if (!kInit && *(volatile int *)&w.sc->status != FREHD_OK) return;
   const Params &p = w.p;
   const Grid &g = w.gr;
@@ -351,12 +394,23 @@ __global__ void __launch_bounds__(TBX *TBY) k_update_geo(View w) {
   __shared__ double sh_V[EY][EX], sh_Z[EY][EX];
   const int i0 = blockIdx.x * TBX, j0 = blockIdx.y * TBY;
   const int tid = threadIdx.y * TBX + threadIdx.x;
-  for (int e = tid; e < EX * EY; e += TBX * TBY) {
-    const int ex = e % EX, ey = e / EX;
+  // Each thread evaluates its own cell; threads 0..TBX-1 then evaluate the north
+  // halo row (only Om, Vym, s are read from it) and threads TBX..TBX+TBY-1 the
+  // east halo column (only Nm, Vxm, s).
+  for (int pass = 0; pass < 2; ++pass) {
+    int ex, ey;
+    if (pass == 0) {
+      ex = threadIdx.x;
+      ey = threadIdx.y;
+    } else {
+      if (tid >= TBX + TBY) break;
+      ex = tid < TBX ? tid : TBX;
+      ey = tid < TBX ? TBY : tid - TBX;
+    }
     const int i = i0 + ex, j = j0 + ey;
     if (i >= g.nx || j >= g.ny) continue;
     const long k = g.at(i, j);
-    const bool own = ex < TBX && ey < TBY;
+    const bool own = pass == 0;
     double s;
     double depth_old = w.depth_cur[k];
     if (kInit) {
@@ -384,12 +438,20 @@ __global__ void __launch_bounds__(TBX *TBY) k_update_geo(View w) {
       }
     }
     int ind = w.ind_cur[k];
-    const SubCell c = compute_sub_area(w, i, j, s, &ind, depth_old);
-    if (own) w.ind_nxt[k] = ind;
     sh_s[ey][ex] = s;
-    sh_Np[ey][ex] = c.Np; sh_Nm[ey][ex] = c.Nm; sh_Op[ey][ex] = c.Op; sh_Om[ey][ex] = c.Om;
-    sh_Vxp[ey][ex] = c.Vxp; sh_Vxm[ey][ex] = c.Vxm; sh_Vyp[ey][ex] = c.Vyp; sh_Vym[ey][ex] = c.Vym;
-    sh_V[ey][ex] = c.V; sh_Z[ey][ex] = c.Z;
+    if (own) {
+      const SubCell c = compute_sub_area<FREHD_LV_ALL>(w, i, j, s, &ind, depth_old);
+      w.ind_nxt[k] = ind;
+      sh_Np[ey][ex] = c.Np; sh_Nm[ey][ex] = c.Nm; sh_Op[ey][ex] = c.Op; sh_Om[ey][ex] = c.Om;
+      sh_Vxp[ey][ex] = c.Vxp; sh_Vxm[ey][ex] = c.Vxm; sh_Vyp[ey][ex] = c.Vyp; sh_Vym[ey][ex] = c.Vym;
+      sh_V[ey][ex] = c.V; sh_Z[ey][ex] = c.Z;
+    } else if (ex == TBX) {
+      const SubCell c = compute_sub_area<FREHD_LV_WEST>(w, i, j, s, &ind, depth_old);
+      sh_Nm[ey][ex] = c.Nm; sh_Vxm[ey][ex] = c.Vxm;
+    } else {
+      const SubCell c = compute_sub_area<FREHD_LV_SOUTH>(w, i, j, s, &ind, depth_old);
+      sh_Om[ey][ex] = c.Om; sh_Vym[ey][ex] = c.Vym;
+    }
   }
   __syncthreads();
   const int tx = threadIdx.x, ty = threadIdx.y;

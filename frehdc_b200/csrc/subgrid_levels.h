@@ -136,6 +136,105 @@ FREHD_HD void frehd_cell_levels_at(const double *zf, long fpitch, int nx, int ny
   o->Om = s * dxf;
 }
 
+/* Parts of the table values frehd_cell_levels_r4 computes. */
+enum { FREHD_LV_ALL = 0, FREHD_LV_WEST = 1, FREHD_LV_SOUTH = 2 };
+
+/*
+ * frehd_cell_levels_at for r == 4, with every fine depth evaluated once: the face
+ * areas reuse the block's own edge depths instead of recomputing them.  Same
+ * operations in the same order, so the same doubles.  `part` selects all ten
+ * values, or only the west-face pair (Nm, Vxm) or the south-face pair (Om, Vym)
+ * that the west or south neighbour's face combination needs.
+ */
+FREHD_HD void frehd_cell_levels_r4(const double *zf, long fpitch, int nx, int ny, int i, int j,
+                                   double h, double dA, double dxf, int part,
+                                   frehd_cell_levels *o) {
+  (void)nx;
+  const double *b = zf + (long)j * 4 * fpitch + (long)i * 4;
+  double d[4][4];
+  if (part == FREHD_LV_ALL) {
+    for (int fj = 0; fj < 4; ++fj)
+      for (int fi = 0; fi < 4; ++fi) d[fj][fi] = frehd_fine_depth(h, b[(long)fj * fpitch + fi]);
+    double sV = 0.0, cnt = 0.0, sxp = 0.0, sxm = 0.0, syp = 0.0, sym = 0.0;
+    for (int fj = 0; fj < 4; ++fj) {
+      double cxp = 0.0, cxm = 0.0, call = 0.0;
+      for (int fi = 0; fi < 4; ++fi) {
+        const double dd = d[fj][fi];
+        sV += dd;
+        if (dd > 0.0) cnt += 1.0;
+        if (fi < 2) cxm += dd; else cxp += dd;
+        call += dd;
+      }
+      sxp += cxp;
+      sxm += cxm;
+      if (fj < 2) sym += call; else syp += call;
+    }
+    o->V = dA * sV;
+    o->Z = dA * cnt;
+    o->Vxp = dA * sxp;
+    o->Vxm = dA * sxm;
+    o->Vyp = dA * syp;
+    o->Vym = dA * sym;
+    double s = 0.0;
+    if (i < nx - 1) {
+      for (int fj = 0; fj < 4; ++fj)
+        s += frehd_min2(d[fj][3], frehd_fine_depth(h, b[(long)fj * fpitch + 4]));
+    } else {
+      for (int fj = 0; fj < 4; ++fj) s += d[fj][3];
+    }
+    o->Np = s * dxf;
+    s = 0.0;
+    if (j < ny - 1) {
+      const double *r1 = b + 4 * fpitch;
+      for (int fi = 0; fi < 4; ++fi) s += frehd_min2(d[3][fi], frehd_fine_depth(h, r1[fi]));
+    } else {
+      for (int fi = 0; fi < 4; ++fi) s += d[3][fi];
+    }
+    o->Op = s * dxf;
+  } else if (part == FREHD_LV_WEST) {
+    for (int fj = 0; fj < 4; ++fj)
+      for (int fi = 0; fi < 2; ++fi) d[fj][fi] = frehd_fine_depth(h, b[(long)fj * fpitch + fi]);
+    double sxm = 0.0;
+    for (int fj = 0; fj < 4; ++fj) {
+      double cxm = 0.0;
+      cxm += d[fj][0];
+      cxm += d[fj][1];
+      sxm += cxm;
+    }
+    o->Vxm = dA * sxm;
+  } else {
+    for (int fj = 0; fj < 2; ++fj)
+      for (int fi = 0; fi < 4; ++fi) d[fj][fi] = frehd_fine_depth(h, b[(long)fj * fpitch + fi]);
+    double sym = 0.0;
+    for (int fj = 0; fj < 2; ++fj) {
+      double call = 0.0;
+      for (int fi = 0; fi < 4; ++fi) call += d[fj][fi];
+      sym += call;
+    }
+    o->Vym = dA * sym;
+  }
+  if (part != FREHD_LV_SOUTH) {  /* Nm: west neighbour's last x-row against own first */
+    double s = 0.0;
+    if (i > 0) {
+      for (int fj = 0; fj < 4; ++fj)
+        s += frehd_min2(frehd_fine_depth(h, b[(long)fj * fpitch - 1]), d[fj][0]);
+    } else {
+      for (int fj = 0; fj < 4; ++fj) s += d[fj][0];
+    }
+    o->Nm = s * dxf;
+  }
+  if (part != FREHD_LV_WEST) {  /* Om: south neighbour's last y-row against own first */
+    double s = 0.0;
+    if (j > 0) {
+      const double *r0 = b - fpitch;
+      for (int fi = 0; fi < 4; ++fi) s += frehd_min2(frehd_fine_depth(h, r0[fi]), d[0][fi]);
+    } else {
+      for (int fi = 0; fi < 4; ++fi) s += d[0][fi];
+    }
+    o->Om = s * dxf;
+  }
+}
+
 /* Coarse bottom and face-bottom elevations of cell (i, j) (host pre-processing;
  * script_CreateSubAreaWithBlockV16.m:153,159-175). */
 FREHD_HD void frehd_cell_bottoms(const double *zf, long fpitch, int nx, int ny, int r,

@@ -12,7 +12,8 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libfrehd_b200.so")
+# the in-tree build; FREHD_B200_LIB names another build of the same library
+LIB_PATH = os.environ.get("FREHD_B200_LIB") or os.path.join(HERE, "libfrehd_b200.so")
 
 _lib = None
 

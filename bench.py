@@ -357,6 +357,125 @@ def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk):
     return 0
 
 
+# ---------------------------------------------------------------- batched / served forms
+def mix_specs(n: int, seed: int, smin: int, smax: int, steps: int):
+    """Seeded mix of basins: sides log-uniform in [smin, smax] (multiples of 8),
+    square or 1:4 (fair coin), depth 0.3-8 m, 0-40 % dry at low tide, tide
+    amplitude 0.1-0.5 m, Manning n 0.02-0.04, dt 1 s, dx 10 m, 4x4 subgrid."""
+    import numpy as np
+
+    from frehdc_b200 import deck as D
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        side = float(np.exp(rng.uniform(np.log(smin), np.log(smax))))
+        a = int(max(8, round(side / 8) * 8))
+        if rng.random() < 0.5:
+            nx = ny = a
+        else:  # 1:4, same cell count scale
+            nx, ny = max(8, (a // 2) // 8 * 8), max(8, (a * 2) // 8 * 8)
+        out.append(D.DeckSpec(nx=nx, ny=ny, dx=10.0, dt=1.0, steps=steps, seed=seed * 1000 + k,
+                              depth_min=0.3, depth_max=8.0,
+                              dry_frac=float(rng.uniform(0.0, 0.4)) or None,
+                              tide_amp=float(rng.uniform(0.1, 0.5)),
+                              manning_n=float(rng.uniform(0.02, 0.04))))
+    return out
+
+
+def run_batched_form(args):
+    """Cell-steps/s of a mix of domains stepped as one batch, against the same
+    mix stepped one domain at a time through the single-domain API."""
+    import torch
+
+    from frehdc_b200 import deck as D
+    from frehdc_b200 import native
+    specs = mix_specs(args.mix, 77, args.mix_min, args.mix_max, args.steps + args.warmup + 5)
+    t0 = time.time()
+    decks = [D.make_deck(sp) for sp in specs]
+    gen_s = time.time() - t0
+    cells = [sp.nx * sp.ny for sp in specs]
+    K = args.steps
+    # plain form: each domain alone, device time of its K steps (kernel events)
+    plain_ms = 0.0
+    for dk in decks:
+        g = native.domain_from_deck(dk)
+        g.run(1, args.warmup)
+        g.sync()
+        g.set_profiling(True)
+        g.run(1 + args.warmup, K)
+        g.sync()
+        kt = g.kernel_times()
+        plain_ms += sum(kt[k] for k in ("explicit_ms", "cg_ms", "update_geo_ms", "update_vel_ms",
+                                        "finish_ms"))
+        g.close()
+    # batched form
+    doms = [native.domain_from_deck(dk) for dk in decks]
+    b = native.Batch(args.budget_gb << 30, args.cells_per_cta)
+    for g in doms:
+        b.admit(g, 1)
+    for _ in range(args.warmup):
+        b.step()
+    b.sync()
+    st = torch.cuda.ExternalStream(b.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        e0.record(st)
+        for _ in range(K):
+            b.step()
+        e1.record(st)
+        e1.synchronize()
+    batch_ms = e0.elapsed_time(e1)
+    info = b.info()
+    b.close()
+    total = float(sum(cells)) * K
+    line = {"metric": METRIC, "form": "batched", "value": total / (batch_ms / 1e3),
+            "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": args.warmup,
+            "ms_per_step": batch_ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{len(specs)} seeded basins, sides log-uniform "
+                                   f"{args.mix_min}-{args.mix_max} (square or 1:4), dx 10 m, "
+                                   "dt 1 s, depth 0.3-8 m, 0-40% dry, tide 0.1-0.5 m, "
+                                   "n 0.02-0.04, 4x4 subgrid, 1 scalar, FP64",
+                       "cells": int(sum(cells)), "cells_per_cta": args.cells_per_cta,
+                       "deck_gen_s": round(gen_s, 1)},
+            "plain_form_same_mix": {"value": total / (plain_ms / 1e3), "unit": UNIT,
+                                    "note": "each domain stepped alone, device time of its "
+                                            "kernels summed over the mix"},
+            "batch": info, "gpu_launches": 5 * K, "clocks": clk.summary()}
+    line["speedup_vs_plain_form"] = line["value"] / line["plain_form_same_mix"]["value"]
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_served_form(args):
+    """A stream of requests with Poisson arrivals served by continuous batching."""
+    import numpy as np
+
+    from frehdc_b200 import deck as D
+    from frehdc_b200 import serve
+    rng = np.random.default_rng(5)
+    specs = mix_specs(args.requests, 91, args.mix_min, args.mix_max, 10)
+    steps = rng.integers(args.req_steps_min, args.req_steps_max + 1, size=len(specs))
+    t0 = time.time()
+    decks = [D.make_deck(sp.replace(steps=int(k) + 5)) for sp, k in zip(specs, steps)]
+    gen_s = time.time() - t0
+    arr = serve.poisson_arrivals(len(specs), args.rate, 17)
+    reqs = [serve.Request(i, dk, int(k), float(a)) for i, (dk, k, a) in enumerate(zip(decks, steps, arr))]
+    with ClockSampler(0) as clk:
+        res = serve.serve(reqs, args.budget_gb << 30, args.cells_per_cta)
+    line = {"metric": METRIC, "form": "served", "value": res["cell_steps_per_s"], "unit": UNIT,
+            "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "p50_latency_s": res["p50_s"], "p99_latency_s": res["p99_s"],
+            "config": {"workload": f"{len(reqs)} requests, Poisson arrivals {args.rate}/s, sides "
+                                   f"log-uniform {args.mix_min}-{args.mix_max}, steps "
+                                   f"{args.req_steps_min}-{args.req_steps_max}, 1 scalar, FP64",
+                       "cells_per_cta": args.cells_per_cta, "deck_gen_s": round(gen_s, 1)},
+            "serving": res, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -370,11 +489,28 @@ def main():
     ap.add_argument("--cg-schedule", default="single_sweep", choices=list(SCHEDULES),
                     help="CG schedule: one sweep and one reduction per iteration, or the "
                          "textbook two-phase ordering")
+    ap.add_argument("--form", default="plain", choices=["plain", "batched", "served"],
+                    help="plain: one 4096^2 domain; batched: a mix of domains as one batch; "
+                         "served: Poisson request stream with continuous batching")
+    ap.add_argument("--mix", type=int, default=64, help="batched form: domains in the mix")
+    ap.add_argument("--mix-min", type=int, default=64)
+    ap.add_argument("--mix-max", type=int, default=512)
+    ap.add_argument("--cells-per-cta", type=float, default=65536.0,
+                    help="batched/served: cells per CTA of a domain's CG")
+    ap.add_argument("--budget-gb", type=int, default=120)
+    ap.add_argument("--requests", type=int, default=120)
+    ap.add_argument("--rate", type=float, default=50.0)
+    ap.add_argument("--req-steps-min", type=int, default=50)
+    ap.add_argument("--req-steps-max", type=int, default=400)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.form == "batched":
+        return run_batched_form(args)
+    if args.form == "served":
+        return run_served_form(args)
     return run_gpu_arm(args)
 
 

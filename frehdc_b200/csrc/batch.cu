@@ -1,0 +1,440 @@
+// Batched stepping of many resident domains (include/frehd_b200.h, frehd_batch_*).
+//
+// Domains are set up one by one with the single-domain calls (create, geometry,
+// tide, init), then admitted into a batch, which owns their stepping until they
+// are released.  One batch step advances every admitted domain by one time step
+// with five launches in total, whatever the number of domains:
+//   k_explicit_batch, k_update_geo_batch, k_update_vel_batch   one block per
+//       (domain, 32 x 8 tile) entry of a tile table over all domains
+//   k_cg1_batch   one cooperative launch; each domain is solved by a group of
+//       CTAs whose size depends on the domain's own cell count only, so a
+//       domain's result does not depend on which other domains share the batch
+//   k_finish_batch   one block per domain; flips the domain's ping-pong half
+// The five launches are captured once per batch composition into a CUDA graph
+// and replayed every step.
+//
+// Admission is by device-memory footprint (a budget given at creation) and by
+// the CTA capacity of the cooperative solve: domains solved by several CTAs get
+// CTAs of their own; domains solved by one CTA are packed onto the remaining
+// CTAs, longest first onto the least loaded (LPT), and solved one after another.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <vector>
+
+#include "cg1.h"
+#include "cg_common.cuh"
+#include "domain_host.h"
+#include "frehd_internal.h"
+#include "kernels.cuh"
+
+using namespace frehd;
+
+#define BATCH_TRY(expr)                                                               \
+  do {                                                                                \
+    cudaError_t e_ = (expr);                                                          \
+    if (e_ != cudaSuccess)                                                            \
+      return fail(FREHD_ERR_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_),     \
+                  __FILE__, __LINE__);                                                \
+  } while (0)
+
+namespace {
+
+struct Slot {
+  frehd_domain *d = nullptr;
+  long long steps = 0;  // batch steps taken since admission
+};
+
+template <class T>
+struct DevArray {
+  T *p = nullptr;
+  size_t cap = 0;
+  int reserve(size_t n) {
+    if (n <= cap) return FREHD_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    const size_t want = std::max<size_t>(n, 16);
+    if (cudaMalloc(&p, sizeof(T) * want) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(FREHD_ERR_NOMEM, "batch tables: %zu bytes", sizeof(T) * want);
+    }
+    cap = want;
+    return FREHD_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+}  // namespace
+
+struct frehd_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  long long budget = 0, used = 0;
+  double cells_per_cta = 0;
+  int capacity = 0;  // co-resident CTAs of k_cg1_batch
+  std::vector<Slot> slots;
+  bool dirty = true;
+  // tables of the current composition
+  DevArray<View> views2;
+  DevArray<const Cg1Maps *> maps;
+  DevArray<BatchTile> tiles;
+  DevArray<FinishJob> fins;
+  DevArray<int> job_start;
+  DevArray<CgJob> jobs;
+  long ntiles = 0;
+  int nfin = 0, nctas = 0;
+  // captured launches
+  int use_graph = 1;
+  cudaGraphExec_t graph = nullptr;
+  int graph_live = 0;
+  long long steps = 0;
+};
+
+namespace {
+
+// CTAs that solve a domain of `cells` cells (by its size alone).
+int group_size(const frehd_batch *b, const frehd_domain *d) {
+  const long ntiles = (long)((d->gr.nx + CTX - 1) / CTX) * ((d->gr.ny + CTY - 1) / CTY);
+  const double cells = (double)d->gr.nx * d->gr.ny;
+  long g = (long)std::lround(cells / b->cells_per_cta);
+  g = std::max(1L, std::min(g, std::min(ntiles, (long)b->capacity)));
+  return (int)g;
+}
+
+// CTAs the batch needs with the given domains: the multi-CTA groups plus one
+// CTA for the single-CTA domains (if any).
+int ctas_needed(const frehd_batch *b, const frehd_domain *extra) {
+  int dedicated = 0, singles = 0;
+  auto add = [&](const frehd_domain *d) {
+    const int g = group_size(b, d);
+    if (g > 1) dedicated += g; else ++singles;
+  };
+  for (const Slot &s : b->slots)
+    if (s.d) add(s.d);
+  if (extra) add(extra);
+  return dedicated + (singles ? 1 : 0);
+}
+
+void drop_graph(frehd_batch *b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+  b->graph_live = 0;
+}
+
+int launch_step(frehd_batch *b) {
+  const dim3 bb(32, 8);
+  k_explicit_batch<<<(unsigned)b->ntiles, bb, 0, b->stream>>>(b->views2.p, b->tiles.p);
+  int rc = cg1_launch_batch(b->views2.p, b->maps.p, b->job_start.p, b->jobs.p, b->nctas, b->stream);
+  if (rc) return rc;
+  k_update_geo_batch<<<(unsigned)b->ntiles, bb, 0, b->stream>>>(b->views2.p, b->tiles.p);
+  k_update_vel_batch<<<(unsigned)b->ntiles, bb, 0, b->stream>>>(b->views2.p, b->tiles.p);
+  k_finish_batch<<<(unsigned)b->nfin, 256, 0, b->stream>>>(b->views2.p, b->fins.p);
+  BATCH_TRY(cudaGetLastError());
+  return FREHD_OK;
+}
+
+// Rebuild the tables for the current composition (and the graph, lazily).
+int rebuild(frehd_batch *b) {
+  drop_graph(b);
+  const int nslot = (int)b->slots.size();
+  std::vector<View> views(2 * (size_t)std::max(nslot, 1));
+  std::vector<const Cg1Maps *> maps(std::max(nslot, 1), nullptr);
+  std::vector<BatchTile> tiles;
+  std::vector<FinishJob> fins;
+  struct Dom {
+    int slot, g;
+    double cells;
+  };
+  std::vector<Dom> doms;
+  for (int s = 0; s < nslot; ++s) {
+    frehd_domain *d = b->slots[s].d;
+    if (!d) continue;
+    views[2 * s] = domain_view(d, 0);
+    views[2 * s + 1] = domain_view(d, 1);
+    maps[s] = d->cg1_maps_dev;
+    const int gx = (d->gr.nx + 31) / 32, gy = (d->gr.ny + 7) / 8;
+    for (int by = 0; by < gy; ++by)
+      for (int bx = 0; bx < gx; ++bx) tiles.push_back(BatchTile{s, bx, by, gx});
+    fins.push_back(FinishJob{s, gx * gy, d->out});
+    doms.push_back(Dom{s, group_size(b, d), (double)d->gr.nx * d->gr.ny});
+  }
+  b->ntiles = (long)tiles.size();
+  b->nfin = (int)fins.size();
+  b->nctas = 0;
+  b->dirty = false;
+  if (doms.empty()) return FREHD_OK;
+
+  // CTA packing: multi-CTA groups on CTAs of their own, then single-CTA domains
+  // longest first onto the least loaded remaining CTA.
+  std::vector<std::vector<CgJob>> per_cta;
+  auto flags_of = [&](int s) {
+    const frehd_domain *d = b->slots[s].d;
+    return (d->x0_mode == FREHD_X0_SURFACE ? 1 : 0) | (d->eliminate ? 2 : 0);
+  };
+  std::vector<Dom> singles;
+  for (const Dom &m : doms) {
+    if (m.g > 1) {
+      for (int r = 0; r < m.g; ++r) per_cta.push_back({CgJob{m.slot, r, m.g, flags_of(m.slot)}});
+    } else {
+      singles.push_back(m);
+    }
+  }
+  const int free_ctas = b->capacity - (int)per_cta.size();
+  if (free_ctas < (singles.empty() ? 0 : 1))
+    return fail(FREHD_ERR_STATE, "batch CTA capacity exceeded (%d CTAs for multi-CTA domains of %d)",
+                (int)per_cta.size(), b->capacity);
+  if (!singles.empty()) {
+    std::stable_sort(singles.begin(), singles.end(),
+                     [](const Dom &a, const Dom &c) { return a.cells > c.cells; });
+    const int nbins = std::min(free_ctas, (int)singles.size());
+    std::vector<double> load(nbins, 0.0);
+    std::vector<std::vector<CgJob>> bins(nbins);
+    for (const Dom &m : singles) {
+      const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      load[k] += m.cells;
+      bins[k].push_back(CgJob{m.slot, 0, 1, flags_of(m.slot)});
+    }
+    for (auto &bin : bins) per_cta.push_back(bin);
+  }
+  std::vector<int> start(per_cta.size() + 1, 0);
+  std::vector<CgJob> jobs;
+  for (size_t c = 0; c < per_cta.size(); ++c) {
+    start[c] = (int)jobs.size();
+    jobs.insert(jobs.end(), per_cta[c].begin(), per_cta[c].end());
+  }
+  start[per_cta.size()] = (int)jobs.size();
+  b->nctas = (int)per_cta.size();
+
+  int rc = 0;
+  rc = rc ? rc : b->views2.reserve(views.size());
+  rc = rc ? rc : b->maps.reserve(maps.size());
+  rc = rc ? rc : b->tiles.reserve(tiles.size());
+  rc = rc ? rc : b->fins.reserve(fins.size());
+  rc = rc ? rc : b->job_start.reserve(start.size());
+  rc = rc ? rc : b->jobs.reserve(jobs.size());
+  if (rc) return rc;
+  BATCH_TRY(cudaMemcpyAsync(b->views2.p, views.data(), sizeof(View) * views.size(), cudaMemcpyHostToDevice, b->stream));
+  BATCH_TRY(cudaMemcpyAsync(b->maps.p, maps.data(), sizeof(const Cg1Maps *) * maps.size(), cudaMemcpyHostToDevice, b->stream));
+  BATCH_TRY(cudaMemcpyAsync(b->tiles.p, tiles.data(), sizeof(BatchTile) * tiles.size(), cudaMemcpyHostToDevice, b->stream));
+  BATCH_TRY(cudaMemcpyAsync(b->fins.p, fins.data(), sizeof(FinishJob) * fins.size(), cudaMemcpyHostToDevice, b->stream));
+  BATCH_TRY(cudaMemcpyAsync(b->job_start.p, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice, b->stream));
+  BATCH_TRY(cudaMemcpyAsync(b->jobs.p, jobs.data(), sizeof(CgJob) * jobs.size(), cudaMemcpyHostToDevice, b->stream));
+  // the host vectors go out of scope: the copies must have left them
+  BATCH_TRY(cudaStreamSynchronize(b->stream));
+  return FREHD_OK;
+}
+
+// Capture the five launches of one step into a graph; on any failure the batch
+// keeps launching them directly.
+void capture(frehd_batch *b) {
+  if (!b->use_graph || b->graph_live || b->nfin == 0) return;
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    b->use_graph = 0;
+    return;
+  }
+  const int rc = launch_step(b);
+  const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  if (rc || e != cudaSuccess || !g) {
+    cudaGetLastError();
+    clear_error();
+    if (g) cudaGraphDestroy(g);
+    b->use_graph = 0;
+    return;
+  }
+  if (cudaGraphInstantiate(&b->graph, g, 0) != cudaSuccess) {
+    cudaGetLastError();
+    b->graph = nullptr;
+    b->use_graph = 0;
+  } else {
+    b->graph_live = 1;
+  }
+  cudaGraphDestroy(g);
+}
+
+}  // namespace
+
+extern "C" int frehd_domain_footprint(const frehd_config *cfg, int r, long long *bytes) {
+  if (!cfg || !bytes || r < 1 || cfg->nx < 2 || cfg->ny < 2) return fail(FREHD_ERR_INVALID, "bad argument");
+  const Grid g = Grid::make(cfg->nx, cfg->ny);
+  const long long tot = g.total, N = (long long)cfg->nx * cfg->ny;
+  const long long T = (long long)(cfg->nx + 2) * (cfg->ny + 2);
+  const long long nvel = (long long)((cfg->nx + 31) / 32) * ((cfg->ny + 7) / 8);
+  long long b = 0;
+  b += 2 * (3 * 8 + 4) * tot;       // surf, depth, S (double) and ind (int), both halves
+  b += 36 * 8 * tot;                // persistent, per-step and CG arrays
+  b += tot;                         // rmv flags
+  b += 4 * N + 2 * 8 * T;           // fix list, staging
+  b += 8 * std::max(nvel, 8LL * 148 + 8) + 4096;  // partials, scratch, maps
+  b += 8 * N * (long long)r * r;    // fine bottoms
+  *bytes = b;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_batch_create(int device, long long hbm_budget_bytes, double cells_per_cta,
+                                  frehd_batch **out) {
+  clear_error();
+  if (!out || hbm_budget_bytes <= 0 || !(cells_per_cta > 0)) return fail(FREHD_ERR_INVALID, "bad argument");
+  *out = nullptr;
+  BATCH_TRY(cudaSetDevice(device));
+  frehd_batch *b = new frehd_batch();
+  b->device = device;
+  b->budget = hbm_budget_bytes;
+  b->cells_per_cta = cells_per_cta;
+  int rc = cg1_batch_capacity(device, &b->capacity);
+  if (!rc && cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+    rc = fail(FREHD_ERR_CUDA, "stream creation failed");
+  if (rc) {
+    delete b;
+    return rc;
+  }
+  *out = b;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_batch_destroy(frehd_batch *b) {
+  if (!b) return FREHD_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (Slot &s : b->slots)
+    if (s.d) {  // hand back in a consistent state before the caller destroys it
+      int cur = 0;
+      cudaMemcpy(&cur, &s.d->sc->cur, sizeof(int), cudaMemcpyDeviceToHost);
+      s.d->cur = cur & 1;
+      s.d->in_batch = 0;
+    }
+  drop_graph(b);
+  b->views2.release();
+  b->maps.release();
+  b->tiles.release();
+  b->fins.release();
+  b->job_start.release();
+  b->jobs.release();
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_batch_admit(frehd_batch *b, frehd_domain *d, int t0, int *slot) {
+  clear_error();
+  if (!b || !d || !slot) return fail(FREHD_ERR_INVALID, "null argument");
+  if (!d->ready) return fail(FREHD_ERR_STATE, "domain has no state (init or upload first)");
+  if (d->in_batch) return fail(FREHD_ERR_STATE, "domain is already in a batch");
+  if (d->device != b->device) return fail(FREHD_ERR_INVALID, "domain and batch are on different devices");
+  if (b->used + d->bytes > b->budget)
+    return fail(FREHD_ERR_NOMEM, "batch memory budget: %lld + %lld bytes > %lld", b->used, d->bytes, b->budget);
+  if (ctas_needed(b, d) > b->capacity)
+    return fail(FREHD_ERR_NOMEM, "batch CTA capacity: %d CTAs needed, %d available", ctas_needed(b, d),
+                b->capacity);
+  BATCH_TRY(cudaSetDevice(b->device));
+  // the domain's own queued work (init, uploads) ends before the batch uses it
+  BATCH_TRY(cudaStreamSynchronize(d->stream));
+  const int cur = d->cur;
+  BATCH_TRY(cudaMemcpy(&d->sc->cur, &cur, sizeof(int), cudaMemcpyHostToDevice));
+  BATCH_TRY(cudaMemcpy(&d->sc->tt, &t0, sizeof(int), cudaMemcpyHostToDevice));
+  int s = -1;
+  for (size_t k = 0; k < b->slots.size(); ++k)
+    if (!b->slots[k].d) {
+      s = (int)k;
+      break;
+    }
+  if (s < 0) {
+    s = (int)b->slots.size();
+    b->slots.push_back(Slot{});
+  }
+  b->slots[s].d = d;
+  b->slots[s].steps = 0;
+  b->used += d->bytes;
+  d->in_batch = 1;
+  b->dirty = true;
+  *slot = s;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_batch_release(frehd_batch *b, int slot, frehd_domain **out) {
+  clear_error();
+  if (!b || slot < 0 || slot >= (int)b->slots.size() || !b->slots[slot].d)
+    return fail(FREHD_ERR_INVALID, "no domain in slot %d", slot);
+  BATCH_TRY(cudaSetDevice(b->device));
+  BATCH_TRY(cudaStreamSynchronize(b->stream));
+  frehd_domain *d = b->slots[slot].d;
+  int cur = 0;
+  BATCH_TRY(cudaMemcpy(&cur, &d->sc->cur, sizeof(int), cudaMemcpyDeviceToHost));
+  d->cur = cur & 1;
+  d->in_batch = 0;
+  b->used -= d->bytes;
+  b->slots[slot].d = nullptr;
+  b->dirty = true;
+  if (out) *out = d;
+  // the last step's statistics (written by k_finish_batch) into d->last
+  return domain_read_stats(d);
+}
+
+extern "C" int frehd_batch_step(frehd_batch *b) {
+  if (!b) return fail(FREHD_ERR_INVALID, "null batch");
+  BATCH_TRY(cudaSetDevice(b->device));
+  if (b->dirty) {
+    const int rc = rebuild(b);
+    if (rc) return rc;
+  }
+  if (b->nfin == 0) return FREHD_OK;
+  capture(b);
+  if (b->graph_live) {
+    BATCH_TRY(cudaGraphLaunch(b->graph, b->stream));
+  } else {
+    const int rc = launch_step(b);
+    if (rc) return rc;
+  }
+  for (Slot &s : b->slots)
+    if (s.d) ++s.steps;
+  ++b->steps;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_batch_sync(frehd_batch *b) {
+  if (!b) return fail(FREHD_ERR_INVALID, "null batch");
+  BATCH_TRY(cudaSetDevice(b->device));
+  BATCH_TRY(cudaStreamSynchronize(b->stream));
+  return FREHD_OK;
+}
+
+extern "C" int frehd_batch_info(frehd_batch *b, frehd_batch_info_t *out) {
+  if (!b || !out) return fail(FREHD_ERR_INVALID, "null argument");
+  if (b->dirty) {
+    BATCH_TRY(cudaSetDevice(b->device));
+    const int rc = rebuild(b);
+    if (rc) return rc;
+  }
+  int n = 0;
+  for (const Slot &s : b->slots) n += s.d != nullptr;
+  out->domains = n;
+  out->cg_ctas = b->nctas;
+  out->cg_capacity = b->capacity;
+  out->tiles = b->ntiles;
+  out->graph = b->graph_live;
+  out->bytes_used = b->used;
+  out->bytes_budget = b->budget;
+  out->steps = b->steps;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_batch_stream(frehd_batch *b, void **stream) {
+  if (!b || !stream) return fail(FREHD_ERR_INVALID, "null argument");
+  *stream = b->stream;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_batch_set_graph(frehd_batch *b, int on) {
+  if (!b) return fail(FREHD_ERR_INVALID, "null batch");
+  drop_graph(b);
+  b->use_graph = on ? 1 : 0;
+  return FREHD_OK;
+}

@@ -9,6 +9,7 @@
 
 #include "cg1.h"
 #include "domain.cuh"
+#include "domain_host.h"
 #include "frehd_internal.h"
 #include "kernels.cuh"
 
@@ -22,54 +23,6 @@ using namespace frehd;
                   __FILE__, __LINE__);                                                 \
   } while (0)
 
-struct frehd_domain {
-  frehd_config cfg;
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  Grid gr;
-  Params p;
-  long N = 0, T = 0;
-  double *surf[2] = {}, *depth[2] = {}, *S[2] = {};
-  int *ind[2] = {};
-  double *u = nullptr, *v = nullptr, *CDXP = nullptr, *CDYP = nullptr, *CFLx = nullptr,
-         *CFLy = nullptr;
-  double *V = nullptr, *Z = nullptr, *Nx = nullptr, *Oy = nullptr, *Vx = nullptr, *Vy = nullptr,
-         *Zx = nullptr, *Zy = nullptr;
-  double *bottomZ = nullptr, *bottomXP = nullptr, *bottomYP = nullptr;
-  double *EnXP = nullptr, *EnYP = nullptr, *Gx = nullptr, *Gy = nullptr, *Ct = nullptr,
-         *b = nullptr;
-  double *Hx = nullptr, *Hy = nullptr;
-  double *x = nullptr, *r = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr;
-  double *cellV = nullptr, *Sm = nullptr, *Fuu = nullptr, *Fvv = nullptr;
-  unsigned char *rmv = nullptr;
-  int *fix_list = nullptr;
-  double *partials = nullptr;
-  long npartials = 0;
-  double *tide = nullptr;
-  int ntide = 0;
-  double *tables = nullptr, *zf = nullptr;
-  Scratch *sc = nullptr;
-  StepOut *out = nullptr;
-  StepOut *out_host = nullptr;  // pinned
-  double *stage = nullptr;      // device staging, T doubles
-  double *stage2 = nullptr;
-  int cur = 0;
-  int x0_mode = FREHD_X0_ZERO;
-  int cg_blocks = 1;
-  int cg_schedule = FREHD_CG_SINGLE_SWEEP;
-  int eliminate = 0;  // FREHD_DECOUPLED_ELIMINATED selected
-  Cg1Maps cg1_maps{};
-  Cg1Maps *cg1_maps_dev = nullptr;  // device copy read by the kernel
-  int cg1_blocks_n = 1;
-  int geom_set = 0, ready = 0;
-  frehd_step_stats last{};
-  std::vector<void *> allocs;
-  // profiling: one event before each kernel of a step plus one after
-  int profiling = 0;
-  std::vector<cudaEvent_t> ev;
-  frehd_kernel_times times{};
-  long long iters_at_prof_start = 0;
-};
 
 namespace {
 
@@ -84,6 +37,7 @@ int dalloc(frehd_domain *d, T **p, long n) {
   }
   cudaMemsetAsync(q, 0, sizeof(T) * (size_t)std::max(n, 1L), d->stream);
   d->allocs.push_back(q);
+  d->bytes += (long long)(sizeof(T) * (size_t)std::max(n, 1L));
   *p = (T *)q;
   return FREHD_OK;
 }
@@ -111,11 +65,11 @@ int check_config(const frehd_config *c) {
   return FREHD_OK;
 }
 
-View make_view(const frehd_domain *d) {
+View make_view_at(const frehd_domain *d, int cur) {
   View w;
   w.p = d->p;
   w.gr = d->gr;
-  const int c = d->cur, n = d->cur ^ 1;
+  const int c = cur, n = cur ^ 1;
   w.surf_cur = d->surf[c]; w.surf_nxt = d->surf[n];
   w.depth_cur = d->depth[c]; w.depth_nxt = d->depth[n];
   w.S_cur = d->S[c]; w.S_nxt = d->S[n];
@@ -133,6 +87,8 @@ View make_view(const frehd_domain *d) {
   w.sc = d->sc;
   return w;
 }
+
+View make_view(const frehd_domain *d) { return make_view_at(d, d->cur); }
 
 dim3 tile_grid(const frehd_domain *d) {
   return dim3((d->gr.nx + 31) / 32, (d->gr.ny + 7) / 8);
@@ -234,6 +190,9 @@ int launch_update(frehd_domain *d, const View &w, cudaEvent_t *ev = nullptr) {
 }
 
 }  // namespace
+
+View frehd::domain_view(const frehd_domain *d, int cur) { return make_view_at(d, cur); }
+int frehd::domain_read_stats(frehd_domain *d) { return read_stats(d); }
 
 // ---------------------------------------------------------------- lifecycle
 extern "C" int frehd_device_count(int *count) {
@@ -362,6 +321,7 @@ extern "C" int frehd_domain_set_tables(frehd_domain *d, int Ne, const double *ta
   CUDA_TRY(cudaMemcpyAsync(d->tables, tables, bytes, cudaMemcpyHostToDevice, d->stream));
   d->p.geom_fine = 0;
   d->p.tab = d->tables;
+  d->bytes += (long long)bytes;
   d->geom_set = 1;
   return FREHD_OK;
 }
@@ -383,6 +343,7 @@ extern "C" int frehd_domain_set_fine_bottoms(frehd_domain *d, int r, const doubl
                              sizeof(double) * cols, rows, cudaMemcpyHostToDevice, d->stream));
   d->p.geom_fine = 1;
   d->p.zf = d->zf;
+  d->bytes += (long long)(sizeof(double) * rows * cols);
   d->p.fpitch = cols;
   d->p.r = r;
   d->geom_set = 1;
@@ -423,6 +384,7 @@ extern "C" int frehd_domain_set_cg_schedule(frehd_domain *d, int schedule) {
 
 // ---------------------------------------------------------------- state I/O
 extern "C" int frehd_domain_upload_state(frehd_domain *d, const frehd_state *st) {
+  if (d && d->in_batch) return fail(FREHD_ERR_STATE, "the domain is stepped by a batch (release it first)");
   if (!d || !st) return fail(FREHD_ERR_INVALID, "null argument");
   CUDA_TRY(cudaSetDevice(d->device));
   const long N = d->N, T = d->T;
@@ -470,6 +432,7 @@ extern "C" int frehd_domain_upload_state(frehd_domain *d, const frehd_state *st)
 }
 
 extern "C" int frehd_domain_download_state(frehd_domain *d, frehd_state *st) {
+  if (d && d->in_batch) return fail(FREHD_ERR_STATE, "the domain is stepped by a batch (release it first)");
   if (!d || !st) return fail(FREHD_ERR_INVALID, "null argument");
   CUDA_TRY(cudaSetDevice(d->device));
   const long N = d->N, T = d->T;
@@ -638,6 +601,7 @@ extern "C" int frehd_domain_init(frehd_domain *d, const double *bottom, const do
 
 // ---------------------------------------------------------------- stepping
 extern "C" int frehd_domain_phase(frehd_domain *d, int phase, int tt, const double *x_ext) {
+  if (d && d->in_batch) return fail(FREHD_ERR_STATE, "the domain is stepped by a batch (release it first)");
   if (!d) return fail(FREHD_ERR_INVALID, "null domain");
   if (!d->ready) return fail(FREHD_ERR_STATE, "domain has no state (init or upload first)");
   CUDA_TRY(cudaSetDevice(d->device));
@@ -670,6 +634,7 @@ extern "C" int frehd_domain_phase(frehd_domain *d, int phase, int tt, const doub
 }
 
 extern "C" int frehd_domain_run(frehd_domain *d, int t0, int nsteps) {
+  if (d && d->in_batch) return fail(FREHD_ERR_STATE, "the domain is stepped by a batch (release it first)");
   if (!d) return fail(FREHD_ERR_INVALID, "null domain");
   if (!d->ready) return fail(FREHD_ERR_STATE, "domain has no state (init or upload first)");
   if (nsteps <= 0) return FREHD_OK;
@@ -714,7 +679,8 @@ extern "C" int frehd_domain_run(frehd_domain *d, int t0, int nsteps) {
   return FREHD_OK;
 }
 
-extern "C" int frehd_domain_step(frehd_domain *d, int tt) { return frehd_domain_run(d, tt, 1); }
+extern "C" int frehd_domain_step(frehd_domain *d, int tt) {
+  if (d && d->in_batch) return fail(FREHD_ERR_STATE, "the domain is stepped by a batch (release it first)"); return frehd_domain_run(d, tt, 1); }
 
 extern "C" int frehd_domain_download_system(frehd_domain *d, double *GnCt, double *GnXP,
                                             double *GnXM, double *GnYP, double *GnYM, double *z) {

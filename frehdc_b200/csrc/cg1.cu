@@ -164,22 +164,19 @@ __device__ __forceinline__ int ring_pos(int t) {
 
 }  // namespace
 
-__global__ void __launch_bounds__(kCgThreads, 1)
-    k_cg1(View w, const Cg1Maps *__restrict__ m, int x0_surface, int eliminate) {
+// One solve of domain w by a group of nb CTAs, of which this CTA is number
+// `rank`.  smem/bars: this CTA's two stages and their mbarriers (initialised by
+// the kernel); seq counts the tiles this CTA consumed so far, across solves, and
+// gives each wait its mbarrier phase.  Returns false after an error (status set).
+static __device__ __forceinline__ bool cg1_solve(const View &w, const Cg1Maps *__restrict__ m, int x0_surface, int eliminate,
+                          unsigned rank, unsigned nb, unsigned char *smem, unsigned long long *bars,
+                          unsigned &seq) {
   Scratch *sc = w.sc;
-  if (*(volatile int *)&sc->status != FREHD_OK) return;
-  // The dynamic region starts after the static shared data (this kernel's and
-  // grid_allreduce's), which only guarantees 16-byte alignment: round the base
-  // up to 128 bytes at run time (the launch requests 128 bytes of slack).
-  extern __shared__ unsigned char smem_raw[];
-  unsigned char *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
-  unsigned long long *bars = reinterpret_cast<unsigned long long *>(smem + 2 * kStageBytes);
   __shared__ int s_ok;
   const Grid g = w.gr;
   const Params &p = w.p;
   const int nx = g.nx, ny = g.ny;
   const long pitch = g.pitch;
-  const unsigned nb = gridDim.x;
   TileIt ti;
   ti.ntx = (nx + CTX - 1) / CTX;
   ti.nty = (ny + CTY - 1) / CTY;
@@ -187,24 +184,13 @@ __global__ void __launch_bounds__(kCgThreads, 1)
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   double *partials = w.partials, *totals = w.partials + kRedStride * (long)nb;
   const double *Ct = w.Ct, *Gx = w.Gx, *Gy = w.Gy;
-
-  // TMA destinations 128-byte aligned, mbarriers 8-byte aligned, tensor maps
-  // 64-byte aligned: refuse (every block alike) otherwise
-  if ((smem_u32(smem) & 127u) || (smem_u32(bars) & 7u) ||
-      (reinterpret_cast<unsigned long long>(m) & 63ull)) {
-    if (threadIdx.x == 0) set_status(sc, FREHD_ERR_CUDA);
-    return;
-  }
+  double *const X = w.x;  // read and written per cell in the sweep: kept in a register
   if (threadIdx.x == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     // the maps were written to global memory by a host copy: make them visible to the TMA unit
     const CUtensorMap *maps = &m->r[0];
     for (int q = 0; q < 6; ++q)
       asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(maps + q) : "memory");
   }
-  __syncthreads();
 
   // A solve of the assembled (non-symmetric) matrix can stall: ||r|| stops
   // falling above eps*||b|| and laspack's CGIter runs on to maxIter.  When ||r||
@@ -214,7 +200,6 @@ __global__ void __launch_bounds__(kCgThreads, 1)
   // read by all between grid reductions)
   __shared__ double s_best;
   __shared__ int s_best_it, s_it_all, s_fallback;
-  unsigned seq = 0;  // tiles consumed by this block: stage = seq & 1, phase parity = (seq >> 1) & 1
   int it = 0;
   double rr = 0.0, bnorm = 0.0;
   if (threadIdx.x == 0) {
@@ -224,7 +209,7 @@ __global__ void __launch_bounds__(kCgThreads, 1)
   for (int attempt = 0;; ++attempt) {
     const int elim = eliminate | (attempt > 0);
     // ---- setup 1: scaled couplings, x~0 = sqrt|Ct| x0, p_{-1} = 0
-    for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb) {
+    for (int tile = rank; tile < ti.ntiles; tile += nb) {
       int i0, j0;
       tile_origin(ti, tile, &i0, &j0);
       const int j = j0 + ty;
@@ -250,13 +235,13 @@ __global__ void __launch_bounds__(kCgThreads, 1)
     }
     {
       double none[1] = {0};
-      if (!grid_allreduce<1, kRedStride>(none, sc, partials, totals, nb)) return;
+      if (!grid_allreduce<1, kRedStride>(none, sc, partials, totals, nb, rank)) return false;
     }
 
     // ---- setup 2: r0 = b - A x0 (eliminated: decoupled neighbours at their exact b/|Ct|),
     //      r~0 = r0/sqrt|Ct|
     double acc[3] = {0, 0, 0};
-    for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb) {
+    for (int tile = rank; tile < ti.ntiles; tile += nb) {
       int i0, j0;
       tile_origin(ti, tile, &i0, &j0);
       const int j = j0 + ty;
@@ -287,7 +272,7 @@ __global__ void __launch_bounds__(kCgThreads, 1)
         }
       }
     }
-    if (!grid_allreduce<3, kRedStride>(acc, sc, partials, totals, nb)) return;
+    if (!grid_allreduce<3, kRedStride>(acc, sc, partials, totals, nb, rank)) return false;
     double gamma = acc[0];
     rr = acc[1];
     bnorm = sqrt(acc[2]);
@@ -297,7 +282,7 @@ __global__ void __launch_bounds__(kCgThreads, 1)
     {
       double d0[1] = {0};
       Stage s(smem);
-      for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb) {
+      for (int tile = rank; tile < ti.ntiles; tile += nb) {
         int i0, j0;
         tile_origin(ti, tile, &i0, &j0);
         __syncthreads();
@@ -323,7 +308,7 @@ __global__ void __launch_bounds__(kCgThreads, 1)
         }
       }
       __syncthreads();
-      if (!grid_allreduce<1, kRedStride>(d0, sc, partials, totals, nb)) return;
+      if (!grid_allreduce<1, kRedStride>(d0, sc, partials, totals, nb, rank)) return false;
       delta = d0[0];
     }
 
@@ -350,9 +335,9 @@ __global__ void __launch_bounds__(kCgThreads, 1)
       // generic writes of the previous sweep (all blocks) come before this sweep's TMA reads
       if (threadIdx.x == 0) {
         asm volatile("fence.proxy.async.global;" ::: "memory");
-        issue_tile(m, cur, ti, blockIdx.x, smem + (seq & 1) * kStageBytes, &bars[seq & 1]);
+        issue_tile(m, cur, ti, rank, smem + (seq & 1) * kStageBytes, &bars[seq & 1]);
       }
-      for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb, ++seq) {
+      for (int tile = rank; tile < ti.ntiles; tile += nb, ++seq) {
         const int st = seq & 1;
         const int next = tile + (int)nb;
         if (threadIdx.x == 0 && next < ti.ntiles)
@@ -367,7 +352,7 @@ __global__ void __launch_bounds__(kCgThreads, 1)
           const int i = i0 + c * 32 + tx;
           const bool in = i < nx && j < ny;
           const long k = g.at(in ? i : 0, in ? j : 0);
-          xs[c] = w.x[k];
+          xs[c] = X[k];
           ds[c] = fabs(Ct[k]);
         }
         if (threadIdx.x == 0) s_ok = mbar_wait(&bars[st], (seq >> 1) & 1, kBarrierTimeoutNs);
@@ -378,7 +363,7 @@ __global__ void __launch_bounds__(kCgThreads, 1)
             set_status(sc, FREHD_ERR_TIMEOUT);
             if (next < ti.ntiles) mbar_wait(&bars[st ^ 1], ((seq + 1) >> 1) & 1, kBarrierTimeoutNs);
           }
-          return;
+          return false;
         }
         mbar_wait(&bars[st], (seq >> 1) & 1, kBarrierTimeoutNs);  // completed: acquire in every thread
         Stage s(smem + st * kStageBytes);
@@ -434,7 +419,7 @@ __global__ void __launch_bounds__(kCgThreads, 1)
             red[3] += pc * wv;
             red[5] += ds[c] * (u * u);
             const long k = g.at(i, j);
-            w.x[k] = xs[c] + alpha * pc;
+            X[k] = xs[c] + alpha * pc;
             rn_out[k] = u;
             pn_out[k] = pc;
           }
@@ -443,7 +428,7 @@ __global__ void __launch_bounds__(kCgThreads, 1)
       }
       // this thread's global writes before the next sweep's TMA reads (other blocks)
       asm volatile("fence.proxy.async.global;" ::: "memory");
-      if (!grid_allreduce<6, kRedStride>(red, sc, partials, totals, nb)) return;
+      if (!grid_allreduce<6, kRedStride>(red, sc, partials, totals, nb, rank)) return false;
       gamma_old = gamma;
       gamma = red[0];
       delta = red[1];
@@ -473,7 +458,7 @@ __global__ void __launch_bounds__(kCgThreads, 1)
   }  // attempt
 
   // ---- x = x~ / sqrt|Ct| (each block its own tiles)
-  for (int tile = blockIdx.x; tile < ti.ntiles; tile += nb) {
+  for (int tile = rank; tile < ti.ntiles; tile += nb) {
     int i0, j0;
     tile_origin(ti, tile, &i0, &j0);
     const int j = j0 + ty;
@@ -486,13 +471,100 @@ __global__ void __launch_bounds__(kCgThreads, 1)
       }
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (rank == 0 && threadIdx.x == 0) {
     sc->cg_iters = s_it_all;
     sc->cg_fallback = s_fallback;
     sc->cg_rr = rr;
     sc->cg_bb = bnorm * bnorm;
   }
+  return true;
 }
+
+// Dynamic shared memory of one CTA: two stages and two mbarriers, the base
+// rounded up to 128 bytes (the region after the static shared data is only
+// 16-byte aligned; the launch requests 128 bytes of slack).  False (and the
+// status set on `sc`) if an alignment the TMA needs does not hold.
+static __device__ __forceinline__ bool cg1_smem(unsigned char *smem_raw, unsigned char **smem,
+                                         unsigned long long **bars) {
+  *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  *bars = reinterpret_cast<unsigned long long *>(*smem + 2 * kStageBytes);
+  if ((smem_u32(*smem) & 127u) || (smem_u32(*bars) & 7u)) return false;
+  if (threadIdx.x == 0) {
+    mbar_init(&(*bars)[0], 1);
+    mbar_init(&(*bars)[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  return true;
+}
+
+__global__ void __launch_bounds__(kCgThreads, 1)
+    k_cg1(View w, const Cg1Maps *__restrict__ m, int x0_surface, int eliminate) {
+  if (*(volatile int *)&w.sc->status != FREHD_OK) return;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char *smem;
+  unsigned long long *bars;
+  // TMA destinations 128-byte aligned, mbarriers 8-byte aligned, tensor maps
+  // 64-byte aligned: refuse (every block alike) otherwise
+  if (!cg1_smem(smem_raw, &smem, &bars) || (reinterpret_cast<unsigned long long>(m) & 63ull)) {
+    if (threadIdx.x == 0) set_status(w.sc, FREHD_ERR_CUDA);
+    return;
+  }
+  // the solve reads the view from shared memory (fewer live registers than the
+  // parameter copy)
+  __shared__ View s_view;
+  {
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(&w);
+    unsigned long long *dst = reinterpret_cast<unsigned long long *>(&s_view);
+    for (int e = threadIdx.x; e < (int)(sizeof(View) / 8); e += blockDim.x) dst[e] = src[e];
+  }
+  __syncthreads();
+  unsigned seq = 0;
+  cg1_solve(s_view, m, x0_surface, eliminate, blockIdx.x, gridDim.x, smem, bars, seq);
+}
+
+// Batched solve: CTA c runs jobs[job_start[c] .. job_start[c+1]) in order, each
+// one CTA's share of one domain's solve (rank `rank` of a group of `nb` CTAs,
+// all co-resident in this cooperative launch; a CTA of a multi-CTA group runs
+// no other job).  Each domain's view is taken at its current parity.
+__global__ void __launch_bounds__(kCgThreads, 1)
+    k_cg1_batch(const View *__restrict__ views2, const Cg1Maps *const *__restrict__ maps,
+                const int *__restrict__ job_start, const CgJob *__restrict__ jobs) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ View s_view;
+  __shared__ int s_cur;
+  unsigned char *smem;
+  unsigned long long *bars;
+  const int q0 = job_start[blockIdx.x], q1 = job_start[blockIdx.x + 1];
+  const bool aligned = cg1_smem(smem_raw, &smem, &bars);
+  unsigned seq = 0;
+  for (int q = q0; q < q1; ++q) {
+    const CgJob jb = jobs[q];
+    __syncthreads();  // the previous job is done with s_view
+    if (threadIdx.x == 0) s_cur = *(volatile int *)&views2[2 * jb.d].sc->cur;
+    __syncthreads();
+    {
+      const unsigned long long *src =
+          reinterpret_cast<const unsigned long long *>(views2 + 2 * jb.d + s_cur);
+      unsigned long long *dst = reinterpret_cast<unsigned long long *>(&s_view);
+      for (int e = threadIdx.x; e < (int)(sizeof(View) / 8); e += blockDim.x) dst[e] = src[e];
+    }
+    __syncthreads();
+    if (*(volatile int *)&s_view.sc->status != FREHD_OK) continue;
+    if (!aligned || (reinterpret_cast<unsigned long long>(maps[jb.d]) & 63ull)) {
+      if (threadIdx.x == 0) set_status(s_view.sc, FREHD_ERR_CUDA);
+      continue;
+    }
+    if (!cg1_solve(s_view, maps[jb.d], jb.flags & 1, (jb.flags >> 1) & 1, jb.rank, jb.nb, smem, bars,
+                   seq)) {
+      // this CTA's later jobs are not run: mark their domains failed
+      for (int r = q + 1; r < q1; ++r)
+        if (threadIdx.x == 0) set_status(views2[2 * jobs[r].d].sc, FREHD_ERR_TIMEOUT);
+      return;
+    }
+  }
+}
+
 
 // ---------------------------------------------------------------- host side
 
@@ -554,6 +626,27 @@ int cg1_blocks(int device, const Grid &g, int *blocks) {
   const long ntiles = (long)((g.nx + CTX - 1) / CTX) * ((g.ny + CTY - 1) / CTY);
   const long cap = (long)nsm * per;
   *blocks = (int)(ntiles < cap ? ntiles : cap);
+  return FREHD_OK;
+}
+
+int cg1_batch_capacity(int device, int *ctas) {
+  static const size_t smem = cg1_smem_bytes();
+  cudaError_t e = cudaFuncSetAttribute(k_cg1_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return fail(FREHD_ERR_CUDA, "k_cg1_batch shared memory: %s", cudaGetErrorString(e));
+  int nsm = 0, per = 0;
+  e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg1_batch, kCgThreads, smem);
+  if (e != cudaSuccess) return fail(FREHD_ERR_CUDA, "k_cg1_batch occupancy: %s", cudaGetErrorString(e));
+  *ctas = nsm * (per > 0 ? per : 0);
+  return *ctas > 0 ? FREHD_OK : fail(FREHD_ERR_CUDA, "k_cg1_batch does not fit on an SM");
+}
+
+int cg1_launch_batch(const View *views2, const Cg1Maps *const *maps, const int *job_start,
+                     const CgJob *jobs, int nctas, cudaStream_t stream) {
+  void *args[] = {&views2, &maps, &job_start, &jobs};
+  cudaError_t e = cudaLaunchCooperativeKernel((void *)k_cg1_batch, dim3(nctas), dim3(kCgThreads), args,
+                                              cg1_smem_bytes(), stream);
+  if (e != cudaSuccess) return fail(FREHD_ERR_CUDA, "k_cg1_batch launch: %s", cudaGetErrorString(e));
   return FREHD_OK;
 }
 

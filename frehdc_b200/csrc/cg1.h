@@ -27,6 +27,19 @@ int cg1_launch(const View &w, const Cg1Maps *m_dev, int blocks, int x0_surface, 
 // Partial sums per block the single-sweep CG keeps in the partials buffer.
 constexpr int kCg1PartialStride = 8;
 
+// One CTA's share of one domain's solve in a batched launch.
+struct CgJob {
+  int d;      // domain slot (views2[2*d + parity])
+  int rank;   // this CTA's rank in the domain's group
+  int nb;     // CTAs of the group (all co-resident)
+  int flags;  // bit 0: x0 = surface; bit 1: decoupled rows eliminated
+};
+// Launch the batched solve: nctas CTAs, CTA c runs jobs[job_start[c] .. job_start[c+1]).
+int cg1_launch_batch(const View *views2, const Cg1Maps *const *maps, const int *job_start,
+                     const CgJob *jobs, int nctas, cudaStream_t stream);
+// CTAs of the batched solve that fit on the device at once.
+int cg1_batch_capacity(int device, int *ctas);
+
 }  // namespace frehd
 
 #endif

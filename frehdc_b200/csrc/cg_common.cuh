@@ -24,11 +24,14 @@ __device__ __forceinline__ unsigned long long gtimer_ns() {
 
 __device__ __forceinline__ double ld(const double *a, long k) { return __ldcg(a + k); }
 
-// Sum of NV values over all threads of all blocks, identical in every block,
-// and a grid barrier.  partials: STRIDE doubles per block; totals: NV doubles.
+// Sum of NV values over all threads of the nblocks blocks that share `sc`,
+// identical in every block, and a barrier among them.  rank: this block's
+// number among them (blockIdx.x when the grid is one group).  partials: STRIDE
+// doubles per block; totals: NV doubles.
 template <int NV, int STRIDE = 4>
-__device__ __forceinline__ bool grid_allreduce(double (&v)[NV], Scratch *sc, double *partials, double *totals,
-                               unsigned nblocks) {
+static __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], Scratch *sc, double *partials,
+                                                      double *totals, unsigned nblocks,
+                                                      unsigned rank = blockIdx.x) {
   static_assert(NV <= STRIDE, "NV values per block must fit the partials stride");
   __shared__ double sh[STRIDE][NWARP];
   __shared__ int s_last, s_ok;
@@ -45,7 +48,7 @@ __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], Scratch *sc, dou
     for (int m = 0; m < NV; ++m) {
       double a = 0;
       for (int q = 0; q < NWARP; ++q) a += sh[m][q];
-      partials[STRIDE * blockIdx.x + m] = a;
+      partials[STRIDE * rank + m] = a;
     }
     // the generation can only move once every block (this one too) arrived
     my_gen = *(volatile unsigned *)&sc->bar_gen;

@@ -75,6 +75,7 @@ struct Scratch {
   int n_cfl_warn;
   int n_fix;                        // scalar-singularity cells queued for the fix-up
   int cg_fallback;                  // 1: the last solve stalled and was redone in eliminated form
+  int cur;                          // batched stepping: which ping-pong half holds the state
   double cg_rr, cg_bb;              // ||r||^2, ||b||^2 at CG exit
   unsigned long long max_cflx_bits, max_cfly_bits;  // positive doubles as ordered bits
   double volume;

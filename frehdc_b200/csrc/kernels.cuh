@@ -36,6 +36,19 @@ __global__ void k_padded_to_ref(double *dst, const double *src, long n, int nx, 
 __global__ void k_ref_to_padded_int(int *dst, const int *src, long n, int nx, int ny, int pitch);
 __global__ void k_padded_to_ref_int(int *dst, const int *src, long n, int nx, int ny, int pitch);
 __global__ void k_fill(double *a, long n, double v);
+// Batched launches over many domains (views2[2*d + half]: domain d's view with
+// ping-pong half `half` current).
+struct BatchTile {
+  int d, bx, by, gx;  // domain slot, tile coordinates, the domain's tile-grid width
+};
+struct FinishJob {
+  int d, nblocks_vel;  // domain slot, its k_update_vel tile count
+  StepOut *out;
+};
+__global__ void k_explicit_batch(const View *views2, const BatchTile *tiles);
+__global__ void k_update_geo_batch(const View *views2, const BatchTile *tiles);
+__global__ void k_update_vel_batch(const View *views2, const BatchTile *tiles);
+__global__ void k_finish_batch(const View *views2, const FinishJob *jobs);
 __global__ void k_interp_velocity(View w, double *uuYP, double *vvXP);
 __global__ void k_system_to_ref(View w, double *GnCt, double *GnXP, double *GnXM, double *GnYP,
                                 double *GnYM, double *z, double *xs);

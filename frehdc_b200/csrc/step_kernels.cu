@@ -156,14 +156,13 @@ __device__ __forceinline__ double gface(double coef, double N, double Vf, double
 // A 32 x 8 block evaluates the explicit term of every x face and y face it
 // needs once: each thread its own east and north face, threads 0-31 the south
 // halo row's north faces and threads 32-39 the west halo column's east faces.
-__global__ void __launch_bounds__(TBX *TBY, 4) k_explicit(View w) {
-  if (*(volatile int *)&w.sc->status != FREHD_OK) return;  // a fatal step stops the run
+static __device__ __forceinline__ void explicit_tile(const View &w, int bx, int by) {
   const Params &p = w.p;
   const Grid &g = w.gr;
   __shared__ double sEx[TBY][TBX + 1], sDx[TBY][TBX + 1];  // x faces, column 0 = west halo
   __shared__ double sEy[TBY + 1][TBX], sDy[TBY + 1][TBX];  // y faces, row 0 = south halo
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TBX + tx;
-  const int i0 = blockIdx.x * TBX, j0 = blockIdx.y * TBY;
+  const int i0 = bx * TBX, j0 = by * TBY;
   const int i = i0 + tx, j = j0 + ty;
   const bool in = i < g.nx && j < g.ny;
   Ex ex{0.0, 0.0}, ey{0.0, 0.0};
@@ -235,6 +234,11 @@ __global__ void __launch_bounds__(TBX *TBY, 4) k_explicit(View w) {
   w.Gy[k] = (j == g.ny - 1) ? 0.0 : gyn;
   w.Ct[k] = iso ? -Ct : Ct;
   w.b[k] = b;
+}
+
+__global__ void __launch_bounds__(TBX *TBY, 4) k_explicit(View w) {
+  if (*(volatile int *)&w.sc->status != FREHD_OK) return;  // a fatal step stops the run
+  explicit_tile(w, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------- subgrid
@@ -385,14 +389,13 @@ __device__ NewSurf new_surface(const View &w, int i, int j) {
 #endif
 
 template <bool kInit>
-__global__ void __launch_bounds__(TBX *TBY, FREHD_GEO_MIN_BLOCKS) k_update_geo(View w) {
-  if (!kInit && *(volatile int *)&w.sc->status != FREHD_OK) return;
+static __device__ __forceinline__ void update_geo_tile(const View &w, int bx, int by) {
   const Params &p = w.p;
   const Grid &g = w.gr;
   __shared__ double sh_s[EY][EX], sh_Np[EY][EX], sh_Nm[EY][EX], sh_Op[EY][EX], sh_Om[EY][EX];
   __shared__ double sh_Vxp[EY][EX], sh_Vxm[EY][EX], sh_Vyp[EY][EX], sh_Vym[EY][EX];
   __shared__ double sh_V[EY][EX], sh_Z[EY][EX];
-  const int i0 = blockIdx.x * TBX, j0 = blockIdx.y * TBY;
+  const int i0 = bx * TBX, j0 = by * TBY;
   const int tid = threadIdx.y * TBX + threadIdx.x;
   // Each thread evaluates its own cell; threads 0..TBX-1 then evaluate the north
   // halo row (only Om, Vym, s are read from it) and threads TBX..TBX+TBY-1 the
@@ -532,6 +535,12 @@ __global__ void __launch_bounds__(TBX *TBY, FREHD_GEO_MIN_BLOCKS) k_update_geo(V
   for (int a = 0; a < 8; ++a) arr[a][k] = val[a];
 }
 
+template <bool kInit>
+__global__ void __launch_bounds__(TBX *TBY, FREHD_GEO_MIN_BLOCKS) k_update_geo(View w) {
+  if (!kInit && *(volatile int *)&w.sc->status != FREHD_OK) return;
+  update_geo_tile<kInit>(w, blockIdx.x, blockIdx.y);
+}
+
 template __global__ void k_update_geo<false>(View);
 template __global__ void k_update_geo<true>(View);
 
@@ -594,12 +603,12 @@ __device__ __forceinline__ unsigned long long dbits(double x) {
   return (unsigned long long)__double_as_longlong(x);
 }
 
-__global__ void __launch_bounds__(TBX *TBY) k_update_vel(View w) {
-  if (*(volatile int *)&w.sc->status != FREHD_OK) return;
+// gx: the domain's tile-grid width (the block's partial-sum slot is by*gx + bx)
+static __device__ __forceinline__ void update_vel_tile(const View &w, int bx, int by, int gx) {
   const Params &p = w.p;
   const Grid &g = w.gr;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = bx * TBX + threadIdx.x;
+  const int j = by * TBY + threadIdx.y;
   double cflx = 0, cfly = 0, vol = 0;
   int nwarn = 0;
   if (i < g.nx && j < g.ny) {
@@ -757,22 +766,27 @@ __global__ void __launch_bounds__(TBX *TBY) k_update_vel(View w) {
       my = fmax(my, sy[q]);
       nw += sw[q];
     }
-    w.partials[blockIdx.y * gridDim.x + blockIdx.x] = a;
+    w.partials[by * gx + bx] = a;
     if (mx > 0) atomicMax(&w.sc->max_cflx_bits, dbits(mx));
     if (my > 0) atomicMax(&w.sc->max_cfly_bits, dbits(my));
     if (nw) atomicAdd(&w.sc->n_cfl_warn, nw);
   }
 }
 
+__global__ void __launch_bounds__(TBX *TBY) k_update_vel(View w) {
+  if (*(volatile int *)&w.sc->status != FREHD_OK) return;
+  update_vel_tile(w, blockIdx.x, blockIdx.y, gridDim.x);
+}
+
 // ---------------------------------------------------------------- k_finish
 // The scalar singularity branch (subgrid.c:1700-1712) also lowers the surface
 // of the cell by its depth; cells are queued by k_update_vel and fixed here so
 // that no kernel reads a half-updated surface.  Then the step statistics.
-__global__ void k_finish(View w, int nblocks_vel, StepOut *out) {
+static __device__ __forceinline__ bool finish_block(const View &w, int nblocks_vel, StepOut *out) {
   const int tid = threadIdx.x;
   if (*(volatile int *)&w.sc->status != FREHD_OK) {  // step skipped or aborted
     if (tid == 0) out->status = w.sc->status;
-    return;
+    return false;
   }
   const int nfix = w.sc->n_fix;
   for (int q = tid; q < nfix; q += blockDim.x) {
@@ -815,6 +829,61 @@ __global__ void k_finish(View w, int nblocks_vel, StepOut *out) {
     if (out->status != FREHD_OK) sc->status = out->status;
     sc->tt = sc->tt + 1;
   }
+  return true;
+}
+
+__global__ void k_finish(View w, int nblocks_vel, StepOut *out) { finish_block(w, nblocks_vel, out); }
+
+// ---------------------------------------------------------------- batched launches
+// One block per table entry (domain slot, tile) over every domain of a batch.
+// Each block stages its domain's view, at the domain's current ping-pong half
+// (sc->cur, flipped by k_finish_batch), in shared memory.
+static __device__ __forceinline__ void stage_view(const View *views2, int d, View *sv, int *s_cur, int tid,
+                                           int nthr) {
+  if (tid == 0) *s_cur = *(volatile int *)&views2[2 * d].sc->cur;
+  __syncthreads();
+  const unsigned long long *src = reinterpret_cast<const unsigned long long *>(views2 + 2 * d + *s_cur);
+  unsigned long long *dst = reinterpret_cast<unsigned long long *>(sv);
+  for (int e = tid; e < (int)(sizeof(View) / 8); e += nthr) dst[e] = src[e];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(TBX *TBY, 4) k_explicit_batch(const View *views2, const BatchTile *tiles) {
+  __shared__ View sv;
+  __shared__ int s_cur;
+  const BatchTile t = tiles[blockIdx.x];
+  stage_view(views2, t.d, &sv, &s_cur, threadIdx.y * TBX + threadIdx.x, TBX * TBY);
+  if (*(volatile int *)&sv.sc->status != FREHD_OK) return;
+  explicit_tile(sv, t.bx, t.by);
+}
+
+__global__ void __launch_bounds__(TBX *TBY, FREHD_GEO_MIN_BLOCKS)
+    k_update_geo_batch(const View *views2, const BatchTile *tiles) {
+  __shared__ View sv;
+  __shared__ int s_cur;
+  const BatchTile t = tiles[blockIdx.x];
+  stage_view(views2, t.d, &sv, &s_cur, threadIdx.y * TBX + threadIdx.x, TBX * TBY);
+  if (*(volatile int *)&sv.sc->status != FREHD_OK) return;
+  update_geo_tile<false>(sv, t.bx, t.by);
+}
+
+__global__ void __launch_bounds__(TBX *TBY) k_update_vel_batch(const View *views2, const BatchTile *tiles) {
+  __shared__ View sv;
+  __shared__ int s_cur;
+  const BatchTile t = tiles[blockIdx.x];
+  stage_view(views2, t.d, &sv, &s_cur, threadIdx.y * TBX + threadIdx.x, TBX * TBY);
+  if (*(volatile int *)&sv.sc->status != FREHD_OK) return;
+  update_vel_tile(sv, t.bx, t.by, t.gx);
+}
+
+// One block per domain: k_finish's work, then the domain's ping-pong half flips.
+__global__ void k_finish_batch(const View *views2, const FinishJob *jobs) {
+  __shared__ View sv;
+  __shared__ int s_cur;
+  const FinishJob f = jobs[blockIdx.x];
+  stage_view(views2, f.d, &sv, &s_cur, threadIdx.x, blockDim.x);
+  const bool ran = finish_block(sv, f.nblocks_vel, f.out);
+  if (ran && threadIdx.x == 0) sv.sc->cur = s_cur ^ 1;
 }
 
 // ---------------------------------------------------------------- layout

@@ -330,6 +330,108 @@ class Domain:
         return s.value or 0
 
 
+class BatchInfo(C.Structure):
+    _fields_ = [("domains", C.c_int), ("cg_ctas", C.c_int), ("cg_capacity", C.c_int),
+                ("tiles", C.c_long), ("graph", C.c_int), ("bytes_used", C.c_longlong),
+                ("bytes_budget", C.c_longlong), ("steps", C.c_longlong)]
+
+
+def _declare_batch(L: C.CDLL) -> None:
+    if hasattr(L, "_batch_declared"):
+        return
+    if not hasattr(L, "_domain_declared"):
+        _declare_domain(L)
+        L._domain_declared = True
+    L.frehd_domain_footprint.argtypes = [C.POINTER(Config), C.c_int, C.POINTER(C.c_longlong)]
+    L.frehd_batch_create.argtypes = [C.c_int, C.c_longlong, C.c_double, C.POINTER(_vp)]
+    L.frehd_batch_destroy.argtypes = [_vp]
+    L.frehd_batch_admit.argtypes = [_vp, _vp, C.c_int, _ip]
+    L.frehd_batch_release.argtypes = [_vp, C.c_int, C.POINTER(_vp)]
+    L.frehd_batch_step.argtypes = [_vp]
+    L.frehd_batch_sync.argtypes = [_vp]
+    L.frehd_batch_info.argtypes = [_vp, C.POINTER(BatchInfo)]
+    L.frehd_batch_stream.argtypes = [_vp, C.POINTER(_vp)]
+    L.frehd_batch_set_graph.argtypes = [_vp, C.c_int]
+    L._batch_declared = True
+
+
+def footprint(cfg: dict, r: int) -> int:
+    """Device bytes one domain of this configuration holds (frehd_domain_footprint)."""
+    L = lib()
+    _declare_batch(L)
+    from .config import fill_struct
+    c = Config()
+    fill_struct(c, cfg)
+    out = C.c_longlong(0)
+    check(L.frehd_domain_footprint(C.byref(c), r, C.byref(out)), "frehd_domain_footprint")
+    return out.value
+
+
+class Batch:
+    """Many resident domains stepped together (frehd_batch_*): each admitted
+    Domain advances one step per step() call; release() hands it back."""
+
+    def __init__(self, budget_bytes: int, cells_per_cta: float, device: int = 0):
+        L = lib()
+        _declare_batch(L)
+        h = _vp()
+        check(L.frehd_batch_create(device, int(budget_bytes), float(cells_per_cta), C.byref(h)),
+              "frehd_batch_create")
+        self.h = h
+        self.members: dict[int, "Domain"] = {}
+
+    def admit(self, dom: "Domain", t0: int = 1) -> int:
+        slot = C.c_int(-1)
+        check(lib().frehd_batch_admit(self.h, dom.h, t0, C.byref(slot)), "frehd_batch_admit")
+        self.members[slot.value] = dom
+        return slot.value
+
+    def try_admit(self, dom: "Domain", t0: int = 1):
+        """The slot, or None when the budget or the CTA capacity is exhausted."""
+        try:
+            return self.admit(dom, t0)
+        except FrehdError as e:
+            if e.status == 4:
+                return None
+            raise
+
+    def release(self, slot: int) -> "Domain":
+        out = _vp()
+        check(lib().frehd_batch_release(self.h, slot, C.byref(out)), "frehd_batch_release")
+        return self.members.pop(slot)
+
+    def step(self):
+        check(lib().frehd_batch_step(self.h), "frehd_batch_step")
+
+    def sync(self):
+        check(lib().frehd_batch_sync(self.h), "frehd_batch_sync")
+
+    def info(self) -> dict:
+        i = BatchInfo()
+        check(lib().frehd_batch_info(self.h, C.byref(i)), "frehd_batch_info")
+        return {n: getattr(i, n) for n, _ in BatchInfo._fields_}
+
+    def stream(self) -> int:
+        s = _vp()
+        check(lib().frehd_batch_stream(self.h, C.byref(s)), "frehd_batch_stream")
+        return s.value or 0
+
+    def set_graph(self, on: bool):
+        check(lib().frehd_batch_set_graph(self.h, int(on)), "frehd_batch_set_graph")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().frehd_batch_destroy(self.h)
+            self.h = None
+            self.members.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def cg_solve_noalloc(nx: int, ny: int, Ct: int, Gx: int, Gy: int, b: int, x: int, eps: float,
                      max_iter: int, x0_from_x: bool = False, stream: int = 0,
                      wait: bool = True):

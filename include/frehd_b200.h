@@ -266,6 +266,50 @@ int frehd_cg_solve_noalloc(int nx, int ny, const double *Ct, const double *Gx, c
                            const double *b, double *x, double eps, int max_iter, int x0_from_x,
                            void *stream, int *iters, double *rel_residual);
 
+/* ------------------------------------------------------------ batches */
+/*
+ * Many resident domains stepped together (the batched form; no counterpart in
+ * the reference, whose driver runs one domain per process).  A domain is set up
+ * with the calls above, then admitted; while admitted, the batch steps it and
+ * the single-domain step/state calls refuse it (FREHD_ERR_STATE).  Every
+ * frehd_batch_step advances every admitted domain by one step with five kernel
+ * launches in total (replayed from a CUDA graph where the driver accepts the
+ * capture).  A domain's results do not depend on which other domains share the
+ * batch: its CG runs on round(cells / cells_per_cta) CTAs (at least
+ * one) whatever the mix.
+ */
+typedef struct frehd_batch frehd_batch;
+typedef struct frehd_batch_info_t {
+  int domains;             /* admitted domains */
+  int cg_ctas;             /* CTAs of the batched CG launch */
+  int cg_capacity;         /* CTAs the device holds at once for it */
+  long tiles;              /* stencil tiles per step over all domains */
+  int graph;               /* 1: steps replay a captured CUDA graph */
+  long long bytes_used, bytes_budget;
+  long long steps;         /* batch steps taken */
+} frehd_batch_info_t;
+
+/* Device memory a domain of this configuration holds, with r x r fine bottoms. */
+int frehd_domain_footprint(const frehd_config *cfg, int r, long long *bytes);
+/* cells_per_cta: cells of a domain per CTA of its CG (the packing granularity). */
+int frehd_batch_create(int device, long long hbm_budget_bytes, double cells_per_cta,
+                       frehd_batch **out);
+/* Domains still admitted are handed back to their owners (not destroyed). */
+int frehd_batch_destroy(frehd_batch *b);
+/* Admit a set-up domain; its next step is tt = t0.  FREHD_ERR_NOMEM when the
+ * memory budget or the CG's CTA capacity would be exceeded (the domain stays
+ * with the caller). */
+int frehd_batch_admit(frehd_batch *b, frehd_domain *d, int t0, int *slot);
+/* Hand a domain back (state and last-step statistics readable again). */
+int frehd_batch_release(frehd_batch *b, int slot, frehd_domain **d);
+/* One step of every admitted domain (queued on the batch's stream). */
+int frehd_batch_step(frehd_batch *b);
+int frehd_batch_sync(frehd_batch *b);
+int frehd_batch_info(frehd_batch *b, frehd_batch_info_t *out);
+int frehd_batch_stream(frehd_batch *b, void **stream);
+/* Replay steps from a captured CUDA graph (default 1) or launch them directly. */
+int frehd_batch_set_graph(frehd_batch *b, int on);
+
 #ifdef __cplusplus
 }
 #endif

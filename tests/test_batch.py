@@ -1,0 +1,102 @@
+"""The batched form (frehd_batch_*): many resident domains, one launch per
+sub-step over all of them.
+
+A domain's arithmetic in a batch is the single-domain step's: the stencil
+kernels run the same tile code, and its CG runs on round(cells/cells_per_cta)
+CTAs.  So with cells_per_cta = 1 (as many CTAs as the single-domain solve uses)
+a batch reproduces single-domain runs bit for bit, and for any fixed
+cells_per_cta a domain's result is the same alone and in a mix.
+"""
+import numpy as np
+import pytest
+
+from frehdc_b200 import native
+from tests.helpers import SPECS, deck_for, mismatches
+
+pytestmark = pytest.mark.gpu
+FIELDS = ["surf", "uuXP", "vvYP", "S", "depth", "cellV", "CDXP", "CDYP", "ind"]
+BUDGET = 8 << 30
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_gpu():
+    if native.device_count() < 1:
+        pytest.fail("no CUDA device visible: the GPU tests need a B200")
+
+
+def _run_batch(names, steps, scratch, cells_per_cta, graph=True):
+    b = native.Batch(BUDGET, cells_per_cta)
+    b.set_graph(graph)
+    doms = {}
+    for n in names:
+        d, _ = deck_for(n, str(scratch))
+        g = native.domain_from_deck(d, geometry="fine")
+        doms[n] = (g, b.admit(g, 1))
+    for _ in range(steps):
+        b.step()
+    info = b.info()
+    out = {}
+    for n, (g, slot) in doms.items():
+        b.release(slot)
+        out[n] = (g.download(FIELDS), g.stats())
+    b.close()
+    return out, info
+
+
+def test_batch_matches_single_domain_bitwise(scratch):
+    names = list(SPECS)
+    got, info = _run_batch(names, 12, scratch, cells_per_cta=1)
+    assert info["domains"] == 3
+    for n in names:
+        d, _ = deck_for(n, str(scratch))
+        g = native.domain_from_deck(d, geometry="fine")
+        assert g.run(1, 12) == 0
+        ref = g.download(FIELDS)
+        assert mismatches(got[n][0], ref, FIELDS) == [], n
+        st = g.stats()
+        assert got[n][1]["step"] == st["step"] == 12
+        assert got[n][1]["volume"] == st["volume"]
+
+
+@pytest.mark.parametrize("graph", [True, False])
+def test_same_alone_and_in_mix(graph, scratch):
+    names = list(SPECS)
+    mix, info = _run_batch(names, 10, scratch, cells_per_cta=1e9, graph=graph)
+    assert info["graph"] == (1 if graph else 0)
+    for n in names:
+        alone, _ = _run_batch([n], 10, scratch, cells_per_cta=1e9, graph=graph)
+        assert mismatches(mix[n][0], alone[n][0], FIELDS) == [], n
+
+
+def test_admission_by_budget(scratch):
+    d, _ = deck_for("wet48x40", str(scratch))
+    need = native.footprint(native.domain_from_deck(d).cfg, d.r)
+    g1 = native.domain_from_deck(d, geometry="fine")
+    g2 = native.domain_from_deck(d, geometry="fine")
+    b = native.Batch(int(1.5 * need), 1e9)
+    assert b.try_admit(g1) is not None
+    assert b.try_admit(g2) is None  # over the budget: refused, still usable alone
+    assert g2.run(1, 2) == 0
+    b.close()
+
+
+def test_served_results_equal_alone(scratch):
+    """Requests served with staggered arrivals (continuous batching) give the
+    same state as each request's domain stepped alone in a batch."""
+    from frehdc_b200 import serve
+    names = list(SPECS)
+    steps = {"wet48x40": 7, "dry40x36": 11, "dry37x29": 5}
+    results = {}
+
+    def done(req):
+        results[req.rid] = req.domain.download(FIELDS)
+
+    reqs = []
+    for k, n in enumerate(names):
+        d, _ = deck_for(n, str(scratch))
+        reqs.append(serve.Request(k, d, steps[n], arrival=0.002 * k))
+    res = serve.serve(reqs, BUDGET, 1e9, on_done=done)
+    assert res["requests"] == 3 and res["failed"] == 0
+    for k, n in enumerate(names):
+        alone, _ = _run_batch([n], steps[n], scratch, cells_per_cta=1e9)
+        assert mismatches(results[k], alone[n][0], FIELDS) == [], n

@@ -231,6 +231,8 @@ def run_gpu_arm(args):
     dom.set_tide(tide)
     dom.set_solver(native.X0_ZERO)
     dom.set_cg_schedule(SCHEDULES[args.cg_schedule])
+    if args.precision == "mixed":
+        dom.set_precision(native.PRECISION_MIXED, args.eps_inner)
     dom.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
     rc = dom.run(1, args.warmup)
     if rc != 0:
@@ -257,6 +259,9 @@ def run_gpu_arm(args):
     value = ws * N * args.steps / (t_max / 1e3)
     iters = kt["cg_iters"] / max(kt["steps"], 1)
     dom.set_profiling(False)
+    errors = None
+    if args.precision == "mixed":
+        errors = mixed_errors(dom, deck, cfg, tide, dev, args.warmup + args.steps, N)
     dom.close()
 
     # ---- e2e: through the C ABI from host buffers
@@ -269,7 +274,32 @@ def run_gpu_arm(args):
         torch.distributed.destroy_process_group()
     if rank != 0:
         return 0
-    return report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk)
+    return report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk, errors)
+
+
+def mixed_errors(dom, deck, cfg, tide, dev, steps, N):
+    """The mixed-precision domain's state after `steps` steps against an FP64
+    run of the same deck and steps."""
+    import numpy as np
+
+    from frehdc_b200 import native
+    ref = native.Domain(cfg, dev)
+    ref.set_fine_bottoms(deck.zf, deck.r)
+    ref.set_tide(tide)
+    ref.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
+    if ref.run(1, steps) != 0:
+        raise RuntimeError("FP64 comparison run failed")
+    names = ["surf", "uuXP", "vvYP", "S"]
+    a, b = dom.download(names), ref.download(names)
+    va, vb = dom.stats()["volume"], ref.stats()["volume"]
+    ref.close()
+
+    def rel(f):
+        return float(np.max(np.abs(a[f][:N] - b[f][:N])) / max(np.max(np.abs(b[f][:N])), 1e-300))
+    return {"steps": steps, "eta_max_abs_m": float(np.max(np.abs(a["surf"][:N] - b["surf"][:N]))),
+            "u_max_rel": rel("uuXP"), "v_max_rel": rel("vvYP"),
+            "S_max_abs": float(np.max(np.abs(a["S"][:N] - b["S"][:N]))),
+            "volume_rel": abs(va - vb) / abs(vb), "against": "the FP64 run of the same deck"}
 
 
 def run_e2e(args, deck, cfg, tide, dev, ws, N):
@@ -306,23 +336,26 @@ def run_e2e(args, deck, cfg, tide, dev, ws, N):
                         "read back, final state download"}
 
 
-def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk):
+def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk, errors=None):
     N = n * n
     peak, peak_kind = measured_hbm_peak()
     cg_launch_ms = kt["cg_ms"] / kt["steps"]
-    cg_bytes = N * (48.0 + 72.0 * iters)
+    per_it = 72.0 if args.precision == "fp64" else 32.0
+    cg_bytes = N * (48.0 + per_it * iters)
     achieved = cg_bytes / (cg_launch_ms / 1e3) / 1e9
     kname = {"single_sweep": "k_cg1 (persistent single-sweep Jacobi-PCG, one launch per step)",
              "two_phase": "k_cg (persistent two-phase Jacobi-PCG, one launch per step)"}
     roof = {"kernel": kname[args.cg_schedule], "bound": "hbm",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_kind": peak_kind, "traffic": None,
-            "bytes_model": "48 B/cell set-up + 72 B/cell per CG iteration",
+            "bytes_model": ("48 B/cell set-up + 72 B/cell per CG iteration" if per_it == 72.0 else
+                            "48 B/cell set-up + 32 B/cell per FP32 inner iteration (FP64 "
+                            "refinement sweeps not counted)"),
             "cg_iters_per_step": iters, "launch_ms": cg_launch_ms}
     # DRAM traffic of one launch from the committed ncu summary (scaled from a
     # smaller capture; it describes the 4096^2 single-sweep solve only)
     prof = os.path.join(REPO, "profiles", "k_cg1_2048x2048_fp64.md")
-    if args.cg_schedule == "single_sweep" and n == 4096 and os.path.exists(prof):
+    if args.cg_schedule == "single_sweep" and n == 4096 and args.precision == "fp64" and os.path.exists(prof):
         import re
         m = re.search(r"traffic_bytes_per_4096_launch:\s*([0-9.eE+]+)", open(prof).read())
         if m:
@@ -334,9 +367,12 @@ def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{n}x{n} plain FP64 subgrid basin (dx 2 m, dt 0.5 s, 4x4 fine, "
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
+        "config": {"workload": f"{n}x{n} {'plain FP64' if args.precision == 'fp64' else 'mixed FP32/FP64'}"
+                               " subgrid basin (dx 2 m, dt 0.5 s, 4x4 fine, "
                                f"~30% dry at low tide, n 0.025, 1 scalar), CG eps 1e-12 from x=0",
+                   "precision": args.precision,
                    "nx": n, "ny": n, "parallelism": f"{ws} replica domain(s), one per GPU",
                    "l2": "no flush: the domain state (>2 GB) exceeds the 126 MB L2",
                    "deck_seed": spec.seed, "deck_gen_s": round(gen_s, 1),
@@ -353,6 +389,8 @@ def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk):
         "cpu_baseline": cpu,
         "last_step": st,
     }
+    if errors is not None:
+        line["errors_vs_fp64"] = errors
     print(json.dumps(line), flush=True)
     return 0
 
@@ -408,8 +446,15 @@ def run_batched_form(args):
         plain_ms += sum(kt[k] for k in ("explicit_ms", "cg_ms", "update_geo_ms", "update_vel_ms",
                                         "finish_ms"))
         g.close()
-    # batched form
-    doms = [native.domain_from_deck(dk) for dk in decks]
+    # batched form (packing granularity and inner tolerance from the autotuner)
+    prec = native.PRECISION_MIXED if args.precision == "mixed" else native.PRECISION_FP64
+    tuning = None
+    if args.cells_per_cta <= 0:
+        from frehdc_b200 import autotune
+        tuning = autotune.tune(decks, args.budget_gb << 30, prec)
+        args.cells_per_cta = tuning["best"]["cells_per_cta"]
+        args.eps_inner = tuning["best"]["eps_inner"]
+    doms = [native.domain_from_deck(dk, precision=prec, eps_inner=args.eps_inner) for dk in decks]
     b = native.Batch(args.budget_gb << 30, args.cells_per_cta)
     for g in doms:
         b.admit(g, 1)
@@ -426,16 +471,41 @@ def run_batched_form(args):
         e1.synchronize()
     batch_ms = e0.elapsed_time(e1)
     info = b.info()
+    slots = list(b.members)
+    for sl in slots:
+        b.release(sl)
     b.close()
+    errors = None
+    if args.precision == "mixed":  # every domain against its FP64 run of the same steps
+        import numpy as np
+        worst = {"eta_max_abs_m": 0.0, "u_max_rel": 0.0, "v_max_rel": 0.0, "volume_rel": 0.0}
+        for g, dk in zip(doms, decks):
+            r = native.domain_from_deck(dk)
+            r.run(1, args.warmup + K)
+            n_ = dk.spec.nx * dk.spec.ny
+            a, c = g.download(["surf", "uuXP", "vvYP"]), r.download(["surf", "uuXP", "vvYP"])
+            worst["eta_max_abs_m"] = max(worst["eta_max_abs_m"],
+                                         float(np.max(np.abs(a["surf"][:n_] - c["surf"][:n_]))))
+            for f, key in (("uuXP", "u_max_rel"), ("vvYP", "v_max_rel")):
+                sc = max(float(np.max(np.abs(c[f][:n_]))), 1e-300)
+                worst[key] = max(worst[key], float(np.max(np.abs(a[f][:n_] - c[f][:n_]))) / sc)
+            va, vc = g.stats()["volume"], r.stats()["volume"]
+            worst["volume_rel"] = max(worst["volume_rel"], abs(va - vc) / abs(vc))
+            r.close()
+        errors = worst
+    for g in doms:
+        g.close()
     total = float(sum(cells)) * K
     line = {"metric": METRIC, "form": "batched", "value": total / (batch_ms / 1e3),
             "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": args.warmup,
             "ms_per_step": batch_ms / K, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{len(specs)} seeded basins, sides log-uniform "
+            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": {"precision": args.precision,
+                       "workload": f"{len(specs)} seeded basins, sides log-uniform "
                                    f"{args.mix_min}-{args.mix_max} (square or 1:4), dx 10 m, "
                                    "dt 1 s, depth 0.3-8 m, 0-40% dry, tide 0.1-0.5 m, "
-                                   "n 0.02-0.04, 4x4 subgrid, 1 scalar, FP64",
+                                   "n 0.02-0.04, 4x4 subgrid, 1 scalar",
                        "cells": int(sum(cells)), "cells_per_cta": args.cells_per_cta,
                        "deck_gen_s": round(gen_s, 1)},
             "plain_form_same_mix": {"value": total / (plain_ms / 1e3), "unit": UNIT,
@@ -443,6 +513,11 @@ def run_batched_form(args):
                                             "kernels summed over the mix"},
             "batch": info, "gpu_launches": 5 * K, "clocks": clk.summary()}
     line["speedup_vs_plain_form"] = line["value"] / line["plain_form_same_mix"]["value"]
+    line["config"]["eps_inner"] = args.eps_inner if args.precision == "mixed" else None
+    if tuning is not None:
+        line["autotune"] = tuning
+    if errors is not None:
+        line["errors_vs_fp64"] = errors
     print(json.dumps(line), flush=True)
     return 0
 
@@ -461,15 +536,22 @@ def run_served_form(args):
     gen_s = time.time() - t0
     arr = serve.poisson_arrivals(len(specs), args.rate, 17)
     reqs = [serve.Request(i, dk, int(k), float(a)) for i, (dk, k, a) in enumerate(zip(decks, steps, arr))]
+    from frehdc_b200 import native
+    prec = native.PRECISION_MIXED if args.precision == "mixed" else native.PRECISION_FP64
+
+    def build(req):
+        return native.domain_from_deck(req.deck, precision=prec, eps_inner=args.eps_inner)
+    if args.cells_per_cta <= 0:
+        args.cells_per_cta = 32768.0
     with ClockSampler(0) as clk:
-        res = serve.serve(reqs, args.budget_gb << 30, args.cells_per_cta)
+        res = serve.serve(reqs, args.budget_gb << 30, args.cells_per_cta, build=build)
     line = {"metric": METRIC, "form": "served", "value": res["cell_steps_per_s"], "unit": UNIT,
             "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
+            "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
             "p50_latency_s": res["p50_s"], "p99_latency_s": res["p99_s"],
             "config": {"workload": f"{len(reqs)} requests, Poisson arrivals {args.rate}/s, sides "
                                    f"log-uniform {args.mix_min}-{args.mix_max}, steps "
-                                   f"{args.req_steps_min}-{args.req_steps_max}, 1 scalar, FP64",
+                                   f"{args.req_steps_min}-{args.req_steps_max}, 1 scalar, {args.precision}",
                        "cells_per_cta": args.cells_per_cta, "deck_gen_s": round(gen_s, 1)},
             "serving": res, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
@@ -495,9 +577,13 @@ def main():
     ap.add_argument("--mix", type=int, default=64, help="batched form: domains in the mix")
     ap.add_argument("--mix-min", type=int, default=64)
     ap.add_argument("--mix-max", type=int, default=512)
-    ap.add_argument("--cells-per-cta", type=float, default=65536.0,
-                    help="batched/served: cells per CTA of a domain's CG")
+    ap.add_argument("--cells-per-cta", type=float, default=0.0,
+                    help="batched/served: cells per CTA of a domain's CG (<= 0: batched form "
+                         "autotunes it on the mix; served form uses 32768)")
     ap.add_argument("--budget-gb", type=int, default=120)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="mixed: FP32 inner CG iterations inside FP64 iterative refinement")
+    ap.add_argument("--eps-inner", type=float, default=1e-5)
     ap.add_argument("--requests", type=int, default=120)
     ap.add_argument("--rate", type=float, default=50.0)
     ap.add_argument("--req-steps-min", type=int, default=50)

@@ -80,6 +80,8 @@ View make_view_at(const frehd_domain *d, int cur) {
   w.bottomZ = d->bottomZ; w.bottomXP = d->bottomXP; w.bottomYP = d->bottomYP;
   w.EnXP = d->EnXP; w.EnYP = d->EnYP; w.Gx = d->Gx; w.Gy = d->Gy; w.Ct = d->Ct; w.b = d->b;
   w.Hx = d->Hx; w.Hy = d->Hy;
+  w.fr0 = d->fr0; w.fr1 = d->fr1; w.fp0 = d->fp0; w.fp1 = d->fp1; w.fd = d->fd;
+  w.fhx = d->fhx; w.fhy = d->fhy;
   w.x = d->x; w.r = d->r; w.p0 = d->p0; w.p1 = d->p1; w.q = d->q;
   w.cellV = d->cellV; w.Sm = d->Sm; w.Fuu = d->Fuu; w.Fvv = d->Fvv;
   w.rmv = d->rmv; w.fix_list = d->fix_list; w.partials = d->partials;
@@ -234,6 +236,8 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
   p.Ne = (int)std::lround((cfg->surfmax - cfg->surfmin) / cfg->dsurf);  // subgrid.c:2115
   p.useThinLayer = cfg->useThinLayer; p.useScalar = cfg->useScalar;
   p.tideFirst = cfg->tideLocFirstP; p.tideLen = cfg->tideLocLengthP; p.maxIter = cfg->maxIter;
+  p.mixed = 0;
+  p.eps_inner = 1e-5;
   const long tot = d->gr.total;
   int r = 0;
   for (int a = 0; a < 2 && !r; ++a) {
@@ -365,6 +369,30 @@ extern "C" int frehd_domain_set_solver(frehd_domain *d, int x0_mode) {
   if (!d || (x0_mode != FREHD_X0_ZERO && x0_mode != FREHD_X0_SURFACE))
     return fail(FREHD_ERR_INVALID, "bad solver option");
   d->x0_mode = x0_mode;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_set_precision(frehd_domain *d, int mode, double eps_inner) {
+  if (!d || (mode != FREHD_PRECISION_FP64 && mode != FREHD_PRECISION_MIXED))
+    return fail(FREHD_ERR_INVALID, "bad precision mode");
+  if (mode == FREHD_PRECISION_MIXED && !(eps_inner > 0 && eps_inner < 1))
+    return fail(FREHD_ERR_INVALID, "eps_inner must lie in (0, 1)");
+  if (d->in_batch) return fail(FREHD_ERR_STATE, "the domain is stepped by a batch (release it first)");
+  CUDA_TRY(cudaSetDevice(d->device));
+  if (mode == FREHD_PRECISION_MIXED && !d->fr0) {
+    const long tot = d->gr.total;
+    int r = 0;
+    float **arrs[] = {&d->fr0, &d->fr1, &d->fp0, &d->fp1, &d->fd, &d->fhx, &d->fhy};
+    for (auto a : arrs)
+      if (!r) r |= dalloc(d, a, tot);
+    if (!r) r |= cg1_make_maps_f32(d->gr, d->fr0, d->fr1, d->fp0, d->fp1, d->fhx, d->fhy, &d->cg1_maps);
+    if (r) return r;
+    CUDA_TRY(cudaMemcpyAsync(d->cg1_maps_dev, &d->cg1_maps, sizeof(Cg1Maps), cudaMemcpyHostToDevice,
+                             d->stream));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+  }
+  d->p.mixed = mode == FREHD_PRECISION_MIXED;
+  if (d->p.mixed) d->p.eps_inner = eps_inner;
   return FREHD_OK;
 }
 

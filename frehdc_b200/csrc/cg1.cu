@@ -1,4 +1,5 @@
-// Single-sweep Jacobi-PCG for the 5-point free-surface system (default solver).
+// Single-sweep Jacobi-PCG for the 5-point free-surface system (default solver),
+// in FP64 or as FP32 inner iterations inside FP64 iterative refinement.
 //
 // Same system, preconditioner, start and stopping rule as k_cg (cg.cu): Jacobi
 // M = diag|Ct|, x0 = 0 (or the surface), stop when ||r||_2 < eps*||b||_2
@@ -31,16 +32,23 @@
 //   A  p_i = r~_i + beta p_{i-1}                 tile + 2 halo (in place)
 //   B  s = A~ p_i, r~_{i+1} = r~_i - alpha s     tile + 1 halo (in place)
 //   C  w = A~ r~_{i+1}; x~ += alpha p_i; sums    tile
-// DRAM traffic per cell and iteration: read r~, p, Hx, Hy, x~, |Ct|; write r~,
-// p, x~ = 72 bytes.  r~ and p ping-pong between two buffers (neighbouring
+// FP64 DRAM traffic per cell and iteration: read r~, p, Hx, Hy, x~, |Ct|; write
+// r~, p, x~ = 72 bytes.  r~ and p ping-pong between two buffers (neighbouring
 // blocks read the old halo while a block writes its new tile); x~ is updated in
 // place and turned back into x = x~/sqrt|Ct| at the end.  The boxes of r~, p,
-// Hx, Hy (132 x 20 doubles each) are double-buffered in shared memory behind
-// one mbarrier per stage: the next tile's loads are in flight while the current
-// tile computes.  Every array holds zeros outside the interior (ghost ring and
-// row padding are never written; rows past the array come back as TMA zero
-// fill), which is what lets the passes run without bounds tests.  All waits are
-// bounded.
+// Hx, Hy are double-buffered in shared memory behind one mbarrier per stage:
+// the next tile's loads are in flight while the current tile computes.  Every
+// array holds zeros outside the interior (ghost ring and row padding are never
+// written; rows past the array come back as TMA zero fill), which is what lets
+// the passes run without bounds tests.  All waits are bounded.
+//
+// Mixed precision (Params::mixed): the outer loop computes r = b - A x in FP64
+// with x in FP64, solves the scaled system A~ d~ = r~ with the same sweep in
+// FP32 (r~, p, d~, Hx, Hy in FP32, 32 bytes per cell and iteration; all dot
+// products accumulated in FP64) until its residual fell by eps_inner, adds
+// x += d~/sqrt|Ct| in FP64, and repeats until the FP64 residual meets the
+// stopping rule above.  A refinement that does not reduce ||r|| tenfold hands
+// the solve to the FP64 path (reported as cg_fallback = 2).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -56,18 +64,54 @@ namespace frehd {
 namespace {
 
 constexpr int kTW = CTX, kTH = CTY;              // owned cells of a tile (128 x 16)
-constexpr int kBW = kTW + 4, kBH = kTH + 4;      // tile + two-cell halo: 132 x 20
-constexpr int kBox = kBW * kBH;                  // doubles per array per stage
-constexpr int kNArr = 4;                         // r~, p, Hx, Hy
-constexpr unsigned kArrBytes = kBox * 8u;        // 21120, a multiple of 128
-constexpr unsigned kStageBytes = kNArr * kArrBytes;
 constexpr int kRing = 2 * (kTW + 2) + 2 * kTH;   // cells of the one-cell halo ring: 292
 constexpr int kRedStride = 8;                    // partial sums per block in grid_allreduce
-static_assert(kArrBytes % 128 == 0, "TMA destinations must stay 128-byte aligned");
-static_assert((kBW * 8) % 16 == 0, "TMA box rows must be a multiple of 16 bytes");
+constexpr int kMaxOuter = 8;                     // refinements of one mixed-precision solve
 static_assert(kTH == kCgThreads / 32, "one warp per tile row");
 static_assert(kRing <= kCgThreads, "one thread per halo-ring cell");
-static_assert(kBox % 2 == 0, "pass A works on double2");
+
+// Box geometry of an element type: the tile sits kLeft cells into a box with a
+// two-cell halo at least, kLeft chosen so that the box's first column is
+// 16-byte aligned in the padded layout (column offset kXOff = 4, tiles start at
+// multiples of 128 cells).
+template <typename T>
+struct Box {
+  static constexpr int kLeft = sizeof(T) == 8 ? 2 : 4;
+  static constexpr int kBW = kTW + 2 * kLeft;      // 132 (FP64) / 136 (FP32)
+  static constexpr int kBH = kTH + 4;              // 20
+  static constexpr int kBox = kBW * kBH;
+  static constexpr unsigned kArrBytes = kBox * (unsigned)sizeof(T);
+  static constexpr unsigned kStageBytes = 4 * kArrBytes;  // r~, p, Hx, Hy
+  static_assert(kArrBytes % 128 == 0, "TMA destinations must stay 128-byte aligned");
+  static_assert((kBW * sizeof(T)) % 16 == 0, "TMA box rows must be a multiple of 16 bytes");
+  static_assert(((kXOff - kLeft) * sizeof(T)) % 16 == 0, "box origin 16-byte aligned");
+  static_assert(kBox % 2 == 0, "pass A works on pairs");
+  // box position of tile cell (lx, ly), lx and ly from -1 (the halo ring)
+  __device__ static __forceinline__ int q(int lx, int ly) { return (ly + 2) * kBW + kLeft + lx; }
+  // box position of cell t of the one-cell halo ring (t < kRing)
+  __device__ static __forceinline__ int ring(int t) {
+    if (t < kTW + 2) return q(t - 1, -1);          // row above the tile
+    t -= kTW + 2;
+    if (t < kTW + 2) return q(t - 1, kTH);         // row below
+    t -= kTW + 2;
+    if (t < kTH) return q(-1, t);                  // column left
+    t -= kTH;
+    return q(kTW, t);                              // column right
+  }
+};
+constexpr unsigned kSmemStages = 2 * Box<double>::kStageBytes;  // FP64 stages are the larger
+static_assert(2 * Box<float>::kStageBytes <= kSmemStages, "FP32 stages fit the FP64 ones");
+
+template <typename T>
+struct Pair;
+template <>
+struct Pair<double> {
+  using type = double2;
+};
+template <>
+struct Pair<float> {
+  using type = float2;
+};
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) {
   return (unsigned)__cvta_generic_to_shared(p);
@@ -115,64 +159,221 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map,
 }
 
 // Shared-memory arrays of one stage.
+template <typename T>
 struct Stage {
-  double *R, *P, *HX, *HY;
+  T *R, *P, *HX, *HY;
   __device__ Stage(unsigned char *base) {
-    R = reinterpret_cast<double *>(base);
-    P = R + kBox;
-    HX = P + kBox;
-    HY = HX + kBox;
+    R = reinterpret_cast<T *>(base);
+    P = R + Box<T>::kBox;
+    HX = P + Box<T>::kBox;
+    HY = HX + Box<T>::kBox;
   }
 };
 
+// The four maps one sweep reads.
+struct SweepMaps {
+  const CUtensorMap *r, *p, *hx, *hy;
+};
+
 // Issue the four box loads of tile `tile` into a stage (one thread).
-__device__ __forceinline__ void issue_tile(const Cg1Maps *m, int cur, const TileIt &ti, int tile,
+template <typename T>
+__device__ __forceinline__ void issue_tile(const SweepMaps &m, const TileIt &ti, int tile,
                                            unsigned char *stage_base, unsigned long long *bar) {
   int i0, j0;
   tile_origin(ti, tile, &i0, &j0);
-  // box origin: cell (i0-2, j0-2) = padded column i0+2 (even: 16-byte aligned), row j0-1
-  const int x = i0 - 2 + kXOff, y = j0 - 2 + 1;
-  Stage s(stage_base);
+  // box origin: cell (i0 - kLeft, j0 - 2) = padded column i0 - kLeft + kXOff (16-byte aligned), row j0 - 1
+  const int x = i0 - Box<T>::kLeft + kXOff, y = j0 - 2 + 1;
+  Stage<T> s(stage_base);
   // generic-proxy writes to this stage (the in-place passes) come before the TMA writes
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  mbar_expect_tx(bar, kStageBytes);
-  tma_load_2d(s.R, &m->r[cur], bar, x, y);
-  tma_load_2d(s.P, &m->p[cur], bar, x, y);
-  tma_load_2d(s.HX, &m->hx, bar, x, y);
-  tma_load_2d(s.HY, &m->hy, bar, x, y);
+  mbar_expect_tx(bar, Box<T>::kStageBytes);
+  tma_load_2d(s.R, m.r, bar, x, y);
+  tma_load_2d(s.P, m.p, bar, x, y);
+  tma_load_2d(s.HX, m.hx, bar, x, y);
+  tma_load_2d(s.HY, m.hy, bar, x, y);
 }
 
 // A~ v at shared-memory position q of a box: unit diagonal, scaled couplings,
 // none for a decoupled row (sign bit of its own HX).
-__device__ __forceinline__ double apply(const double *V, const double *HX, const double *HY, int q) {
-  const double he = HX[q];
-  const double off = fabs(he) * V[q + 1] + fabs(HX[q - 1]) * V[q - 1] + HY[q] * V[q + kBW] +
-                     HY[q - kBW] * V[q - kBW];
+template <typename T>
+__device__ __forceinline__ T apply(const T *V, const T *HX, const T *HY, int q) {
+  constexpr int W = Box<T>::kBW;
+  const T he = HX[q];
+  const T off = fabs(he) * V[q + 1] + fabs(HX[q - 1]) * V[q - 1] + HY[q] * V[q + W] + HY[q - W] * V[q - W];
   return signbit(he) ? V[q] : V[q] - off;
 }
 
-// Box position of cell t of the tile's one-cell halo ring (t < kRing).
-__device__ __forceinline__ int ring_pos(int t) {
-  if (t < kTW + 2) return kBW + 1 + t;                  // row above the tile
-  t -= kTW + 2;
-  if (t < kTW + 2) return (kTH + 2) * kBW + 1 + t;      // row below
-  t -= kTW + 2;
-  if (t < kTH) return (2 + t) * kBW + 1;                // column left
-  t -= kTH;
-  return (2 + t) * kBW + kTW + 2;                       // column right
+// One CG sweep over this CTA's tiles (rank of nb): p = r~ + beta p_old,
+// s = A~ p, r~' = r~ - alpha s, w = A~ r~', X += alpha p; r~' and p stored to
+// rn_out / pn_out.  red += (r~',r~'), (w,r~'), (r~',s), (p,w), (p,s) and
+// sum D r~'^2 (kUnscaled; D = |Ct|) or (r~',r~') again.  seq: tiles this CTA
+// consumed so far (stage and mbarrier phase).
+template <typename T, bool kUnscaled, typename XT>
+__device__ __forceinline__ bool sweep(const SweepMaps &m, T *rn_out, T *pn_out, XT *X, const double *Ct,
+                                      const Grid &g, const TileIt &ti, unsigned rank, unsigned nb,
+                                      T alpha, T beta, double (&red)[6], unsigned char *smem,
+                                      unsigned long long *bars, unsigned &seq, Scratch *sc) {
+  using B = Box<T>;
+  __shared__ int s_ok;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  // generic writes of the previous sweep (all blocks) come before this sweep's TMA reads
+  if (threadIdx.x == 0) {
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    issue_tile<T>(m, ti, rank, smem + (seq & 1) * B::kStageBytes, &bars[seq & 1]);
+  }
+  for (int tile = rank; tile < ti.ntiles; tile += nb, ++seq) {
+    const int st = seq & 1;
+    const int next = tile + (int)nb;
+    if (threadIdx.x == 0 && next < ti.ntiles)
+      issue_tile<T>(m, ti, next, smem + (st ^ 1) * B::kStageBytes, &bars[st ^ 1]);
+    int i0, j0;
+    tile_origin(ti, tile, &i0, &j0);
+    // X and |Ct| of the owned cells: in flight while the boxes arrive
+    const int j = j0 + ty;
+    XT xs[CPT];
+    double ds[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int i = i0 + c * 32 + tx;
+      const bool in = i < g.nx && j < g.ny;
+      const long k = g.at(in ? i : 0, in ? j : 0);
+      xs[c] = X[k];
+      ds[c] = kUnscaled ? fabs(Ct[k]) : 0.0;
+    }
+    if (threadIdx.x == 0) s_ok = mbar_wait(&bars[st], (seq >> 1) & 1, kBarrierTimeoutNs);
+    __syncthreads();
+    if (!s_ok) {
+      // the other stage may hold a load issued for the next tile: let it land
+      if (threadIdx.x == 0) {
+        set_status(sc, FREHD_ERR_TIMEOUT);
+        if (next < ti.ntiles) mbar_wait(&bars[st ^ 1], ((seq + 1) >> 1) & 1, kBarrierTimeoutNs);
+      }
+      return false;
+    }
+    mbar_wait(&bars[st], (seq >> 1) & 1, kBarrierTimeoutNs);  // completed: acquire in every thread
+    Stage<T> s(smem + st * B::kStageBytes);
+
+    // pass A: p_i = r~_i + beta p_{i-1} on the whole box
+    {
+      using P2 = typename Pair<T>::type;
+      P2 *pp = reinterpret_cast<P2 *>(s.P);
+      const P2 *rp = reinterpret_cast<const P2 *>(s.R);
+#pragma unroll
+      for (int e = threadIdx.x; e < B::kBox / 2; e += kCgThreads) {
+        const P2 rv = rp[e];
+        P2 pv = pp[e];
+        pv.x = rv.x + beta * pv.x;
+        pv.y = rv.y + beta * pv.y;
+        pp[e] = pv;
+      }
+    }
+    __syncthreads();
+
+    // pass B: r~_{i+1} = r~_i - alpha A~ p_i on the tile (4 cells per thread) and its ring;
+    // it reads only P, HX, HY besides each thread's own R cells, so R is updated in place
+    {
+      T rb[CPT];
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        const int q = B::q(c * 32 + tx, ty);
+        const T sv = apply<T>(s.P, s.HX, s.HY, q);
+        rb[c] = s.R[q] - alpha * sv;
+        if (i0 + c * 32 + tx < g.nx && j < g.ny) {
+          red[2] += (double)rb[c] * (double)sv;
+          red[4] += (double)s.P[q] * (double)sv;
+        }
+      }
+      T rring = 0;
+      const int qr = threadIdx.x < kRing ? B::ring(threadIdx.x) : 0;
+      if (threadIdx.x < kRing) rring = s.R[qr] - alpha * apply<T>(s.P, s.HX, s.HY, qr);
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) s.R[B::q(c * 32 + tx, ty)] = rb[c];
+      if (threadIdx.x < kRing) s.R[qr] = rring;
+    }
+    __syncthreads();
+
+    // pass C: w = A~ r~_{i+1}; sums; X_{i+1} = X_i + alpha p_i; store r~, p, X
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int i = i0 + c * 32 + tx;
+      if (i < g.nx && j < g.ny) {
+        const int q = B::q(c * 32 + tx, ty);
+        const T u = s.R[q], pc = s.P[q];
+        const T wv = apply<T>(s.R, s.HX, s.HY, q);
+        const double ud = u;
+        red[0] += ud * ud;
+        red[1] += (double)wv * ud;
+        red[3] += (double)pc * (double)wv;
+        red[5] += kUnscaled ? ds[c] * (ud * ud) : ud * ud;
+        const long k = g.at(i, j);
+        X[k] = xs[c] + alpha * pc;
+        rn_out[k] = u;
+        pn_out[k] = pc;
+      }
+    }
+    __syncthreads();  // stage st is free for the tile after next
+  }
+  // this thread's global writes before the next sweep's TMA reads (other blocks)
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+  return true;
+}
+
+// delta0 = (A~ v, v) of a stored scaled vector v (plain halo loads into stage 0).
+template <typename T>
+__device__ __forceinline__ double first_delta(const T *V, const T *HXg, const T *HYg, const Grid &g,
+                                              const TileIt &ti, unsigned rank, unsigned nb,
+                                              unsigned char *smem) {
+  using B = Box<T>;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  double d0 = 0.0;
+  Stage<T> s(smem);
+  for (int tile = rank; tile < ti.ntiles; tile += nb) {
+    int i0, j0;
+    tile_origin(ti, tile, &i0, &j0);
+    __syncthreads();
+    // V, Hx, Hy of the tile and its one-cell ring (zeros outside the interior)
+    for (int e = threadIdx.x; e < (kTW + 2) * (kTH + 2); e += kCgThreads) {
+      const int ly = e / (kTW + 2) - 1, lx = e % (kTW + 2) - 1;
+      const int i = i0 + lx, jj = j0 + ly;
+      const bool in = (unsigned)i < (unsigned)g.nx && (unsigned)jj < (unsigned)g.ny;
+      const long k = in ? g.at(i, jj) : 0;
+      const int q = B::q(lx, ly);
+      s.R[q] = in ? __ldcg(V + k) : T(0);
+      s.HX[q] = in ? __ldcg(HXg + k) : T(0);
+      s.HY[q] = in ? __ldcg(HYg + k) : T(0);
+    }
+    __syncthreads();
+    const int j = j0 + ty;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int i = i0 + c * 32 + tx;
+      if (i < g.nx && j < g.ny) {
+        const int q = B::q(c * 32 + tx, ty);
+        d0 += (double)apply<T>(s.R, s.HX, s.HY, q) * (double)s.R[q];
+      }
+    }
+  }
+  __syncthreads();
+  return d0;
+}
+
+__device__ __forceinline__ void acquire_maps(const CUtensorMap *maps, int n) {
+  // the maps were written to global memory by a host copy: make them visible to the TMA unit
+  for (int q = 0; q < n; ++q)
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(maps + q) : "memory");
 }
 
 }  // namespace
 
-// One solve of domain w by a group of nb CTAs, of which this CTA is number
+// FP64 solve of domain w by a group of nb CTAs, of which this CTA is number
 // `rank`.  smem/bars: this CTA's two stages and their mbarriers (initialised by
 // the kernel); seq counts the tiles this CTA consumed so far, across solves, and
 // gives each wait its mbarrier phase.  Returns false after an error (status set).
-static __device__ __forceinline__ bool cg1_solve(const View &w, const Cg1Maps *__restrict__ m, int x0_surface, int eliminate,
-                          unsigned rank, unsigned nb, unsigned char *smem, unsigned long long *bars,
-                          unsigned &seq) {
+static __device__ __forceinline__ bool cg1_fp64(const View &w, const Cg1Maps *__restrict__ m,
+                                                int x0_surface, int eliminate, unsigned rank,
+                                                unsigned nb, unsigned char *smem,
+                                                unsigned long long *bars, unsigned &seq) {
   Scratch *sc = w.sc;
-  __shared__ int s_ok;
   const Grid g = w.gr;
   const Params &p = w.p;
   const int nx = g.nx, ny = g.ny;
@@ -184,13 +385,8 @@ static __device__ __forceinline__ bool cg1_solve(const View &w, const Cg1Maps *_
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   double *partials = w.partials, *totals = w.partials + kRedStride * (long)nb;
   const double *Ct = w.Ct, *Gx = w.Gx, *Gy = w.Gy;
-  double *const X = w.x;  // read and written per cell in the sweep: kept in a register
-  if (threadIdx.x == 0) {
-    // the maps were written to global memory by a host copy: make them visible to the TMA unit
-    const CUtensorMap *maps = &m->r[0];
-    for (int q = 0; q < 6; ++q)
-      asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(maps + q) : "memory");
-  }
+  double *const X = w.x;
+  if (threadIdx.x == 0) acquire_maps(&m->r[0], 6);
 
   // A solve of the assembled (non-symmetric) matrix can stall: ||r|| stops
   // falling above eps*||b|| and laspack's CGIter runs on to maxIter.  When ||r||
@@ -228,7 +424,7 @@ static __device__ __forceinline__ bool cg1_solve(const View &w, const Cg1Maps *_
           // row k's decoupled flag rides in the sign bit of its own east coupling
           w.Hx[k] = ct < 0 ? -fabs(hx) : fabs(hx);
           w.Hy[k] = hy;
-          w.x[k] = x0_surface ? d * w.surf_cur[k] : 0.0;
+          X[k] = x0_surface ? d * w.surf_cur[k] : 0.0;
           w.p0[k] = 0.0;
         }
       }
@@ -277,37 +473,10 @@ static __device__ __forceinline__ bool cg1_solve(const View &w, const Cg1Maps *_
     rr = acc[1];
     bnorm = sqrt(acc[2]);
 
-    // ---- setup 3: delta0 = (A~ r~0, r~0) (plain halo loads into stage 0)
+    // ---- setup 3: delta0 = (A~ r~0, r~0)
     double delta;
     {
-      double d0[1] = {0};
-      Stage s(smem);
-      for (int tile = rank; tile < ti.ntiles; tile += nb) {
-        int i0, j0;
-        tile_origin(ti, tile, &i0, &j0);
-        __syncthreads();
-        // r~0, Hx, Hy of the tile and its one-cell ring (zeros outside the interior)
-        for (int e = threadIdx.x; e < (kTW + 2) * (kTH + 2); e += kCgThreads) {
-          const int ly = 1 + e / (kTW + 2), lx = 1 + e % (kTW + 2);
-          const int i = i0 - 2 + lx, jj = j0 - 2 + ly;
-          const bool in = (unsigned)i < (unsigned)nx && (unsigned)jj < (unsigned)ny;
-          const long k = in ? g.at(i, jj) : 0;
-          s.R[ly * kBW + lx] = in ? ld(w.r, k) : 0.0;
-          s.HX[ly * kBW + lx] = in ? ld(w.Hx, k) : 0.0;
-          s.HY[ly * kBW + lx] = in ? ld(w.Hy, k) : 0.0;
-        }
-        __syncthreads();
-        const int j = j0 + ty;
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-          const int i = i0 + c * 32 + tx;
-          if (i < nx && j < ny) {
-            const int q = (ty + 2) * kBW + c * 32 + tx + 2;
-            d0[0] += apply(s.R, s.HX, s.HY, q) * s.R[q];
-          }
-        }
-      }
-      __syncthreads();
+      double d0[1] = {first_delta<double>(w.r, w.Hx, w.Hy, g, ti, rank, nb, smem)};
       if (!grid_allreduce<1, kRedStride>(d0, sc, partials, totals, nb, rank)) return false;
       delta = d0[0];
     }
@@ -332,102 +501,10 @@ static __device__ __forceinline__ bool cg1_solve(const View &w, const Cg1Maps *_
       double *rn_out = cur ? w.r : w.q, *pn_out = cur ? w.p0 : w.p1;
       // (r~', r~'), (A~ r~', r~'), (r~', A~ p), (p, A~ r~'), (p, A~ p), ||r'||^2; r~' = r~_{i+1}
       double red[6] = {0, 0, 0, 0, 0, 0};
-      // generic writes of the previous sweep (all blocks) come before this sweep's TMA reads
-      if (threadIdx.x == 0) {
-        asm volatile("fence.proxy.async.global;" ::: "memory");
-        issue_tile(m, cur, ti, rank, smem + (seq & 1) * kStageBytes, &bars[seq & 1]);
-      }
-      for (int tile = rank; tile < ti.ntiles; tile += nb, ++seq) {
-        const int st = seq & 1;
-        const int next = tile + (int)nb;
-        if (threadIdx.x == 0 && next < ti.ntiles)
-          issue_tile(m, cur, ti, next, smem + (st ^ 1) * kStageBytes, &bars[st ^ 1]);
-        int i0, j0;
-        tile_origin(ti, tile, &i0, &j0);
-        // x~ and |Ct| of the owned cells: in flight while the boxes arrive
-        const int j = j0 + ty;
-        double xs[CPT], ds[CPT];
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-          const int i = i0 + c * 32 + tx;
-          const bool in = i < nx && j < ny;
-          const long k = g.at(in ? i : 0, in ? j : 0);
-          xs[c] = X[k];
-          ds[c] = fabs(Ct[k]);
-        }
-        if (threadIdx.x == 0) s_ok = mbar_wait(&bars[st], (seq >> 1) & 1, kBarrierTimeoutNs);
-        __syncthreads();
-        if (!s_ok) {
-          // the other stage may hold a load issued for the next tile: let it land
-          if (threadIdx.x == 0) {
-            set_status(sc, FREHD_ERR_TIMEOUT);
-            if (next < ti.ntiles) mbar_wait(&bars[st ^ 1], ((seq + 1) >> 1) & 1, kBarrierTimeoutNs);
-          }
-          return false;
-        }
-        mbar_wait(&bars[st], (seq >> 1) & 1, kBarrierTimeoutNs);  // completed: acquire in every thread
-        Stage s(smem + st * kStageBytes);
-
-        // pass A: p_i = r~_i + beta p_{i-1} on the whole box
-        {
-          double2 *P2 = reinterpret_cast<double2 *>(s.P);
-          const double2 *R2 = reinterpret_cast<const double2 *>(s.R);
-#pragma unroll
-          for (int e = threadIdx.x; e < kBox / 2; e += kCgThreads) {
-            const double2 rv = R2[e];
-            double2 pv = P2[e];
-            pv.x = rv.x + beta * pv.x;
-            pv.y = rv.y + beta * pv.y;
-            P2[e] = pv;
-          }
-        }
-        __syncthreads();
-
-        // pass B: r~_{i+1} = r~_i - alpha A~ p_i on the tile (4 cells per thread) and its ring;
-        // it reads only P, HX, HY besides each thread's own R cells, so R is updated in place
-        {
-          double rb[CPT];
-#pragma unroll
-          for (int c = 0; c < CPT; ++c) {
-            const int q = (ty + 2) * kBW + c * 32 + tx + 2;
-            const double sv = apply(s.P, s.HX, s.HY, q);
-            rb[c] = s.R[q] - alpha * sv;
-            if (i0 + c * 32 + tx < nx && j < ny) {
-              red[2] += rb[c] * sv;
-              red[4] += s.P[q] * sv;
-            }
-          }
-          double rring = 0.0;
-          const int qr = threadIdx.x < kRing ? ring_pos(threadIdx.x) : 0;
-          if (threadIdx.x < kRing) rring = s.R[qr] - alpha * apply(s.P, s.HX, s.HY, qr);
-#pragma unroll
-          for (int c = 0; c < CPT; ++c) s.R[(ty + 2) * kBW + c * 32 + tx + 2] = rb[c];
-          if (threadIdx.x < kRing) s.R[qr] = rring;
-        }
-        __syncthreads();
-
-        // pass C: w = A~ r~_{i+1}; sums; x~_{i+1} = x~_i + alpha p_i; store r~, p, x~
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-          const int i = i0 + c * 32 + tx;
-          if (i < nx && j < ny) {
-            const int q = (ty + 2) * kBW + c * 32 + tx + 2;
-            const double u = s.R[q], pc = s.P[q];
-            const double wv = apply(s.R, s.HX, s.HY, q);
-            red[0] += u * u;
-            red[1] += wv * u;
-            red[3] += pc * wv;
-            red[5] += ds[c] * (u * u);
-            const long k = g.at(i, j);
-            X[k] = xs[c] + alpha * pc;
-            rn_out[k] = u;
-            pn_out[k] = pc;
-          }
-        }
-        __syncthreads();  // stage st is free for the tile after next
-      }
-      // this thread's global writes before the next sweep's TMA reads (other blocks)
-      asm volatile("fence.proxy.async.global;" ::: "memory");
+      const SweepMaps sm{&m->r[cur], &m->p[cur], &m->hx, &m->hy};
+      if (!sweep<double, true, double>(sm, rn_out, pn_out, X, Ct, g, ti, rank, nb, alpha, beta, red,
+                                       smem, bars, seq, sc))
+        return false;
       if (!grid_allreduce<6, kRedStride>(red, sc, partials, totals, nb, rank)) return false;
       gamma_old = gamma;
       gamma = red[0];
@@ -467,7 +544,7 @@ static __device__ __forceinline__ bool cg1_solve(const View &w, const Cg1Maps *_
       const int i = i0 + c * 32 + tx;
       if (i < nx && j < ny) {
         const long k = g.at(i, j);
-        w.x[k] = w.x[k] / sqrt(fabs(Ct[k]));
+        X[k] = X[k] / sqrt(fabs(Ct[k]));
       }
     }
   }
@@ -480,14 +557,191 @@ static __device__ __forceinline__ bool cg1_solve(const View &w, const Cg1Maps *_
   return true;
 }
 
+// Mixed-precision solve (FP32 inner iterations, FP64 refinement).  Returns 0
+// after an error (status set), 1 when done, 2 when the refinement stalled and
+// the FP64 solve must take over (x is then overwritten by it).
+static __device__ __forceinline__ int cg1_mixed(const View &w, const Cg1Maps *__restrict__ m,
+                                               int x0_surface, int elim, unsigned rank, unsigned nb,
+                                               unsigned char *smem, unsigned long long *bars,
+                                               unsigned &seq) {
+  Scratch *sc = w.sc;
+  const Grid g = w.gr;
+  const Params &p = w.p;
+  const int nx = g.nx, ny = g.ny;
+  const long pitch = g.pitch;
+  TileIt ti;
+  ti.ntx = (nx + CTX - 1) / CTX;
+  ti.nty = (ny + CTY - 1) / CTY;
+  ti.ntiles = ti.ntx * ti.nty;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  double *partials = w.partials, *totals = w.partials + kRedStride * (long)nb;
+  const double *Ct = w.Ct, *Gx = w.Gx, *Gy = w.Gy;
+  double *const X = w.x;
+  float *const FD = w.fd;
+  if (threadIdx.x == 0) acquire_maps(&m->fr[0], 6);
+
+  // ---- setup: x = x0 (FP64, unscaled), FP32 scaled couplings with the row flag
+  for (int tile = rank; tile < ti.ntiles; tile += nb) {
+    int i0, j0;
+    tile_origin(ti, tile, &i0, &j0);
+    const int j = j0 + ty;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int i = i0 + c * 32 + tx;
+      if (i < nx && j < ny) {
+        const long k = g.at(i, j);
+        const double ct = Ct[k], ce = Ct[k + 1], cn = Ct[k + pitch];
+        const double d = sqrt(fabs(ct));
+        double hx = Gx[k] / (d * sqrt(fabs(ce))), hy = Gy[k] / (d * sqrt(fabs(cn)));
+        if (elim) {
+          if (!(ct > 0 && ce > 0)) hx = 0.0;
+          if (!(ct > 0 && cn > 0)) hy = 0.0;
+        }
+        const float hxf = fabsf((float)hx);
+        w.fhx[k] = ct < 0 ? -hxf : hxf;
+        w.fhy[k] = (float)hy;
+        X[k] = x0_surface ? w.surf_cur[k] : 0.0;
+      }
+    }
+  }
+  {
+    double none[1] = {0};
+    if (!grid_allreduce<1, kRedStride>(none, sc, partials, totals, nb, rank)) return 0;
+  }
+  auto converged = [&](double rr_, double bn) {
+    const double rn = sqrt(rr_);
+    return rn < p.eps * bn || (bn == 0.0 && 1.0 + rn == 1.0);
+  };
+  double rr = 0.0, rr_prev = 0.0, bnorm = 0.0;
+  int it_all = 0, done = 0;
+  for (int outer = 0; outer < kMaxOuter; ++outer) {
+    // ---- residual in FP64: r = b - A x; r~ = r/sqrt|Ct| in FP32; d~ = 0, p_{-1} = 0
+    double acc[3] = {0, 0, 0};
+    for (int tile = rank; tile < ti.ntiles; tile += nb) {
+      int i0, j0;
+      tile_origin(ti, tile, &i0, &j0);
+      const int j = j0 + ty;
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        const int i = i0 + c * 32 + tx;
+        if (i < nx && j < ny) {
+          const long k = g.at(i, j);
+          const double ct = Ct[k], bk = w.b[k];
+          auto xv = [&](long kk) -> double {
+            const double cc = Ct[kk];
+            return (elim && cc < 0) ? w.b[kk] / (-cc) : __ldcg(X + kk);
+          };
+          double r;
+          if (ct > 0) {
+            const double ax = ct * __ldcg(X + k) - (Gx[k] * xv(k + 1) + Gx[k - 1] * xv(k - 1) +
+                                                    Gy[k] * xv(k + pitch) + Gy[k - pitch] * xv(k - pitch));
+            r = bk - ax;
+          } else {
+            r = bk - (-ct) * __ldcg(X + k);
+          }
+          const float rs = (float)(r / sqrt(fabs(ct)));
+          acc[0] += (double)rs * (double)rs;
+          acc[1] += r * r;
+          acc[2] += bk * bk;
+          w.fr0[k] = rs;
+          w.fp0[k] = 0.0f;
+          FD[k] = 0.0f;
+        }
+      }
+    }
+    if (!grid_allreduce<3, kRedStride>(acc, sc, partials, totals, nb, rank)) return 0;
+    rr = acc[1];
+    if (outer == 0) bnorm = sqrt(acc[2]);
+    if (converged(rr, bnorm)) {
+      done = 1;
+      break;
+    }
+    if (outer > 0 && rr > 1e-2 * rr_prev) break;  // no tenfold gain: FP64 takes over
+    rr_prev = rr;
+
+    // ---- inner FP32 solve of A~ d~ = r~ until (r~, r~) fell by eps_inner^2
+    const double g0 = acc[0];
+    double gamma = g0, delta;
+    {
+      double d0[1] = {first_delta<float>(w.fr0, w.fhx, w.fhy, g, ti, rank, nb, smem)};
+      if (!grid_allreduce<1, kRedStride>(d0, sc, partials, totals, nb, rank)) return 0;
+      delta = d0[0];
+    }
+    double gamma_old = 1.0, e1 = 0.0, e2 = 0.0, e3 = 0.0;
+    int cur = 0, it = 0;
+    const double stop = p.eps_inner * p.eps_inner * g0;
+    while (gamma > stop && it < p.maxIter) {
+      const double beta = it == 0 ? 0.0 : gamma / gamma_old;
+      const double alpha = gamma / (delta + beta * (e1 + e2) + beta * beta * e3);
+      ++it;
+      float *rn_out = cur ? w.fr0 : w.fr1, *pn_out = cur ? w.fp0 : w.fp1;
+      double red[6] = {0, 0, 0, 0, 0, 0};
+      const SweepMaps sm{&m->fr[cur], &m->fp[cur], &m->fhx, &m->fhy};
+      if (!sweep<float, false, float>(sm, rn_out, pn_out, FD, Ct, g, ti, rank, nb, (float)alpha,
+                                      (float)beta, red, smem, bars, seq, sc))
+        return 0;
+      if (!grid_allreduce<6, kRedStride>(red, sc, partials, totals, nb, rank)) return 0;
+      gamma_old = gamma;
+      gamma = red[0];
+      delta = red[1];
+      e1 = red[2];
+      e2 = red[3];
+      e3 = red[4];
+      cur ^= 1;
+    }
+    it_all += it;
+
+    // ---- x += d~/sqrt|Ct| in FP64 (each block its own cells; the barrier orders
+    //      them before the next residual reads neighbours)
+    for (int tile = rank; tile < ti.ntiles; tile += nb) {
+      int i0, j0;
+      tile_origin(ti, tile, &i0, &j0);
+      const int j = j0 + ty;
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        const int i = i0 + c * 32 + tx;
+        if (i < nx && j < ny) {
+          const long k = g.at(i, j);
+          X[k] = X[k] + (double)FD[k] / sqrt(fabs(Ct[k]));
+        }
+      }
+    }
+    double none[1] = {0};
+    if (!grid_allreduce<1, kRedStride>(none, sc, partials, totals, nb, rank)) return 0;
+  }
+  if (!done) return 2;
+  if (rank == 0 && threadIdx.x == 0) {
+    sc->cg_iters = it_all;
+    sc->cg_fallback = 0;
+    sc->cg_rr = rr;
+    sc->cg_bb = bnorm * bnorm;
+  }
+  return 1;
+}
+
+// The domain's solve in its configured precision.
+static __device__ __forceinline__ bool cg1_solve(const View &w, const Cg1Maps *__restrict__ m,
+                                                 int x0_surface, int eliminate, unsigned rank,
+                                                 unsigned nb, unsigned char *smem,
+                                                 unsigned long long *bars, unsigned &seq) {
+  if (w.p.mixed) {
+    const int r = cg1_mixed(w, m, x0_surface, eliminate, rank, nb, smem, bars, seq);
+    if (r != 2) return r == 1;
+    const bool ok = cg1_fp64(w, m, x0_surface, eliminate, rank, nb, smem, bars, seq);
+    if (ok && rank == 0 && threadIdx.x == 0) w.sc->cg_fallback = 2;
+    return ok;
+  }
+  return cg1_fp64(w, m, x0_surface, eliminate, rank, nb, smem, bars, seq);
+}
+
 // Dynamic shared memory of one CTA: two stages and two mbarriers, the base
 // rounded up to 128 bytes (the region after the static shared data is only
-// 16-byte aligned; the launch requests 128 bytes of slack).  False (and the
-// status set on `sc`) if an alignment the TMA needs does not hold.
+// 16-byte aligned; the launch requests 128 bytes of slack).  False if an
+// alignment the TMA needs does not hold.
 static __device__ __forceinline__ bool cg1_smem(unsigned char *smem_raw, unsigned char **smem,
-                                         unsigned long long **bars) {
+                                                unsigned long long **bars) {
   *smem = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
-  *bars = reinterpret_cast<unsigned long long *>(*smem + 2 * kStageBytes);
+  *bars = reinterpret_cast<unsigned long long *>(*smem + kSmemStages);
   if ((smem_u32(*smem) & 127u) || (smem_u32(*bars) & 7u)) return false;
   if (threadIdx.x == 0) {
     mbar_init(&(*bars)[0], 1);
@@ -510,8 +764,7 @@ __global__ void __launch_bounds__(kCgThreads, 1)
     if (threadIdx.x == 0) set_status(w.sc, FREHD_ERR_CUDA);
     return;
   }
-  // the solve reads the view from shared memory (fewer live registers than the
-  // parameter copy)
+  // the solve reads the view from shared memory
   __shared__ View s_view;
   {
     const unsigned long long *src = reinterpret_cast<const unsigned long long *>(&w);
@@ -565,7 +818,6 @@ __global__ void __launch_bounds__(kCgThreads, 1)
   }
 }
 
-
 // ---------------------------------------------------------------- host side
 
 namespace {
@@ -582,16 +834,19 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-int encode(const Grid &g, double *base, CUtensorMap *out) {
+template <typename T>
+int encode(const Grid &g, T *base, CUtensorMap *out) {
   auto fn = encode_fn();
   if (!fn) return fail(FREHD_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
   const cuuint64_t dims[2] = {(cuuint64_t)g.pitch, (cuuint64_t)(g.ny + 2)};
-  const cuuint64_t strides[1] = {(cuuint64_t)g.pitch * sizeof(double)};
-  const cuuint32_t box[2] = {(cuuint32_t)kBW, (cuuint32_t)kBH};
+  const cuuint64_t strides[1] = {(cuuint64_t)g.pitch * sizeof(T)};
+  const cuuint32_t box[2] = {(cuuint32_t)Box<T>::kBW, (cuuint32_t)Box<T>::kBH};
   const cuuint32_t estr[2] = {1, 1};
-  CUresult e = fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, base, dims, strides, box, estr,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  const CUtensorMapDataType dt =
+      sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  CUresult e = fn(out, dt, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (e != CUDA_SUCCESS) return fail(FREHD_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)e);
   return FREHD_OK;
 }
@@ -611,8 +866,20 @@ int cg1_make_maps(const Grid &g, double *r0, double *r1, double *p0, double *p1,
   return rc;
 }
 
+int cg1_make_maps_f32(const Grid &g, float *r0, float *r1, float *p0, float *p1, float *hx,
+                      float *hy, Cg1Maps *m) {
+  int rc = 0;
+  rc = rc ? rc : encode(g, r0, &m->fr[0]);
+  rc = rc ? rc : encode(g, r1, &m->fr[1]);
+  rc = rc ? rc : encode(g, p0, &m->fp[0]);
+  rc = rc ? rc : encode(g, p1, &m->fp[1]);
+  rc = rc ? rc : encode(g, hx, &m->fhx);
+  rc = rc ? rc : encode(g, hy, &m->fhy);
+  return rc;
+}
+
 // two stages, two mbarriers, and slack to align the base to 128 bytes
-size_t cg1_smem_bytes() { return 2 * (size_t)kStageBytes + 2 * sizeof(unsigned long long) + 128; }
+size_t cg1_smem_bytes() { return (size_t)kSmemStages + 2 * sizeof(unsigned long long) + 128; }
 
 int cg1_blocks(int device, const Grid &g, int *blocks) {
   static const size_t smem = cg1_smem_bytes();

@@ -11,14 +11,19 @@
 namespace frehd {
 
 // Tensor maps over the padded layout: the scaled residual and direction (two
-// buffers each) and the scaled face couplings Hx, Hy.  The kernel reads them
-// from global memory (a device copy, 64-byte aligned).
+// buffers each) and the scaled face couplings Hx, Hy, in FP64, and the same
+// arrays of the mixed-precision solve in FP32 (zero when it is not enabled).
+// The kernel reads them from global memory (a device copy, 64-byte aligned).
 struct Cg1Maps {
   CUtensorMap r[2], p[2], hx, hy;
+  CUtensorMap fr[2], fp[2], fhx, fhy;
 };
 
 int cg1_make_maps(const Grid &g, double *r0, double *r1, double *p0, double *p1, double *hx,
                   double *hy, Cg1Maps *m);
+// The FP32 maps of the mixed-precision solve.
+int cg1_make_maps_f32(const Grid &g, float *r0, float *r1, float *p0, float *p1, float *hx,
+                      float *hy, Cg1Maps *m);
 size_t cg1_smem_bytes();
 // Co-resident blocks for a cooperative launch, at most one per tile.
 int cg1_blocks(int device, const Grid &g, int *blocks);

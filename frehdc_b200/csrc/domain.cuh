@@ -58,6 +58,8 @@ struct Params {
   double dx, dy, dt, g, NUx, NUy, Kx, Ky, manningN, hD, minDepth, wtfh, CFLl, CFLh;
   double offset, surfmin, dsurf, tidePS, subR, dxf, dyf, eps;
   int Ne, useThinLayer, useScalar, tideFirst, tideLen, maxIter;
+  int mixed;          // CG: FP32 inner iterations inside FP64 iterative refinement
+  double eps_inner;   // relative residual reduction of one FP32 inner solve
   // geometry source
   int geom_fine;          // 0: tables, 1: fine bottoms
   const double *tab;      // tables: 10 * Ne * N, level-major (subgrid.c:118-119)
@@ -97,6 +99,9 @@ struct View {
   // per-step work
   double *EnXP, *EnYP, *Gx, *Gy, *Ct, *b;
   double *Hx, *Hy;  // symmetrically scaled couplings of the single-sweep CG
+  // FP32 arrays of the mixed-precision CG (null unless enabled): scaled residual
+  // and direction (two buffers each), correction, scaled couplings
+  float *fr0, *fr1, *fp0, *fp1, *fd, *fhx, *fhy;
   double *x, *r, *p0, *p1, *q;
   double *cellV, *Sm, *Fuu, *Fvv;
   unsigned char *rmv;

@@ -29,6 +29,8 @@ struct frehd_domain {
   double *EnXP = nullptr, *EnYP = nullptr, *Gx = nullptr, *Gy = nullptr, *Ct = nullptr,
          *b = nullptr;
   double *Hx = nullptr, *Hy = nullptr;
+  float *fr0 = nullptr, *fr1 = nullptr, *fp0 = nullptr, *fp1 = nullptr, *fd = nullptr,
+        *fhx = nullptr, *fhy = nullptr;  // mixed-precision CG (allocated when enabled)
   double *x = nullptr, *r = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr;
   double *cellV = nullptr, *Sm = nullptr, *Fuu = nullptr, *Fvv = nullptr;
   unsigned char *rmv = nullptr;

@@ -133,6 +133,7 @@ PHASE_EXPLICIT, PHASE_SOLVE, PHASE_UPDATE = 1, 2, 3
 X0_ZERO, X0_SURFACE = 0, 1
 CG_SINGLE_SWEEP, CG_TWO_PHASE = 0, 1
 DECOUPLED_AS_ASSEMBLED, DECOUPLED_ELIMINATED = 0, 1
+PRECISION_FP64, PRECISION_MIXED = 0, 1
 STATUS = {0: "ok", 1: "invalid", 2: "unsupported", 3: "cuda", 4: "nomem", 5: "cg_noconverge",
           6: "cfl", 7: "timeout", 8: "state"}
 
@@ -155,6 +156,7 @@ def _declare_domain(L: C.CDLL) -> None:
     L.frehd_domain_set_solver.argtypes = [_vp, C.c_int]
     L.frehd_domain_set_cg_schedule.argtypes = [_vp, C.c_int]
     L.frehd_domain_set_decoupled.argtypes = [_vp, C.c_int]
+    L.frehd_domain_set_precision.argtypes = [_vp, C.c_int, C.c_double]
     L.frehd_domain_upload_state.argtypes = [_vp, C.POINTER(State)]
     L.frehd_domain_download_state.argtypes = [_vp, C.POINTER(State)]
     L.frehd_domain_init.argtypes = [_vp] + [_dp] * 7 + [C.c_int]
@@ -228,6 +230,9 @@ class Domain:
 
     def set_decoupled(self, mode: int):
         check(lib().frehd_domain_set_decoupled(self.h, mode), "set_decoupled")
+
+    def set_precision(self, mode: int, eps_inner: float = 1e-5):
+        check(lib().frehd_domain_set_precision(self.h, mode, eps_inner), "set_precision")
 
     def init(self, bottom, bottomXP, bottomYP, surf0, u0=None, v0=None, S0=None,
              round_trip_output: bool = True):
@@ -456,7 +461,8 @@ def cg_solve_noalloc(nx: int, ny: int, Ct: int, Gx: int, Gy: int, b: int, x: int
 
 
 def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0_ZERO,
-                     schedule: int = CG_SINGLE_SWEEP, decoupled: int = DECOUPLED_AS_ASSEMBLED):
+                     schedule: int = CG_SINGLE_SWEEP, decoupled: int = DECOUPLED_AS_ASSEMBLED,
+                     precision: int = PRECISION_FP64, eps_inner: float = 1e-5):
     """A Domain initialised from a generated deck (frehdc_b200.deck)."""
     from . import deck as D
     d = Domain(D.config_dict(deck), device)
@@ -472,5 +478,7 @@ def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0
     d.set_solver(x0)
     d.set_cg_schedule(schedule)
     d.set_decoupled(decoupled)
+    if precision != PRECISION_FP64:
+        d.set_precision(precision, eps_inner)
     d.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
     return d

@@ -237,6 +237,19 @@ int frehd_domain_set_cg_schedule(frehd_domain *d, int schedule);
 enum { FREHD_DECOUPLED_AS_ASSEMBLED = 0, FREHD_DECOUPLED_ELIMINATED = 1 };
 int frehd_domain_set_decoupled(frehd_domain *d, int mode);
 
+/* Precision of the solve (no counterpart in the reference, which is FP64).
+ * FREHD_PRECISION_FP64 (default): the CG in FP64.
+ * FREHD_PRECISION_MIXED: iterative refinement; each refinement forms the
+ * residual in FP64, solves the scaled system in FP32 (all dot products and
+ * norms accumulated in FP64) until its residual fell by eps_inner (e.g. 1e-5),
+ * and adds the correction to the FP64 solution.  Stops on the same FP64
+ * residual test ||r|| < eps*||b||; a refinement that does not gain a factor 10
+ * hands the step to the FP64 solve (cg_fallback = 2).  Single-sweep schedule
+ * only; costs 7 FP32 arrays (28 bytes per cell) more device memory.  The
+ * stencil kernels stay FP64. */
+enum { FREHD_PRECISION_FP64 = 0, FREHD_PRECISION_MIXED = 1 };
+int frehd_domain_set_precision(frehd_domain *d, int mode, double eps_inner);
+
 /* The free-surface CG solve alone, for callers that cannot allocate device
  * memory.  No counterpart in the reference (it solves through laspack inside
  * the step, nsfunctions.c:1004-1017); this entry point exists for hosts whose

@@ -85,3 +85,19 @@ def build_library(verbose: bool = False, force: bool = False) -> str:
 
 if __name__ == "__main__":
     build_library(verbose=True, force="--force" in sys.argv)
+
+
+DROPIN = os.path.join(HERE, "dropin")
+DROPIN_BIN = os.path.join(DROPIN, "_build", "frehd_dropin")
+
+
+def build_dropin(ref_src: str, quiet: bool = True) -> str | None:
+    """Build the drop-in host (the reference's host program with nssolve_b200.c
+    in place of nssolve.c, linked against the library) from the reference
+    sources under ref_src.  Without those sources an existing binary is kept;
+    returns its path, or None when there is none."""
+    if os.path.isdir(os.path.join(ref_src, "frehdc5+")):
+        build_library(verbose=False)
+        subprocess.run(["make", "-C", DROPIN, "-j8", f"REF={ref_src}"], check=True,
+                       stdout=subprocess.DEVNULL if quiet else None)
+    return DROPIN_BIN if os.path.exists(DROPIN_BIN) else None

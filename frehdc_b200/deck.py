@@ -352,16 +352,20 @@ DATA_DAT_LABELS = [
 
 
 def write_reference_deck(deck: Deck, path: str, tables: np.ndarray | None = None,
-                         binary_tables: bool = False) -> str:
+                         binary_tables: bool = False, out_steps: int | None = None) -> str:
     """Write data.dat + input/ for the reference model under ``path``.
 
     binary_tables additionally writes each subgrid table as raw little-endian
     doubles (``<name>.dat.bin``); the oracle harness reads those when present
-    instead of parsing hundreds of millions of text values.
+    instead of parsing hundreds of millions of text values.  out_steps sets the
+    output interval OutItvl in steps (default: beyond the last step).
     """
     os.makedirs(os.path.join(path, "input", "subdata"), exist_ok=True)
     os.makedirs(os.path.join(path, "output"), exist_ok=True)
-    vals = data_dat_values(deck)
+    out_hours = None
+    if out_steps is not None:  # OutItvl = hours*3600/dt truncated (configuration.c:27)
+        out_hours = (out_steps + 0.5) * deck.spec.dt / 3600.0
+    vals = data_dat_values(deck, out_hours)
     with open(os.path.join(path, "data.dat"), "w") as f:
         f.write("# FrehdC input deck written by frehdc_b200.deck\n")
         for v, lab in zip(vals, DATA_DAT_LABELS):

@@ -1,8 +1,8 @@
 /*
- * Link-time wraps used when the unchanged reference sources are built as the
- * oracle (test infrastructure; see oracle/ref/Makefile).  No reference source
- * file is edited; these definitions replace calls across translation units via
- * `ld --wrap`.
+ * Link-time fixes for building the reference's unchanged host program: the
+ * drop-in host (frehdc_b200/dropin/Makefile) and the oracle builds
+ * (oracle/ref/Makefile) both link them.  No reference source file is edited;
+ * these definitions replace calls across translation units via `ld --wrap`.
  *
  *  __wrap_dateNum   utilities.c:97-109 builds the date from getTime(), whose
  *                   char val[N] is passed to atof() without a terminator
@@ -13,7 +13,7 @@
  *                   read from it as raw little-endian values (the deck writer
  *                   emits the same doubles in both forms) -- this only skips
  *                   text parsing of large subgrid tables.
- *  __wrap_malloc/free (parity build only, -DFREHD_ZERO_GUARD): every block is
+ *  __wrap_malloc/free (parity builds, -DFREHD_ZERO_GUARD): every block is
  *                   zero-filled and surrounded by zero guard zones, so the
  *                   reference's out-of-bounds reads (velocityInterp
  *                   nsfunctions.c:342-345, limiterCFL nsfunctions.c:465-468,
@@ -33,7 +33,7 @@ time_t __wrap_dateNum(char *t) {
   memset(&tm, 0, sizeof(tm));
   int y = 0, m = 0, d = 0;
   if (sscanf(t, "%4d-%2d-%2d", &y, &m, &d) != 3) {
-    fprintf(stderr, "oracle: cannot parse start date '%s'\n", t);
+    fprintf(stderr, "frehd host: cannot parse start date '%s'\n", t);
     exit(2);
   }
   tm.tm_year = y - 1900;
@@ -55,7 +55,7 @@ void __wrap_ReadFile(double *arr, char filename[], int N) {
   size_t got = fread(arr, sizeof(double), (size_t)N, f);
   fclose(f);
   if (got != (size_t)N) {
-    fprintf(stderr, "oracle: %s holds %zu of %d values\n", bin, got, N);
+    fprintf(stderr, "frehd host: %s holds %zu of %d values\n", bin, got, N);
     exit(2);
   }
 }

@@ -1,12 +1,13 @@
-/* Aborting definitions of the MPI calls the reference names (test infrastructure;
- * the oracle runs with useMPI = 0 so none of them is ever called). */
+/* Aborting definitions of the MPI calls the reference host program names, for
+ * builds of it without an MPI installation (the drop-in host and the oracle
+ * builds).  Both run with useMPI = 0, so none of them is ever called. */
 #include <stdio.h>
 #include <stdlib.h>
 
 #include "mpi.h"
 
 static int unreachable(const char *f) {
-  fprintf(stderr, "oracle: %s called with useMPI = 0\n", f);
+  fprintf(stderr, "frehd host: %s called with useMPI = 0\n", f);
   abort();
   return 1;
 }

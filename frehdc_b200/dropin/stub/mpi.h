@@ -1,11 +1,12 @@
 /*
  * Minimal MPI declarations so that the reference's mpifunctions.c and FREHD.c
- * compile without an MPI installation.  The oracle runs the reference with
- * useMPI = 0, where none of these functions is reached; each definition in
- * mpi_stub.c aborts if it ever is.  Test infrastructure only.
+ * compile without an MPI installation (drop-in host and oracle builds).  Both
+ * run the reference host with useMPI = 0, where none of these functions is
+ * reached; each definition in mpi_stub.c aborts if it ever is.  A build with a
+ * real MPI drops this directory from the include path and links libmpi.
  */
-#ifndef FREHD_ORACLE_MPI_STUB_H
-#define FREHD_ORACLE_MPI_STUB_H
+#ifndef FREHD_MPI_STUB_H
+#define FREHD_MPI_STUB_H
 
 typedef int MPI_Comm;
 typedef int MPI_Datatype;

@@ -420,14 +420,41 @@ def mix_specs(n: int, seed: int, smin: int, smax: int, steps: int):
     return out
 
 
+def _dist_init():
+    """(world size, rank, device) of this process; under torchrun one process
+    per GPU with an NCCL group used only for host-side gathers of metrics."""
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def _dist_done(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_batched_form(args):
     """Cell-steps/s of a mix of domains stepped as one batch, against the same
-    mix stepped one domain at a time through the single-domain API."""
+    mix stepped one domain at a time through the single-domain API.  Under
+    torchrun the mix is partitioned across ranks by cell count
+    (frehdc_b200.shard.balance); each rank batches its share on its own GPU
+    and the slowest rank's device time sets the whole-job rate."""
     import torch
 
     from frehdc_b200 import deck as D
-    from frehdc_b200 import native
-    specs = mix_specs(args.mix, 77, args.mix_min, args.mix_max, args.steps + args.warmup + 5)
+    from frehdc_b200 import native, shard
+    ws, rank, dev = _dist_init()
+    specs_all = mix_specs(args.mix, 77, args.mix_min, args.mix_max, args.steps + args.warmup + 5)
+    mine = shard.balance([sp.nx * sp.ny for sp in specs_all], ws)[rank]
+    specs = [specs_all[i] for i in mine]
     t0 = time.time()
     decks = [D.make_deck(sp) for sp in specs]
     gen_s = time.time() - t0
@@ -436,7 +463,7 @@ def run_batched_form(args):
     # plain form: each domain alone, device time of its K steps (kernel events)
     plain_ms = 0.0
     for dk in decks:
-        g = native.domain_from_deck(dk)
+        g = native.domain_from_deck(dk, device=dev)
         g.run(1, args.warmup)
         g.sync()
         g.set_profiling(True)
@@ -446,24 +473,30 @@ def run_batched_form(args):
         plain_ms += sum(kt[k] for k in ("explicit_ms", "cg_ms", "update_geo_ms", "update_vel_ms",
                                         "finish_ms"))
         g.close()
-    # batched form (packing granularity and inner tolerance from the autotuner)
+    # batched form (packing granularity and inner tolerance from the autotuner,
+    # tuned on rank 0's share and used by every rank)
     prec = native.PRECISION_MIXED if args.precision == "mixed" else native.PRECISION_FP64
     tuning = None
     if args.cells_per_cta <= 0:
         from frehdc_b200 import autotune
-        tuning = autotune.tune(decks, args.budget_gb << 30, prec)
+        if rank == 0:
+            tuning = autotune.tune(decks, args.budget_gb << 30, prec, device=dev)
+        tuning = shard.broadcast(tuning, ws)
         args.cells_per_cta = tuning["best"]["cells_per_cta"]
         args.eps_inner = tuning["best"]["eps_inner"]
-    doms = [native.domain_from_deck(dk, precision=prec, eps_inner=args.eps_inner) for dk in decks]
-    b = native.Batch(args.budget_gb << 30, args.cells_per_cta)
+    doms = [native.domain_from_deck(dk, device=dev, precision=prec, eps_inner=args.eps_inner)
+            for dk in decks]
+    b = native.Batch(args.budget_gb << 30, args.cells_per_cta, dev)
     for g in doms:
         b.admit(g, 1)
     for _ in range(args.warmup):
         b.step()
     b.sync()
-    st = torch.cuda.ExternalStream(b.stream())
+    if ws > 1:
+        torch.distributed.barrier()
+    st = torch.cuda.ExternalStream(b.stream(), device=dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(0) as clk:
+    with ClockSampler(dev) as clk:
         e0.record(st)
         for _ in range(K):
             b.step()
@@ -480,7 +513,7 @@ def run_batched_form(args):
         import numpy as np
         worst = {"eta_max_abs_m": 0.0, "u_max_rel": 0.0, "v_max_rel": 0.0, "volume_rel": 0.0}
         for g, dk in zip(doms, decks):
-            r = native.domain_from_deck(dk)
+            r = native.domain_from_deck(dk, device=dev)
             r.run(1, args.warmup + K)
             n_ = dk.spec.nx * dk.spec.ny
             a, c = g.download(["surf", "uuXP", "vvYP"]), r.download(["surf", "uuXP", "vvYP"])
@@ -495,65 +528,96 @@ def run_batched_form(args):
         errors = worst
     for g in doms:
         g.close()
-    total = float(sum(cells)) * K
-    line = {"metric": METRIC, "form": "batched", "value": total / (batch_ms / 1e3),
-            "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": args.warmup,
-            "ms_per_step": batch_ms / K, "higher_is_better": True, "scaling": "weak",
+    parts = shard.gather({"batch_ms": batch_ms, "plain_ms": plain_ms, "cells": int(sum(cells)),
+                          "domains": len(decks), "errors": errors, "clocks": clk.summary(),
+                          "info": info, "gen_s": gen_s}, ws)
+    _dist_done(ws)
+    if rank != 0:
+        return 0
+    t_batch = max(p["batch_ms"] for p in parts)
+    t_plain = max(p["plain_ms"] for p in parts)
+    total_cells = sum(p["cells"] for p in parts)
+    total = float(total_cells) * K
+    line = {"metric": METRIC, "form": "batched", "value": total / (t_batch / 1e3),
+            "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": args.warmup,
+            "ms_per_step": t_batch / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
             "data": "synthetic",
             "config": {"precision": args.precision,
-                       "workload": f"{len(specs)} seeded basins, sides log-uniform "
+                       "workload": f"{len(specs_all)} seeded basins, sides log-uniform "
                                    f"{args.mix_min}-{args.mix_max} (square or 1:4), dx 10 m, "
                                    "dt 1 s, depth 0.3-8 m, 0-40% dry, tide 0.1-0.5 m, "
                                    "n 0.02-0.04, 4x4 subgrid, 1 scalar",
-                       "cells": int(sum(cells)), "cells_per_cta": args.cells_per_cta,
-                       "deck_gen_s": round(gen_s, 1)},
-            "plain_form_same_mix": {"value": total / (plain_ms / 1e3), "unit": UNIT,
+                       "cells": int(total_cells), "cells_per_cta": args.cells_per_cta,
+                       "sharding": "by cell count over ranks" if ws > 1 else None,
+                       "deck_gen_s": round(max(p["gen_s"] for p in parts), 1)},
+            "plain_form_same_mix": {"value": total / (t_plain / 1e3), "unit": UNIT,
                                     "note": "each domain stepped alone, device time of its "
                                             "kernels summed over the mix"},
-            "batch": info, "gpu_launches": 5 * K, "clocks": clk.summary()}
+            "batch": parts[0]["info"] if ws == 1 else [p["info"] for p in parts],
+            "gpu_launches": 5 * K, "clocks": parts[0]["clocks"]}
+    if ws > 1:
+        line["per_rank"] = [{"domains": p["domains"], "cells": p["cells"], "batch_ms": p["batch_ms"]}
+                            for p in parts]
     line["speedup_vs_plain_form"] = line["value"] / line["plain_form_same_mix"]["value"]
     line["config"]["eps_inner"] = args.eps_inner if args.precision == "mixed" else None
     if tuning is not None:
         line["autotune"] = tuning
-    if errors is not None:
-        line["errors_vs_fp64"] = errors
+    if args.precision == "mixed":
+        errs = [p["errors"] for p in parts if p["errors"]]
+        line["errors_vs_fp64"] = {k: max(e[k] for e in errs) for k in errs[0]} if errs else None
     print(json.dumps(line), flush=True)
     return 0
 
 
 def run_served_form(args):
-    """A stream of requests with Poisson arrivals served by continuous batching."""
+    """A stream of requests with Poisson arrivals served by continuous batching.
+    Under torchrun each request goes to the rank with the least work assigned
+    so far, in arrival order (frehdc_b200.shard.assign_stream); every rank
+    serves its share on its own GPU at the original arrival times."""
     import numpy as np
 
     from frehdc_b200 import deck as D
-    from frehdc_b200 import serve
+    from frehdc_b200 import native, serve, shard
+    ws, rank, dev = _dist_init()
     rng = np.random.default_rng(5)
     specs = mix_specs(args.requests, 91, args.mix_min, args.mix_max, 10)
     steps = rng.integers(args.req_steps_min, args.req_steps_max + 1, size=len(specs))
-    t0 = time.time()
-    decks = [D.make_deck(sp.replace(steps=int(k) + 5)) for sp, k in zip(specs, steps)]
-    gen_s = time.time() - t0
     arr = serve.poisson_arrivals(len(specs), args.rate, 17)
-    reqs = [serve.Request(i, dk, int(k), float(a)) for i, (dk, k, a) in enumerate(zip(decks, steps, arr))]
-    from frehdc_b200 import native
+    owner = shard.assign_stream(arr, [sp.nx * sp.ny * int(k) for sp, k in zip(specs, steps)], ws)
+    mine = [i for i in range(len(specs)) if owner[i] == rank]
+    t0 = time.time()
+    decks = {i: D.make_deck(specs[i].replace(steps=int(steps[i]) + 5)) for i in mine}
+    gen_s = time.time() - t0
+    reqs = [serve.Request(i, decks[i], int(steps[i]), float(arr[i])) for i in mine]
     prec = native.PRECISION_MIXED if args.precision == "mixed" else native.PRECISION_FP64
 
     def build(req):
-        return native.domain_from_deck(req.deck, precision=prec, eps_inner=args.eps_inner)
+        return native.domain_from_deck(req.deck, device=dev, precision=prec,
+                                       eps_inner=args.eps_inner)
     if args.cells_per_cta <= 0:
         args.cells_per_cta = 32768.0
-    with ClockSampler(0) as clk:
-        res = serve.serve(reqs, args.budget_gb << 30, args.cells_per_cta, build=build)
-    line = {"metric": METRIC, "form": "served", "value": res["cell_steps_per_s"], "unit": UNIT,
-            "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+    if ws > 1:
+        import torch
+        torch.distributed.barrier()
+    with ClockSampler(dev) as clk:
+        res = serve.serve(reqs, args.budget_gb << 30, args.cells_per_cta, device=dev, build=build)
+    parts = shard.gather({**res, "clocks": clk.summary(), "gen_s": gen_s}, ws)
+    _dist_done(ws)
+    if rank != 0:
+        return 0
+    merged = shard.merge_served(parts)
+    line = {"metric": METRIC, "form": "served", "value": merged["cell_steps_per_s"], "unit": UNIT,
+            "n_gpus": ws, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
-            "p50_latency_s": res["p50_s"], "p99_latency_s": res["p99_s"],
-            "config": {"workload": f"{len(reqs)} requests, Poisson arrivals {args.rate}/s, sides "
+            "p50_latency_s": merged["p50_s"], "p99_latency_s": merged["p99_s"],
+            "config": {"workload": f"{len(specs)} requests, Poisson arrivals {args.rate}/s, sides "
                                    f"log-uniform {args.mix_min}-{args.mix_max}, steps "
                                    f"{args.req_steps_min}-{args.req_steps_max}, 1 scalar, {args.precision}",
-                       "cells_per_cta": args.cells_per_cta, "deck_gen_s": round(gen_s, 1)},
-            "serving": res, "clocks": clk.summary()}
+                       "cells_per_cta": args.cells_per_cta,
+                       "sharding": "least assigned work, arrival order" if ws > 1 else None,
+                       "deck_gen_s": round(max(p["gen_s"] for p in parts), 1)},
+            "serving": merged, "clocks": parts[0]["clocks"]}
     print(json.dumps(line), flush=True)
     return 0
 

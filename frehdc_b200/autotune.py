@@ -19,12 +19,14 @@ EPS_INNER = (1e-4, 1e-5, 1e-6)
 
 
 def time_batch(decks, cells_per_cta: float, steps: int, warmup: int, budget: int,
-               precision: int = native.PRECISION_FP64, eps_inner: float = 1e-5) -> float:
+               precision: int = native.PRECISION_FP64, eps_inner: float = 1e-5,
+               device: int = 0) -> float:
     """Device milliseconds of `steps` batch steps of the decks' domains, or None
     when the mix does not fit the batch (memory budget or CG CTA capacity)."""
     import torch
-    doms = [native.domain_from_deck(dk, precision=precision, eps_inner=eps_inner) for dk in decks]
-    b = native.Batch(budget, cells_per_cta)
+    doms = [native.domain_from_deck(dk, device=device, precision=precision, eps_inner=eps_inner)
+            for dk in decks]
+    b = native.Batch(budget, cells_per_cta, device)
     try:
         for g in doms:
             if b.try_admit(g, 1) is None:
@@ -49,12 +51,13 @@ def time_batch(decks, cells_per_cta: float, steps: int, warmup: int, budget: int
 
 
 def tune(decks, budget: int, precision: int = native.PRECISION_FP64, steps: int = 4,
-         warmup: int = 2, cells_candidates=CELLS_PER_CTA, eps_candidates=EPS_INNER) -> dict:
+         warmup: int = 2, cells_candidates=CELLS_PER_CTA, eps_candidates=EPS_INNER,
+         device: int = 0) -> dict:
     """The fastest (cells_per_cta, eps_inner) on this mix, and every timing."""
     eps_list = eps_candidates if precision == native.PRECISION_MIXED else (1e-5,)
     results = []
     for cpc, ein in itertools.product(cells_candidates, eps_list):
-        ms = time_batch(decks, cpc, steps, warmup, budget, precision, ein)
+        ms = time_batch(decks, cpc, steps, warmup, budget, precision, ein, device)
         if ms is None:  # the mix does not fit with this granularity
             continue
         results.append({"cells_per_cta": cpc, "eps_inner": ein, "ms_per_step": ms / steps})

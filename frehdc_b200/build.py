@@ -5,6 +5,13 @@ with --fmad=false so that a*b+c is never contracted: together with an unchanged
 evaluation order this keeps their doubles identical to the host restatement of
 the reference step.  Objects are cached under ``frehdc_b200/_build`` and rebuilt
 when a source or header is newer.
+
+Each .cu file is compiled whole-program (no relocatable device code; no device
+symbol crosses files).  With -rdc the device linker lays out the function-scope
+__shared__ variables of all files in one range, and a kernel's static shared
+memory becomes the end of that range: k_cg1 grew from 3.9 KB to 32 KB and
+k_update_vel from 0.2 KB to 13 KB, which shrank the L1 carve-out and cost the
+CG 12 % at 4096 x 4096 (16.0 -> 14.3 ms per solve once removed).
 """
 from __future__ import annotations
 
@@ -67,7 +74,7 @@ def build_library(verbose: bool = False, force: bool = False) -> str:
         if not force and not _stale(obj, [src] + hdrs + [__file__]):
             continue
         extra = EXTRA.get(base, EXTRA["default"])
-        cmd = [nvcc] + ARCH + COMMON + extra + ["-dc" if src.endswith(".cu") else "-c", src, "-o", obj]
+        cmd = [nvcc] + ARCH + COMMON + extra + ["-c", src, "-o", obj]
         if src.endswith(".cpp"):
             cmd = [shutil.which("g++") or "g++", "-O2", "-fPIC", "-std=c++17", "-fno-fast-math",
                    "-I", INCLUDE, "-I", CSRC, "-I", "/usr/local/cuda/include", "-c", src, "-o", obj]

@@ -181,7 +181,7 @@ void mark(cudaEvent_t *ev, int slot, cudaStream_t st) {
 int launch_update(frehd_domain *d, const View &w, cudaEvent_t *ev = nullptr) {
   const dim3 gb = tile_grid(d), bb(32, 8);
   mark(ev, 2, d->stream);
-  k_update_geo<false><<<gb, bb, 0, d->stream>>>(w);
+  k_update_geo<<<gb, bb, 0, d->stream>>>(w);
   mark(ev, 3, d->stream);
   k_update_vel<<<gb, bb, 0, d->stream>>>(w);
   mark(ev, 4, d->stream);
@@ -612,7 +612,7 @@ extern "C" int frehd_domain_init(frehd_domain *d, const double *bottom, const do
   if (rc) return rc;
   {
     View w = make_view(d);
-    k_update_geo<true><<<tile_grid(d), dim3(32, 8), 0, d->stream>>>(w);
+    k_update_geo_init<<<tile_grid(d), dim3(32, 8), 0, d->stream>>>(w);
     CUDA_TRY(cudaGetLastError());
     std::swap(d->ind[0], d->ind[1]);  // the evaluated indices become current
   }

@@ -27,8 +27,8 @@ __device__ __forceinline__ double warp_max(double v) {
 }
 
 __global__ void k_explicit(View w);
-template <bool kInit>
 __global__ void k_update_geo(View w);
+__global__ void k_update_geo_init(View w);
 __global__ void k_update_vel(View w);
 __global__ void k_finish(View w, int nblocks_vel, StepOut *out);
 __global__ void k_ref_to_padded(double *dst, const double *src, long n, int nx, int ny, int pitch);

@@ -535,14 +535,15 @@ static __device__ __forceinline__ void update_geo_tile(const View &w, int bx, in
   for (int a = 0; a < 8; ++a) arr[a][k] = val[a];
 }
 
-template <bool kInit>
 __global__ void __launch_bounds__(TBX *TBY, FREHD_GEO_MIN_BLOCKS) k_update_geo(View w) {
-  if (!kInit && *(volatile int *)&w.sc->status != FREHD_OK) return;
-  update_geo_tile<kInit>(w, blockIdx.x, blockIdx.y);
+  if (*(volatile int *)&w.sc->status != FREHD_OK) return;
+  update_geo_tile<false>(w, blockIdx.x, blockIdx.y);
 }
 
-template __global__ void k_update_geo<false>(View);
-template __global__ void k_update_geo<true>(View);
+// The geometry of the initial state (Init's computeSubArea + combineSubArea).
+__global__ void __launch_bounds__(TBX *TBY, FREHD_GEO_MIN_BLOCKS) k_update_geo_init(View w) {
+  update_geo_tile<true>(w, blockIdx.x, blockIdx.y);
+}
 
 // ---------------------------------------------------------------- k_update_vel
 // Final velocity of the east face of (i, j): updateVelocitySub (subgrid.c:1084-1176),

@@ -331,7 +331,15 @@ extern "C" int frehd_domain_set_tables(frehd_domain *d, int Ne, const double *ta
 }
 
 extern "C" int frehd_domain_set_fine_bottoms(frehd_domain *d, int r, const double *zf, long fpitch) {
-  if (!d || !zf || r <= 0) return fail(FREHD_ERR_INVALID, "bad argument");
+  return frehd_domain_set_fine_bottoms_ex(d, r, zf, fpitch, 0);
+}
+
+extern "C" int frehd_domain_set_fine_bottoms_ex(frehd_domain *d, int r, const double *zf, long fpitch,
+                                                int flags) {
+  if (!d || !zf || r <= 0 || (flags & ~FREHD_GEOM_BLOCK_CHECK))
+    return fail(FREHD_ERR_INVALID, "bad argument");
+  const int check_block = (flags & FREHD_GEOM_BLOCK_CHECK) && r > 1;
+  if (check_block && r > 8) return fail(FREHD_ERR_UNSUPPORTED, "block check needs r <= 8 (r = %d)", r);
   if (fpitch < (long)d->gr.nx * r) return fail(FREHD_ERR_INVALID, "fine pitch too small");
   if (std::fabs(d->cfg.dx / d->cfg.dxf - r) > 1e-9 * r)
     return fail(FREHD_ERR_INVALID, "r=%d does not match dx/dxf", r);
@@ -350,6 +358,7 @@ extern "C" int frehd_domain_set_fine_bottoms(frehd_domain *d, int r, const doubl
   d->bytes += (long long)(sizeof(double) * rows * cols);
   d->p.fpitch = cols;
   d->p.r = r;
+  d->p.check_block = check_block;
   d->geom_set = 1;
   return FREHD_OK;
 }

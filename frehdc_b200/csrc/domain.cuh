@@ -62,6 +62,7 @@ struct Params {
   double eps_inner;   // relative residual reduction of one FP32 inner solve
   // geometry source
   int geom_fine;          // 0: tables, 1: fine bottoms
+  int check_block;        // fine bottoms: block-check face areas (FREHD_GEOM_BLOCK_CHECK)
   const double *tab;      // tables: 10 * Ne * N, level-major (subgrid.c:118-119)
   const double *zf;       // fine bottoms, zf[fj*fpitch + fi]
   long fpitch;

@@ -257,12 +257,12 @@ __device__ __forceinline__ double level_surf(const Params &p, int k) {
 __device__ __forceinline__ void level_values(const Params &p, int i, int j, int k, frehd_cell_levels *o,
                                              int part) {
   if (p.geom_fine) {
-    if (p.r == 4)
+    if (p.r == 4 && !p.check_block)
       frehd_cell_levels_r4(p.zf, p.fpitch, p.nx, p.ny, i, j, frehd_level(p.surfmin, p.dsurf, k),
                            p.dxf * p.dyf, p.dxf, part, o);
-    else
+    else  // every value (a part's caller reads only its own)
       frehd_cell_levels_at(p.zf, p.fpitch, p.nx, p.ny, p.r, i, j, frehd_level(p.surfmin, p.dsurf, k),
-                           p.dxf * p.dyf, p.dxf, o);
+                           p.dxf * p.dyf, p.dxf, p.check_block, o);
   } else {
     const long N = (long)p.nx * p.ny, T = N * p.Ne;
     const double *t = p.tab + (long)k * N + (long)j * p.nx + i;

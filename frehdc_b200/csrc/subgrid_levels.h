@@ -18,7 +18,22 @@
  * MATLAB arrays there are (x, y, level) with x the first (fastest) index, which is
  * the reference C layout ii = j*nx + i.  Summation order is fixed here: MATLAB's
  * sum(A(:)) is a flat x-fastest sweep and sum(sum(A)) is a sum of column (x) sums.
- * The block-check option (checkBlock=1, bwlabel based) is not implemented.
+ *
+ * Block check (checkBlock = 1, script_CreateSubAreaWithBlockV16.m:27,214-216,
+ * 262-283 and ComputeFaceAreaWithBlockCheck.m:14-171), for 1 < r <= 8:
+ *   1. a block's wet pixels (level > bottom) are reduced to their largest
+ *      4-connected cluster (bwlabel(.,4), :33-55; equal sizes: the cluster that
+ *      bwlabel numbers first, i.e. whose first pixel comes first in MATLAB's
+ *      column-major scan, x fastest); a cluster below 0.01*r*r pixels leaves the
+ *      block dry;
+ *   2. a face between two blocks gets sum over its pixel pairs of
+ *      min(depth masked by one block's cluster, depth masked by the other's) * dx
+ *      (:127-172), which is zero exactly where the blocks' clusters do not touch
+ *      across the face, so the cross-cell blocking flags (:88-123) change nothing
+ *      further;
+ *   3. a face on the domain boundary keeps its unmasked edge sum (:140-145,
+ *      :162-167) unless the block's cluster has no pixel on that edge (:61-76).
+ * V, Z and the half volumes never use the clusters.
  *
  * Fine array layout: zf[fj * fpitch + fi], fi in [0, nx*r) along x, fj along y.
  */
@@ -46,6 +61,66 @@ FREHD_HD double frehd_min2(double a, double b) { return b < a ? b : a; }
 /* Half-block split round(r/2) of the pre-processor (MATLAB round: .5 away from 0). */
 FREHD_HD int frehd_half(int r) { return (r + 1) / 2; }
 
+/* Wet pixels (h > z) of the r x r block at b, bit fj*r + fi (r <= 8). */
+FREHD_HD unsigned long long frehd_wet_bits(const double *b, long fpitch, int r, double h) {
+  unsigned long long m = 0;
+  for (int fj = 0; fj < r; ++fj)
+    for (int fi = 0; fi < r; ++fi)
+      if (frehd_fine_depth(h, b[(long)fj * fpitch + fi]) > 0.0) m |= 1ull << (fj * r + fi);
+  return m;
+}
+
+FREHD_HD int frehd_popc64(unsigned long long v) {
+#ifdef __CUDA_ARCH__
+  return __popcll(v);
+#else
+  return __builtin_popcountll(v);
+#endif
+}
+
+/* The largest 4-connected cluster of the wet bits m of an r x r block (bit
+ * fj*r + fi).  Clusters are grown from their lowest bit in increasing order, so
+ * among equal sizes the one whose first pixel comes first in MATLAB's
+ * column-major (x fastest) scan is kept, as bwlabel numbers it first.  A cluster
+ * below 0.01*r*r pixels leaves the block dry (ComputeFaceAreaWithBlockCheck.m:33-55). */
+FREHD_HD unsigned long long frehd_cluster_bits(unsigned long long m, int r) {
+  const unsigned long long all = r * r >= 64 ? ~0ull : ((1ull << (r * r)) - 1ull);
+  unsigned long long first = 0, last = 0;
+  for (int fj = 0; fj < r; ++fj) {
+    first |= 1ull << (fj * r);
+    last |= 1ull << (fj * r + r - 1);
+  }
+  unsigned long long best = 0, rem = m & all;
+  int best_n = 0;
+  while (rem) {
+    unsigned long long c = rem & (~rem + 1ull);
+    for (;;) {
+      unsigned long long g = c | ((c << 1) & ~first) | ((c >> 1) & ~last) | (c << r) | (c >> r);
+      g &= m & all;
+      if (g == c) break;
+      c = g;
+    }
+    const int n = frehd_popc64(c);
+    if (n > best_n) {
+      best = c;
+      best_n = n;
+    }
+    rem &= ~c;
+  }
+  if ((double)best_n < 0.01 * r * r) return 0;
+  return best;
+}
+
+/* Cluster of block (i, j) at level h. */
+FREHD_HD unsigned long long frehd_block_cluster(const double *zf, long fpitch, int r, int i, int j,
+                                                double h) {
+  return frehd_cluster_bits(frehd_wet_bits(zf + (long)j * r * fpitch + (long)i * r, fpitch, r, h), r);
+}
+
+FREHD_HD double frehd_masked(double d, unsigned long long m, int bit) {
+  return ((m >> bit) & 1ull) ? d : 0.0;
+}
+
 /*
  * All ten table values of cell (i, j) at level h (level in the deck's own datum,
  * i.e. without the model's bathymetry offset).
@@ -55,7 +130,7 @@ FREHD_HD int frehd_half(int r) { return (r + 1) / 2; }
  */
 FREHD_HD void frehd_cell_levels_at(const double *zf, long fpitch, int nx, int ny, int r,
                                    int i, int j, double h, double dA, double dxf,
-                                   frehd_cell_levels *o) {
+                                   int check_block, frehd_cell_levels *o) {
   const long fi0 = (long)i * r, fj0 = (long)j * r;
   const double *b = zf + fj0 * fpitch + fi0;
   if (r == 1) {
@@ -89,6 +164,65 @@ FREHD_HD void frehd_cell_levels_at(const double *zf, long fpitch, int nx, int ny
   o->Vxm = dA * sxm;
   o->Vyp = dA * syp;
   o->Vym = dA * sym;
+
+  if (check_block) {
+    const unsigned long long mo = frehd_block_cluster(zf, fpitch, r, i, j, h);
+    unsigned long long edge_w = 0, edge_e = 0, edge_s = 0, edge_n = 0;
+    for (int q = 0; q < r; ++q) {
+      edge_w |= 1ull << (q * r);
+      edge_e |= 1ull << (q * r + r - 1);
+      edge_s |= 1ull << q;
+      edge_n |= 1ull << ((r - 1) * r + q);
+    }
+    double s = 0.0;
+    if (i < nx - 1) {
+      const unsigned long long me = frehd_block_cluster(zf, fpitch, r, i + 1, j, h);
+      for (int fj = 0; fj < r; ++fj) {
+        const double *row = b + (long)fj * fpitch;
+        s += frehd_min2(frehd_masked(frehd_fine_depth(h, row[r - 1]), mo, fj * r + r - 1),
+                        frehd_masked(frehd_fine_depth(h, row[r]), me, fj * r));
+      }
+    } else {
+      for (int fj = 0; fj < r; ++fj) s += frehd_fine_depth(h, b[(long)fj * fpitch + r - 1]);
+    }
+    o->Np = (mo & edge_e) ? s * dxf : 0.0;
+    s = 0.0;
+    if (i > 0) {
+      const unsigned long long mw = frehd_block_cluster(zf, fpitch, r, i - 1, j, h);
+      for (int fj = 0; fj < r; ++fj) {
+        const double *row = b + (long)fj * fpitch;
+        s += frehd_min2(frehd_masked(frehd_fine_depth(h, row[-1]), mw, fj * r + r - 1),
+                        frehd_masked(frehd_fine_depth(h, row[0]), mo, fj * r));
+      }
+    } else {
+      for (int fj = 0; fj < r; ++fj) s += frehd_fine_depth(h, b[(long)fj * fpitch]);
+    }
+    o->Nm = (mo & edge_w) ? s * dxf : 0.0;
+    s = 0.0;
+    if (j < ny - 1) {
+      const unsigned long long mn = frehd_block_cluster(zf, fpitch, r, i, j + 1, h);
+      const double *r0 = b + (long)(r - 1) * fpitch, *r1 = b + (long)r * fpitch;
+      for (int fi = 0; fi < r; ++fi)
+        s += frehd_min2(frehd_masked(frehd_fine_depth(h, r0[fi]), mo, (r - 1) * r + fi),
+                        frehd_masked(frehd_fine_depth(h, r1[fi]), mn, fi));
+    } else {
+      const double *r0 = b + (long)(r - 1) * fpitch;
+      for (int fi = 0; fi < r; ++fi) s += frehd_fine_depth(h, r0[fi]);
+    }
+    o->Op = (mo & edge_n) ? s * dxf : 0.0;
+    s = 0.0;
+    if (j > 0) {
+      const unsigned long long ms = frehd_block_cluster(zf, fpitch, r, i, j - 1, h);
+      const double *r0 = b - fpitch;
+      for (int fi = 0; fi < r; ++fi)
+        s += frehd_min2(frehd_masked(frehd_fine_depth(h, r0[fi]), ms, (r - 1) * r + fi),
+                        frehd_masked(frehd_fine_depth(h, b[fi]), mo, fi));
+    } else {
+      for (int fi = 0; fi < r; ++fi) s += frehd_fine_depth(h, b[fi]);
+    }
+    o->Om = (mo & edge_s) ? s * dxf : 0.0;
+    return;
+  }
 
   /* Np: own last x-row against the east neighbour's first x-row. */
   double s = 0.0;

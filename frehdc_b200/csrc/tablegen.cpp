@@ -10,11 +10,15 @@
 #include "frehd_internal.h"
 #include "subgrid_levels.h"
 
-extern "C" int frehd_build_tables(const double *zf, long fpitch, int nx, int ny, int r,
-                                  double dxf, double dyf, double surfmin, double dsurf, int Ne,
-                                  double *tables) {
-  if (!zf || !tables || nx <= 0 || ny <= 0 || r <= 0 || Ne <= 0 || fpitch < (long)nx * r)
+extern "C" int frehd_build_tables_ex(const double *zf, long fpitch, int nx, int ny, int r,
+                                     double dxf, double dyf, double surfmin, double dsurf, int Ne,
+                                     int flags, double *tables) {
+  if (!zf || !tables || nx <= 0 || ny <= 0 || r <= 0 || Ne <= 0 || fpitch < (long)nx * r ||
+      (flags & ~FREHD_GEOM_BLOCK_CHECK))
     return frehd::fail(FREHD_ERR_INVALID, "frehd_build_tables: bad arguments");
+  const int check_block = (flags & FREHD_GEOM_BLOCK_CHECK) && r > 1;
+  if (check_block && r > 8)
+    return frehd::fail(FREHD_ERR_UNSUPPORTED, "block check needs r <= 8 (r = %d)", r);
   const long N = (long)nx * ny;
   const double dA = dxf * dyf;
   unsigned nth = std::thread::hardware_concurrency();
@@ -26,7 +30,7 @@ extern "C" int frehd_build_tables(const double *zf, long fpitch, int nx, int ny,
       for (int j = 0; j < ny; ++j)
         for (int i = 0; i < nx; ++i) {
           frehd_cell_levels o;
-          frehd_cell_levels_at(zf, fpitch, nx, ny, r, i, j, h, dA, dxf, &o);
+          frehd_cell_levels_at(zf, fpitch, nx, ny, r, i, j, h, dA, dxf, check_block, &o);
           const long ii = (long)j * nx + i, base = N * k + ii, T = N * (long)Ne;
           tables[0 * T + base] = o.V;
           tables[1 * T + base] = o.Z;
@@ -49,6 +53,12 @@ extern "C" int frehd_build_tables(const double *zf, long fpitch, int nx, int ny,
   }
   for (auto &th : pool) th.join();
   return FREHD_OK;
+}
+
+extern "C" int frehd_build_tables(const double *zf, long fpitch, int nx, int ny, int r,
+                                  double dxf, double dyf, double surfmin, double dsurf, int Ne,
+                                  double *tables) {
+  return frehd_build_tables_ex(zf, fpitch, nx, ny, r, dxf, dyf, surfmin, dsurf, Ne, 0, tables);
 }
 
 extern "C" int frehd_build_bottoms(const double *zf, long fpitch, int nx, int ny, int r,

@@ -56,6 +56,7 @@ class DeckSpec:
     scalar_sigma: float = 100.0
     scalar_peak: float = 1.0
     scalar_in_window: bool = False  # plume at the centre of the (cropped) window, not the basin
+    block_check: bool = False       # checkBlock = 1 face areas (largest wet cluster per block)
     dsurf: float = 0.01
     eps: float = 1e-12
     max_iter: int = 100000
@@ -241,7 +242,8 @@ def build_tables(deck: Deck) -> np.ndarray:
     """(10, Ne, N) subgrid tables of a deck (frehd_build_tables)."""
     from . import native
     return native.build_tables(deck.zf, deck.nx, deck.ny, deck.r, deck.spec.dx / deck.r,
-                               deck.spec.dx / deck.r, deck.surfmin, deck.dsurf, deck.Ne)
+                               deck.spec.dx / deck.r, deck.surfmin, deck.dsurf, deck.Ne,
+                               block_check=deck.spec.block_check)
 
 
 # --------------------------------------------------------------------------- tide

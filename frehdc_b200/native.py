@@ -91,6 +91,8 @@ def _declare(L: C.CDLL) -> None:
     L.frehd_version.restype = C.c_char_p
     L.frehd_build_tables.argtypes = [_dp, C.c_long, C.c_int, C.c_int, C.c_int, C.c_double,
                                      C.c_double, C.c_double, C.c_double, C.c_int, _dp]
+    L.frehd_build_tables_ex.argtypes = [_dp, C.c_long, C.c_int, C.c_int, C.c_int, C.c_double,
+                                        C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, _dp]
     L.frehd_build_bottoms.argtypes = [_dp, C.c_long, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]
     L.frehd_config_defaults.argtypes = [C.POINTER(Config)]
     L.frehd_config_defaults.restype = None
@@ -107,12 +109,16 @@ def as_dp(a: np.ndarray):
     return a.ctypes.data_as(_dp)
 
 
+GEOM_BLOCK_CHECK = 1
+
+
 def build_tables(zf: np.ndarray, nx: int, ny: int, r: int, dxf: float, dyf: float,
-                 surfmin: float, dsurf: float, Ne: int) -> np.ndarray:
+                 surfmin: float, dsurf: float, Ne: int, block_check: bool = False) -> np.ndarray:
     zf = np.ascontiguousarray(zf, dtype=np.float64)
     out = np.empty((10, Ne, nx * ny), dtype=np.float64)
-    check(lib().frehd_build_tables(as_dp(zf), zf.shape[1], nx, ny, r, dxf, dyf, surfmin, dsurf,
-                                   Ne, as_dp(out)), "frehd_build_tables")
+    check(lib().frehd_build_tables_ex(as_dp(zf), zf.shape[1], nx, ny, r, dxf, dyf, surfmin, dsurf,
+                                      Ne, GEOM_BLOCK_CHECK if block_check else 0, as_dp(out)),
+          "frehd_build_tables")
     return out
 
 
@@ -152,6 +158,7 @@ def _declare_domain(L: C.CDLL) -> None:
     L.frehd_domain_destroy.argtypes = [_vp]
     L.frehd_domain_set_tables.argtypes = [_vp, C.c_int, _dp]
     L.frehd_domain_set_fine_bottoms.argtypes = [_vp, C.c_int, _dp, C.c_long]
+    L.frehd_domain_set_fine_bottoms_ex.argtypes = [_vp, C.c_int, _dp, C.c_long, C.c_int]
     L.frehd_domain_set_tide.argtypes = [_vp, C.c_int, _dp]
     L.frehd_domain_set_solver.argtypes = [_vp, C.c_int]
     L.frehd_domain_set_cg_schedule.argtypes = [_vp, C.c_int]
@@ -214,9 +221,11 @@ class Domain:
         t = np.ascontiguousarray(tables, dtype=np.float64)
         check(lib().frehd_domain_set_tables(self.h, t.shape[1], as_dp(t)), "set_tables")
 
-    def set_fine_bottoms(self, zf: np.ndarray, r: int):
+    def set_fine_bottoms(self, zf: np.ndarray, r: int, block_check: bool = False):
         z = np.ascontiguousarray(zf, dtype=np.float64)
-        check(lib().frehd_domain_set_fine_bottoms(self.h, r, as_dp(z), z.shape[1]), "set_fine_bottoms")
+        check(lib().frehd_domain_set_fine_bottoms_ex(self.h, r, as_dp(z), z.shape[1],
+                                                     GEOM_BLOCK_CHECK if block_check else 0),
+              "set_fine_bottoms")
 
     def set_tide(self, tideP: np.ndarray):
         t = np.ascontiguousarray(tideP, dtype=np.float64)
@@ -467,7 +476,7 @@ def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0
     from . import deck as D
     d = Domain(D.config_dict(deck), device)
     if geometry == "fine":
-        d.set_fine_bottoms(deck.zf, deck.r)
+        d.set_fine_bottoms(deck.zf, deck.r, block_check=deck.spec.block_check)
     else:
         tabs = deck.extra.get("tables")
         if tabs is None:

@@ -87,6 +87,15 @@ void frehd_config_defaults(frehd_config *cfg);
 int frehd_build_tables(const double *zf, long fpitch, int nx, int ny, int r,
                        double dxf, double dyf, double surfmin, double dsurf, int Ne,
                        double *tables);
+/* Geometry options of the pre-processor.
+ * FREHD_GEOM_BLOCK_CHECK: checkBlock = 1 of script_CreateSubAreaWithBlockV16.m:27
+ * (ComputeFaceAreaWithBlockCheck.m): each block's wet pixels are reduced to their
+ * largest 4-connected cluster and face areas count only pixel pairs wet in both
+ * blocks' clusters.  Needs 1 < r <= 8 (r = 1: no effect). */
+enum { FREHD_GEOM_BLOCK_CHECK = 1 };
+int frehd_build_tables_ex(const double *zf, long fpitch, int nx, int ny, int r,
+                          double dxf, double dyf, double surfmin, double dsurf, int Ne,
+                          int flags, double *tables);
 /* Coarse bottom.dat / bottomXP.dat / bottomYP.dat of a deck (N doubles each). */
 int frehd_build_bottoms(const double *zf, long fpitch, int nx, int ny, int r,
                         double *bottom, double *bottomXP, double *bottomYP);
@@ -144,6 +153,10 @@ int frehd_domain_destroy(frehd_domain *d);
  *   with the same arithmetic as frehd_build_tables (no tables in HBM). */
 int frehd_domain_set_tables(frehd_domain *d, int Ne, const double *tables);
 int frehd_domain_set_fine_bottoms(frehd_domain *d, int r, const double *zf, long fpitch);
+/* The same with geometry options (FREHD_GEOM_BLOCK_CHECK), evaluated on the device
+ * as frehd_build_tables_ex would tabulate them. */
+int frehd_domain_set_fine_bottoms_ex(frehd_domain *d, int r, const double *zf, long fpitch,
+                                     int flags);
 
 /* Tidal elevation series bc->tideP (initialize.h:28-32), indexed by step tt. */
 int frehd_domain_set_tide(frehd_domain *d, int n, const double *tideP);

@@ -22,6 +22,8 @@
 #ifndef FREHD_B200_H
 #define FREHD_B200_H
 
+#include <stddef.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -207,6 +209,30 @@ int frehd_domain_download_solution(frehd_domain *d, double *x);
 int frehd_domain_stats(frehd_domain *d, frehd_step_stats *out);
 /* Wait for all work queued on the domain's stream. */
 int frehd_domain_sync(frehd_domain *d);
+
+/* ------------------------------------------------------------ output files */
+/*
+ * The reference's output files written from the device state: one value per
+ * line as fprintf("%4.4f \n") prints it (WriteFile, fileio.c:158-181), to
+ * <prefix><name>_<tt>.dat, formatted on the GPU with printf's rounding (to
+ * nearest, ties to even, on the exact binary value); only the text crosses to
+ * the host.
+ *   frehd_domain_write_output: the files of DataOutput (fileio.c:62-122) and
+ *     SubOutput (fileio.c:125-155) selected by `fields`: uVelocity, vVelocity,
+ *     surfaceZ (surf - offset), depth, cdxp and cdyp, scalar; SubNx, SubOy,
+ *     SubVx, SubVy, SubV, SubZ.  Like DataOutput it then round-trips the
+ *     interior surface through the output datum (surf = (surf - offset) + offset),
+ *     which the next step starts from.
+ *   frehd_domain_write_restart: restart_<tt>.dat of writeRestartFile
+ *     (fileio.c:192-242): tNEnd, dx, dy, then surf - offset, uu, vv and S.
+ *   frehd_format_fixed4: the same formatting of n host values into `out`
+ *     (`*len` bytes; `out` may be NULL to ask for the length).
+ */
+enum { FREHD_OUT_SURFACE = 1, FREHD_OUT_U = 2, FREHD_OUT_V = 4, FREHD_OUT_DEPTH = 8,
+       FREHD_OUT_CD = 16, FREHD_OUT_SCALAR = 32, FREHD_OUT_SUB = 64 };
+int frehd_domain_write_output(frehd_domain *d, const char *prefix, int tt, int fields);
+int frehd_domain_write_restart(frehd_domain *d, const char *prefix, int tt, double tNEnd);
+int frehd_format_fixed4(const double *values, long n, char *out, size_t cap, size_t *len);
 
 /* Accumulated device time per kernel (CUDA events on the domain's stream)
  * while profiling is on, and the CG iterations those steps ran. */

@@ -27,6 +27,10 @@
  *                       velocities back every step); otherwise one summary line
  *                       per device run when a cell exceeded CFL 2
  *   FREHD_CHUNK         most steps per device run between host checks (1000)
+ *   FREHD_DEVICE_OUTPUT 1: write the output files from the device
+ *                       (frehd_domain_write_output: the same bytes, formatted on
+ *                       the GPU) instead of copying the state back for the
+ *                       reference's DataOutput/SubOutput
  *   FREHD_DUMP          path: after the last step, write the final state in
  *                       full precision (FRHDDUMP: "FRHDDUMP", int32 version 1,
  *                       int32 count, then per array char name[24], int64 n,
@@ -331,6 +335,20 @@ static void dump_step(const char *pattern, Data *data, Sub *sub, Config *setting
   fclose(f);
 }
 
+/* The files DataOutput and SubOutput write for these settings (fileio.c:100-121,
+ * 145-153; SubOutput is called only in subgrid mode, nssolve.c:92). */
+static int output_fields(const Config *s) {
+  int f = 0;
+  if (s->saveuu == 1) f |= FREHD_OUT_U;
+  if (s->savevv == 1) f |= FREHD_OUT_V;
+  if (s->savesurface == 1) f |= FREHD_OUT_SURFACE;
+  if (s->savedepth == 1) f |= FREHD_OUT_DEPTH;
+  if (s->saveCD == 1) f |= FREHD_OUT_CD;
+  if (s->useScalar == 1 && s->savescalar == 1) f |= FREHD_OUT_SCALAR;
+  if (s->useSubgrid != 0 && s->savesub == 1) f |= FREHD_OUT_SUB;
+  return f;
+}
+
 /* ------------------------------------------------------------ nssolve.h entry points */
 
 /* The time loop (nssolve.c:48-107).  Steps run on the device in runs that end
@@ -355,6 +373,8 @@ void SolveAll(Data **data, Sub **sub, Maps *map, BC *bc, Bath *bath, Config *set
   const char *dump = getenv("FREHD_DUMP");
   if (dump && !*dump) dump = NULL;
   const int dump_every = dump && strstr(dump, "%d") != NULL;
+  /* vloss (checkConservation) has no device counterpart: the host writes then */
+  const int device_output = env_int("FREHD_DEVICE_OUTPUT", 0) && setting->checkConservation != 1;
   if (irank == 0) printf("Ready for time stepping ...\n");
   int tt = 1;
   while (tt <= setting->Nt) {
@@ -399,7 +419,15 @@ void SolveAll(Data **data, Sub **sub, Maps *map, BC *bc, Bath *bath, Config *set
       printf("WARNING: %d cells with CFL > 2 at step %d (max CFL x %lf, y %lf)\n", s.n_cfl_warn,
              s.step, s.max_cflx, s.max_cfly);
     }
-    if (itvl > 0 && last % itvl == 0) {
+    if (itvl > 0 && last % itvl == 0 && device_output) {
+      rc = frehd_domain_write_output(g_dom, setting->saveFolder, last, output_fields(setting));
+      if (rc) die("frehd_domain_write_output", rc);
+      if (dump_every) {
+        rc = frehd_gpu_sync_to_host(*data, *sub);
+        if (rc) die("frehd_gpu_sync_to_host", rc);
+        dump_step(dump, *data, *sub, setting, last);
+      }
+    } else if (itvl > 0 && last % itvl == 0) {
       rc = frehd_gpu_sync_to_host(*data, *sub);
       if (rc) die("frehd_gpu_sync_to_host", rc);
       DataOutput(data, bath, setting, last, root, irank);

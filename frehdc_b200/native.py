@@ -175,8 +175,28 @@ def _declare_domain(L: C.CDLL) -> None:
     L.frehd_domain_stats.argtypes = [_vp, C.POINTER(StepStats)]
     L.frehd_domain_sync.argtypes = [_vp]
     L.frehd_device_count.argtypes = [_ip]
+    L.frehd_domain_write_output.argtypes = [_vp, C.c_char_p, C.c_int, C.c_int]
+    L.frehd_domain_write_restart.argtypes = [_vp, C.c_char_p, C.c_int, C.c_double]
+    L.frehd_format_fixed4.argtypes = [_dp, C.c_long, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
     L.frehd_cg_solve_noalloc.argtypes = [C.c_int, C.c_int] + [_vp] * 5 + \
         [C.c_double, C.c_int, C.c_int, _vp, _ip, C.POINTER(C.c_double)]
+
+
+OUT_SURFACE, OUT_U, OUT_V, OUT_DEPTH, OUT_CD, OUT_SCALAR, OUT_SUB = 1, 2, 4, 8, 16, 32, 64
+
+
+def format_fixed4(values) -> bytes:
+    """The reference's "%4.4f \n" lines of the values, formatted on the GPU."""
+    L = lib()
+    if not hasattr(L, "_domain_declared"):
+        _declare_domain(L)
+        L._domain_declared = True
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    n = C.c_size_t(0)
+    check(L.frehd_format_fixed4(as_dp(v), v.size, None, 0, C.byref(n)), "format_fixed4")
+    buf = C.create_string_buffer(n.value + 1)
+    check(L.frehd_format_fixed4(as_dp(v), v.size, buf, n.value, C.byref(n)), "format_fixed4")
+    return buf.raw[:n.value]
 
 
 def device_count() -> int:
@@ -329,6 +349,13 @@ class Domain:
 
     def sync(self):
         check(lib().frehd_domain_sync(self.h), "sync")
+
+    def write_output(self, prefix: str, tt: int, fields: int):
+        """DataOutput/SubOutput files of the current state (OUT_* flags)."""
+        check(lib().frehd_domain_write_output(self.h, prefix.encode(), tt, fields), "write_output")
+
+    def write_restart(self, prefix: str, tt: int, tNEnd: float):
+        check(lib().frehd_domain_write_restart(self.h, prefix.encode(), tt, tNEnd), "write_restart")
 
     def set_profiling(self, on: bool):
         check(lib().frehd_domain_set_profiling(self.h, int(on)), "set_profiling")

@@ -5,7 +5,9 @@ nssolve.c, stepping on the GPU through the C ABI.
 CPU: the binary is linked against the library, defines the nssolve.h entry
 points and the frehd_dropin.h API, and fails loudly when no device is present
 (there is no host fallback).  GPU: on the same deck it writes the same output
-files as the reference program (Jacobi-preconditioned build), and its
+files as the reference program (Jacobi-preconditioned build), whether the
+reference's DataOutput prints them from copied-back state or the device formats
+them (FREHD_DEVICE_OUTPUT=1), and its
 full-precision state at the output steps matches the reference's to the
 rounding level of two Jacobi-PCG solves.
 """
@@ -91,8 +93,9 @@ def _read_outputs(folder: str) -> dict:
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("output", ["host", "device"])
 @pytest.mark.parametrize("name", ["wet48x40", "dry40x36"])
-def test_dropin_matches_reference_program(name, tmp_path):
+def test_dropin_matches_reference_program(name, output, tmp_path):
     if native.device_count() < 1:
         pytest.fail("no CUDA device visible: the GPU tests need a B200")
     if not os.path.exists(refrun.JACOBI_BIN):
@@ -104,7 +107,8 @@ def test_dropin_matches_reference_program(name, tmp_path):
     steps = SPECS[name].steps                      # a multiple of OUT_STEPS, < Nt
     assert steps % OUT_STEPS == 0 and steps < d.Nt
     ref = refrun.run(ref_deck, steps, str(tmp_path / "ref.bin"), precond="jacobi")
-    env = dict(os.environ, FREHD_DUMP=str(tmp_path / "gpu_%d.bin"))
+    env = dict(os.environ, FREHD_DUMP=str(tmp_path / "gpu_%d.bin"),
+               FREHD_DEVICE_OUTPUT="1" if output == "device" else "0")
     r = subprocess.run([b], cwd=gpu_deck, env=env, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:] + r.stdout[-2000:]
     assert "Time stepping completed" in r.stdout

@@ -56,8 +56,8 @@ int check_config(const frehd_config *c) {
   if (c->useWind || c->useEvap || c->useRain || c->inflowLocLength || c->useSubStep ||
       c->checkConservation)
     return fail(FREHD_ERR_UNSUPPORTED, "wind/evaporation/rain/inflow/sub-stepping not implemented");
-  if (c->useScalar && (c->scalarAdv != 1 || c->useConstTidePS != 1))
-    return fail(FREHD_ERR_UNSUPPORTED, "scalar: only scalarAdv=1 with a constant tidal scalar");
+  if (c->useScalar && ((c->scalarAdv != 1 && c->scalarAdv != 2) || c->useConstTidePS != 1))
+    return fail(FREHD_ERR_UNSUPPORTED, "scalar: scalarAdv 1 or 2 with a constant tidal scalar");
   if (c->tideLocFirstP < 0 || c->tideLocLengthP < 0 || c->tideLocFirstP + c->tideLocLengthP > c->nx)
     return fail(FREHD_ERR_INVALID, "tidal cells outside the YP row");
   if (!(c->dsurf > 0) || !(c->dx > 0) || !(c->dy > 0) || !(c->dt > 0))
@@ -183,7 +183,10 @@ int launch_update(frehd_domain *d, const View &w, cudaEvent_t *ev = nullptr) {
   mark(ev, 2, d->stream);
   k_update_geo<<<gb, bb, 0, d->stream>>>(w);
   mark(ev, 3, d->stream);
-  k_update_vel<<<gb, bb, 0, d->stream>>>(w);
+  if (d->p.scalarAdv == 2)
+    k_update_vel_tvd<<<gb, bb, 0, d->stream>>>(w);
+  else
+    k_update_vel<<<gb, bb, 0, d->stream>>>(w);
   mark(ev, 4, d->stream);
   k_finish<<<1, 256, 0, d->stream>>>(w, (int)(gb.x * gb.y), d->out);
   mark(ev, 5, d->stream);
@@ -234,7 +237,7 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
   p.offset = cfg->offset; p.surfmin = cfg->surfmin; p.dsurf = cfg->dsurf; p.tidePS = cfg->tidePS;
   p.subR = cfg->subR; p.dxf = cfg->dxf; p.dyf = cfg->dyf; p.eps = cfg->eps;
   p.Ne = (int)std::lround((cfg->surfmax - cfg->surfmin) / cfg->dsurf);  // subgrid.c:2115
-  p.useThinLayer = cfg->useThinLayer; p.useScalar = cfg->useScalar;
+  p.useThinLayer = cfg->useThinLayer; p.useScalar = cfg->useScalar; p.scalarAdv = cfg->scalarAdv;
   p.tideFirst = cfg->tideLocFirstP; p.tideLen = cfg->tideLocLengthP; p.maxIter = cfg->maxIter;
   p.mixed = 0;
   p.eps_inner = 1e-5;

@@ -58,6 +58,7 @@ struct Params {
   double dx, dy, dt, g, NUx, NUy, Kx, Ky, manningN, hD, minDepth, wtfh, CFLl, CFLh;
   double offset, surfmin, dsurf, tidePS, subR, dxf, dyf, eps;
   int Ne, useThinLayer, useScalar, tideFirst, tideLen, maxIter;
+  int scalarAdv;      // 1: first-order upwind, 2: TVD with the superbee limiter
   int mixed;          // CG: FP32 inner iterations inside FP64 iterative refinement
   double eps_inner;   // relative residual reduction of one FP32 inner solve
   // geometry source

@@ -30,6 +30,7 @@ __global__ void k_explicit(View w);
 __global__ void k_update_geo(View w);
 __global__ void k_update_geo_init(View w);
 __global__ void k_update_vel(View w);
+__global__ void k_update_vel_tvd(View w);
 __global__ void k_finish(View w, int nblocks_vel, StepOut *out);
 __global__ void k_ref_to_padded(double *dst, const double *src, long n, int nx, int ny, int pitch);
 __global__ void k_padded_to_ref(double *dst, const double *src, long n, int nx, int ny, int pitch);

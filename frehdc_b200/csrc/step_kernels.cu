@@ -600,11 +600,125 @@ __device__ double face_v(const View &w, int i, int j) {
   return v;
 }
 
+// Face flow rates as computeFaceFlowRateSub stores them (subgrid.c:1190-1212)
+// for any face the TVD stencil reaches: interior faces recomputed, the ghost
+// column/row faces from the boundary cell's velocity copied by enforceVelocityBC
+// (nsfunctions.c:289-314) times the ghost's own face area.
+__device__ double flux_u(const View &w, int i, int j) {
+  const int ib = i < 0 ? 0 : (i >= w.gr.nx ? w.gr.nx - 1 : i);
+  return face_u(w, ib, j) * w.Nx[w.gr.at(i, j)];
+}
+
+__device__ double flux_v(const View &w, int i, int j) {
+  const int jb = j < 0 ? 0 : (j >= w.gr.ny ? w.gr.ny - 1 : j);
+  return face_v(w, i, jb) * w.Oy[w.gr.at(i, j)];
+}
+
+// Superbee limiter (scalar.c:115-119).
+__device__ __forceinline__ double superbee(double r) {
+  double p1, p2, phi;
+  if (2 * r > 1) p1 = 1; else p1 = 2 * r;
+  if (r > 2) p2 = 2; else p2 = r;
+  if (p1 > 0) phi = p1; else phi = 0;
+  if (p2 > phi) phi = p2;
+  return phi;
+}
+
+// TVD face values of cell (i, j) (scalarAdvection with scalarAdv = 2,
+// scalar.c:99-249).  The two-cell maps are map.c:66-97's: iPPjc/iMMjc and icjPP
+// stop at the ghost ring; icjMM of the second row (j = 1) is never assigned by
+// the reference and reads 0 (cell (0, 0)) under the zero-filled allocation the
+// parity build uses.  The YM Courant number uses dx, as the reference's does.
+__device__ void tvd_faces(const View &w, int i, int j, double FE, double FW, double FN, double FS,
+                          double uE, double uW, double vst, double vS, double *Sd_, double *Su_,
+                          double *Sr_, double *Sl_) {
+  const Params &p = w.p;
+  const Grid &g = w.gr;
+  const double *S = w.S_cur;
+  const double dSmin = 0.00001;
+  const long k = g.at(i, j);
+  const double Sc = S[k], SE = S[g.at(i + 1, j)], SW = S[g.at(i - 1, j)];
+  const double SNn = S[g.at(i, j + 1)], SS = S[g.at(i, j - 1)];
+  const int iee = i <= g.nx - 3 ? i + 2 : g.nx, iww = i >= 2 ? i - 2 : -1;
+  const int jnn = j <= g.ny - 3 ? j + 2 : g.ny;
+  const double SEE = S[g.at(iee, j)], SWW = S[g.at(iww, j)], SNN = S[g.at(i, jnn)];
+  double SSS, Fss;
+  if (j >= 2) { SSS = S[g.at(i, j - 2)]; Fss = flux_v(w, i, j - 2); }
+  else if (j == 1) { SSS = S[g.at(0, 0)]; Fss = flux_v(w, 0, 0); }
+  else { SSS = S[g.at(i, -1)]; Fss = flux_v(w, i, -1); }
+  double Sd, Su, Sr, Sl, Cu, r;
+  // XP face
+  Cu = uE * p.dt / p.dx;
+  if (FE > 0) {
+    if (FW <= 0) Sd = Sc;
+    else {
+      if (fabs(SE - Sc) < dSmin) r = 0; else r = (Sc - SW) / (SE - Sc);
+      Sd = Sc + 0.5 * superbee(r) * (SE - Sc) * Cu * (1 - Cu);
+    }
+  } else {
+    if (flux_u(w, i + 1, j) >= 0) Sd = SE;
+    else {
+      if (fabs(SE - Sc) < dSmin) r = 0; else r = (SE - SEE) / (Sc - SE);
+      Sd = SE + 0.5 * superbee(r) * (Sc - SE) * Cu * (1 - Cu);
+    }
+  }
+  // XM face
+  Cu = uW * p.dt / p.dx;
+  if (FW > 0) {
+    if (flux_u(w, iww, j) <= 0) Su = SW;
+    else {
+      if (fabs(Sc - SW) < dSmin) r = 0; else r = (SW - SWW) / (Sc - SW);
+      Su = SW + 0.5 * superbee(r) * (Sc - SW) * Cu * (1 - Cu);
+    }
+  } else {
+    if (FE >= 0) Su = Sc;
+    else {
+      if (fabs(Sc - SW) < dSmin) r = 0; else r = (Sc - SE) / (SW - Sc);
+      Su = Sc + 0.5 * superbee(r) * (SW - Sc) * Cu * (1 - Cu);
+    }
+  }
+  // YP face
+  Cu = vst * p.dt / p.dy;
+  if (FN > 0) {
+    if (FS <= 0) Sr = Sc;
+    else {
+      if (fabs(SNn - Sc) < dSmin) r = 0; else r = (Sc - SS) / (SNn - Sc);
+      Sr = Sc + 0.5 * superbee(r) * (SNn - Sc) * Cu * (1 - Cu);
+    }
+  } else {
+    if (flux_v(w, i, j + 1) >= 0) Sr = SNn;
+    else {
+      if (fabs(SNn - Sc) < dSmin) r = 0; else r = (SNn - SNN) / (Sc - SNn);
+      Sr = SNn + 0.5 * superbee(r) * (Sc - SNn) * Cu * (1 - Cu);
+    }
+  }
+  // YM face
+  Cu = vS * p.dt / p.dx;
+  if (FS > 0) {
+    if (Fss <= 0) Sl = SS;
+    else {
+      if (fabs(Sc - SS) < dSmin) r = 0; else r = (SS - SSS) / (Sc - SS);
+      Sl = SS + 0.5 * superbee(r) * (Sc - SS) * Cu * (1 - Cu);
+    }
+  } else {
+    if (FN >= 0) Sl = Sc;
+    else {
+      if (fabs(Sc - SS) < dSmin) r = 0; else r = (Sc - SNn) / (SS - Sc);
+      Sl = Sc + 0.5 * superbee(r) * (SS - Sc) * Cu * (1 - Cu);
+    }
+  }
+  *Sd_ = Sd;
+  *Su_ = Su;
+  *Sr_ = Sr;
+  *Sl_ = Sl;
+}
+
 __device__ __forceinline__ unsigned long long dbits(double x) {
   return (unsigned long long)__double_as_longlong(x);
 }
 
 // gx: the domain's tile-grid width (the block's partial-sum slot is by*gx + bx)
+template <bool kTVD>
 static __device__ __forceinline__ void update_vel_tile(const View &w, int bx, int by, int gx) {
   const Params &p = w.p;
   const Grid &g = w.gr;
@@ -694,7 +808,7 @@ static __device__ __forceinline__ void update_vel_tile(const View &w, int bx, in
     }
     w.CDXP[k] = CDX;
     w.CDYP[k] = CDY;
-    // scalarTransport: upwind advection (scalar.c:72-97), scalarDiffusionSub
+    // scalarTransport: upwind or TVD advection (scalar.c:72-249), scalarDiffusionSub
     // (subgrid.c:1552-1567), updateScalarSub (subgrid.c:1570-1713), enforceScalarBC
     // (scalar.c:419-471)
     if (p.useScalar) {
@@ -702,8 +816,15 @@ static __device__ __forceinline__ void update_vel_tile(const View &w, int bx, in
       const double Sc = S[k], SE = rd(S, g, i + 1, j), SW = rd(S, g, i - 1, j);
       const double SNn = rd(S, g, i, j + 1), SS = rd(S, g, i, j - 1);
       double Sm = Sc * cv_old;  // computeVolumeSub: Sm = S * cellV
-      const double Sd = FE > 0 ? Sc : SE, Su = FW > 0 ? SW : Sc;
-      const double Sr = FN > 0 ? Sc : SNn, Sl = FS > 0 ? SS : Sc;
+      double Sd, Su, Sr, Sl;
+      if (kTVD) {
+        tvd_faces(w, i, j, FE, FW, FN, FS, uE, uW, vstore, vS, &Sd, &Su, &Sr, &Sl);
+      } else {
+        Sd = FE > 0 ? Sc : SE;
+        Su = FW > 0 ? SW : Sc;
+        Sr = FN > 0 ? Sc : SNn;
+        Sl = FS > 0 ? SS : Sc;
+      }
       Sm = Sm + p.dt * (-FE * Sd + FW * Su - FN * Sr + FS * Sl);
       Sm = Sm + p.dt * ((p.Kx * w.Nx[k] / p.dx) * (SE - Sc) - (p.Kx * NxW / p.dx) * (Sc - SW) +
                         (p.Ky * w.Oy[k] / p.dy) * (SNn - Sc) - (p.Ky * OyS / p.dy) * (Sc - SS));
@@ -776,7 +897,15 @@ static __device__ __forceinline__ void update_vel_tile(const View &w, int bx, in
 
 __global__ void __launch_bounds__(TBX *TBY) k_update_vel(View w) {
   if (*(volatile int *)&w.sc->status != FREHD_OK) return;
-  update_vel_tile(w, blockIdx.x, blockIdx.y, gridDim.x);
+  update_vel_tile<false>(w, blockIdx.x, blockIdx.y, gridDim.x);
+}
+
+// The same for decks with TVD scalar advection (scalarAdv = 2): a kernel of its
+// own, so that the wider stencil's registers do not cost the upwind kernel
+// occupancy.
+__global__ void __launch_bounds__(TBX *TBY) k_update_vel_tvd(View w) {
+  if (*(volatile int *)&w.sc->status != FREHD_OK) return;
+  update_vel_tile<true>(w, blockIdx.x, blockIdx.y, gridDim.x);
 }
 
 // ---------------------------------------------------------------- k_finish
@@ -874,7 +1003,10 @@ __global__ void __launch_bounds__(TBX *TBY) k_update_vel_batch(const View *views
   const BatchTile t = tiles[blockIdx.x];
   stage_view(views2, t.d, &sv, &s_cur, threadIdx.y * TBX + threadIdx.x, TBX * TBY);
   if (*(volatile int *)&sv.sc->status != FREHD_OK) return;
-  update_vel_tile(sv, t.bx, t.by, t.gx);
+  if (sv.p.scalarAdv == 2)
+    update_vel_tile<true>(sv, t.bx, t.by, t.gx);
+  else
+    update_vel_tile<false>(sv, t.bx, t.by, t.gx);
 }
 
 // One block per domain: k_finish's work, then the domain's ping-pong half flips.

@@ -57,6 +57,7 @@ class DeckSpec:
     scalar_peak: float = 1.0
     scalar_in_window: bool = False  # plume at the centre of the (cropped) window, not the basin
     block_check: bool = False       # checkBlock = 1 face areas (largest wet cluster per block)
+    scalar_adv: int = 1             # scalarAdv: 1 first-order upwind, 2 TVD (superbee)
     dsurf: float = 0.01
     eps: float = 1e-12
     max_iter: int = 100000
@@ -308,7 +309,7 @@ def data_dat_values(deck: Deck, out_hours: float | None = None) -> list:
         1, 1, M,                                                # 23..25 tideM (unused)
         0, 1, 1, 0, 0, M,                                       # 26..31 no inflow cells
         0, 0, M, M,                                             # 32..35 no wind
-        1, 1, 1, 0.0, 1, 0.0, M, 1, 0.0, M,                     # 36..45 scalar, tide S = 0
+        1, s.scalar_adv, 1, 0.0, 1, 0.0, M, 1, 0.0, M,          # 36..45 scalar, tide S = 0
         0.0, 0.0, 0.0, 0.0, 0, 1, 1, 0,                         # 46..53 IC from files
         1, 0, s.dx / s.r, s.dx / s.r,                           # 54..57 subgrid
         deck.surfmax, deck.surfmin, deck.dsurf,                 # 58..60

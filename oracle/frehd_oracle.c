@@ -19,7 +19,7 @@
  *
  * Supported Config subset (others are rejected at creation): useSubgrid = 1,
  * staggeredV = 1, useSubDrag = 0, CDnotN = 0, useminA = 0, useminV not in {1,2},
- * bcType = 1, no wind/evaporation/rain/inflow/sub-stepping, scalarAdv = 1,
+ * bcType = 1, no wind/evaporation/rain/inflow/sub-stepping, scalarAdv = 1 or 2,
  * useConstTidePS = 1, checkConservation = 0.
  */
 #include <math.h>
@@ -39,6 +39,7 @@ struct oracle_domain {
   long N, T;
   /* maps (map.c:31-143) */
   int *iPjc, *iMjc, *icjP, *icjM, *trps, *sprt;
+  int *iPPjc, *iMMjc, *icjPP, *icjMM;
   int *iPbd, *iPgt, *iMbd, *iMgt, *jPbd, *jPgt, *jMbd, *jMgt;
   int iMjP, iPjP, iPjM, iMjM;
   /* Data (initialize.h:10-21) */
@@ -87,6 +88,18 @@ static void make_maps(oracle_domain *d) {
     d->iPjc[ii] = i == nx - 1 ? (int)(N + 2 * nx + j) : (int)(ii + 1);
     d->iMjc[ii] = i == 0 ? (int)(N + 2 * nx + ny + j) : (int)(ii - 1);
   }
+  /* two-cell maps of the TVD scheme (map.c:66-77,89-97).  icjMM of the second
+   * row (j = 1) is never assigned there: the first loop writes from index 2nx
+   * on (and past the array's end), the second the first row.  Under the
+   * zero-filled allocator of the parity build it holds 0, i.e. cell (0, 0). */
+  d->iPPjc = iz(N); d->iMMjc = iz(N); d->icjPP = iz(N); d->icjMM = iz(N);
+  for (long ii = 0; ii < N; ++ii) {
+    int i = (int)(ii % nx), j = (int)(ii / nx);
+    d->icjPP[ii] = j < ny - 1 ? d->icjP[d->icjP[ii]] : d->icjP[ii];
+    d->icjMM[ii] = j >= 2 ? (int)(ii - 2 * nx) : (j == 0 ? d->icjM[ii] : 0);
+    d->iPPjc[ii] = i == nx - 1 ? d->iPjc[ii] : d->iPjc[d->iPjc[ii]];
+    d->iMMjc[ii] = i == 0 ? d->iMjc[ii] : d->iMjc[d->iMjc[ii]];
+  }
   d->iMjP = (int)d->T - 4;
   d->iPjP = (int)d->T - 3;
   d->iPjM = (int)d->T - 2;
@@ -125,7 +138,7 @@ static int check_cfg(oracle_domain *d) {
   if (c->bcType != 1) FAIL("bcType=%d unsupported", c->bcType);
   if (c->useWind || c->useEvap || c->useRain || c->inflowLocLength || c->useSubStep)
     FAIL("wind/evap/rain/inflow/substep unsupported");
-  if (c->useScalar && (c->scalarAdv != 1 || c->useConstTidePS != 1))
+  if (c->useScalar && ((c->scalarAdv != 1 && c->scalarAdv != 2) || c->useConstTidePS != 1))
     FAIL("scalar options unsupported");
   if (c->tideLocFirstP < 0 || c->tideLocFirstP + c->tideLocLengthP > c->nx)
     FAIL("tidal cells outside the YP row");
@@ -166,7 +179,8 @@ oracle_domain *oracle_create(const oracle_cfg *cfg, char *errbuf, int errlen) {
 
 void oracle_destroy(oracle_domain *d) {
   if (!d) return;
-  void *ptrs[] = {d->iPjc, d->iMjc, d->icjP, d->icjM, d->trps, d->sprt, d->iPbd, d->iPgt,
+  void *ptrs[] = {d->iPjc, d->iMjc, d->icjP, d->icjM, d->iPPjc, d->iMMjc, d->icjPP, d->icjMM,
+                  d->trps, d->sprt, d->iPbd, d->iPgt,
                   d->iMbd, d->iMgt, d->jPbd, d->jPgt, d->jMbd, d->jMgt, d->uuXP, d->uuYP,
                   d->vvXP, d->vvYP, d->surf, d->surfOld, d->Fuu, d->Fvv, d->cellV, d->depth,
                   d->depthXP, d->depthYP, d->EnXP, d->EnYP, d->DragXP, d->DragYP, d->CDXP,
@@ -952,18 +966,110 @@ static void update_data(oracle_domain *d) {
 }
 
 /* ------------------------------------------------------------- scalar */
+/* The superbee limiter of scalar.c:115-119 (and its three repetitions). */
+static double superbee(double r) {
+  double p1, p2, phi;
+  if (2 * r > 1) p1 = 1; else p1 = 2 * r;
+  if (r > 2) p2 = 2; else p2 = r;
+  if (p1 > 0) phi = p1; else phi = 0;
+  if (p2 > phi) phi = p2;
+  return phi;
+}
+
 static void scalar_transport(oracle_domain *d) {
   const long N = d->N;
   const double dt = d->c.dt, dx = d->c.dx, dy = d->c.dy, Kx = d->c.Kx, Ky = d->c.Ky;
   double *S = d->S, *Sm = d->Sm, *F = d->Fuu, *G = d->Fvv;
-  /* scalarAdvection, first-order upwind (scalar.c:72-97) */
-  for (long ii = 0; ii < N; ++ii) {
-    const int e = d->iPjc[ii], w = d->iMjc[ii], n = d->icjP[ii], s = d->icjM[ii];
-    double Sd = F[ii] > 0 ? S[ii] : S[e];
-    double Su = F[w] > 0 ? S[w] : S[ii];
-    double Sr = G[ii] > 0 ? S[ii] : S[n];
-    double Sl = G[s] > 0 ? S[s] : S[ii];
-    Sm[ii] = Sm[ii] + dt * (-F[ii] * Sd + F[w] * Su - G[ii] * Sr + G[s] * Sl);
+  if (d->c.scalarAdv == 2) {
+    /* scalarAdvection, TVD with the superbee limiter (scalar.c:99-249), term by
+     * term: first-order upwind where the stencil reaches a face without flow
+     * toward the cell, r = 0 below dSmin; the YM Courant number uses dx
+     * (scalar.c:214). */
+    const double dSmin = 0.00001;
+    for (long ii = 0; ii < N; ++ii) {
+      const int e = d->iPjc[ii], w = d->iMjc[ii], n = d->icjP[ii], s = d->icjM[ii];
+      const int ee = d->iPPjc[ii], ww = d->iMMjc[ii], nn = d->icjPP[ii], ss = d->icjMM[ii];
+      double Sd, Su, Sr, Sl, Cu, r;
+      /* XP face */
+      Cu = d->uuXP[ii] * dt / dx;
+      if (F[ii] > 0) {
+        if (F[w] <= 0) Sd = S[ii];
+        else {
+          if (fabs(S[e] - S[ii]) < dSmin) r = 0;
+          else r = (S[ii] - S[w]) / (S[e] - S[ii]);
+          Sd = S[ii] + 0.5 * superbee(r) * (S[e] - S[ii]) * Cu * (1 - Cu);
+        }
+      } else {
+        if (F[e] >= 0) Sd = S[e];
+        else {
+          if (fabs(S[e] - S[ii]) < dSmin) r = 0;
+          else r = (S[e] - S[ee]) / (S[ii] - S[e]);
+          Sd = S[e] + 0.5 * superbee(r) * (S[ii] - S[e]) * Cu * (1 - Cu);
+        }
+      }
+      /* XM face */
+      Cu = d->uuXP[w] * dt / dx;
+      if (F[w] > 0) {
+        if (F[ww] <= 0) Su = S[w];
+        else {
+          if (fabs(S[ii] - S[w]) < dSmin) r = 0;
+          else r = (S[w] - S[ww]) / (S[ii] - S[w]);
+          Su = S[w] + 0.5 * superbee(r) * (S[ii] - S[w]) * Cu * (1 - Cu);
+        }
+      } else {
+        if (F[ii] >= 0) Su = S[ii];
+        else {
+          if (fabs(S[ii] - S[w]) < dSmin) r = 0;
+          else r = (S[ii] - S[e]) / (S[w] - S[ii]);
+          Su = S[ii] + 0.5 * superbee(r) * (S[w] - S[ii]) * Cu * (1 - Cu);
+        }
+      }
+      /* YP face */
+      Cu = d->vvYP[ii] * dt / dy;
+      if (G[ii] > 0) {
+        if (G[s] <= 0) Sr = S[ii];
+        else {
+          if (fabs(S[n] - S[ii]) < dSmin) r = 0;
+          else r = (S[ii] - S[s]) / (S[n] - S[ii]);
+          Sr = S[ii] + 0.5 * superbee(r) * (S[n] - S[ii]) * Cu * (1 - Cu);
+        }
+      } else {
+        if (G[n] >= 0) Sr = S[n];
+        else {
+          if (fabs(S[n] - S[ii]) < dSmin) r = 0;
+          else r = (S[n] - S[nn]) / (S[ii] - S[n]);
+          Sr = S[n] + 0.5 * superbee(r) * (S[ii] - S[n]) * Cu * (1 - Cu);
+        }
+      }
+      /* YM face */
+      Cu = d->vvYP[s] * dt / dx;
+      if (G[s] > 0) {
+        if (G[ss] <= 0) Sl = S[s];
+        else {
+          if (fabs(S[ii] - S[s]) < dSmin) r = 0;
+          else r = (S[s] - S[ss]) / (S[ii] - S[s]);
+          Sl = S[s] + 0.5 * superbee(r) * (S[ii] - S[s]) * Cu * (1 - Cu);
+        }
+      } else {
+        if (G[ii] >= 0) Sl = S[ii];
+        else {
+          if (fabs(S[ii] - S[s]) < dSmin) r = 0;
+          else r = (S[ii] - S[n]) / (S[s] - S[ii]);
+          Sl = S[ii] + 0.5 * superbee(r) * (S[s] - S[ii]) * Cu * (1 - Cu);
+        }
+      }
+      Sm[ii] = Sm[ii] + dt * (-F[ii] * Sd + F[w] * Su - G[ii] * Sr + G[s] * Sl);
+    }
+  } else {
+    /* scalarAdvection, first-order upwind (scalar.c:72-97) */
+    for (long ii = 0; ii < N; ++ii) {
+      const int e = d->iPjc[ii], w = d->iMjc[ii], n = d->icjP[ii], s = d->icjM[ii];
+      double Sd = F[ii] > 0 ? S[ii] : S[e];
+      double Su = F[w] > 0 ? S[w] : S[ii];
+      double Sr = G[ii] > 0 ? S[ii] : S[n];
+      double Sl = G[s] > 0 ? S[s] : S[ii];
+      Sm[ii] = Sm[ii] + dt * (-F[ii] * Sd + F[w] * Su - G[ii] * Sr + G[s] * Sl);
+    }
   }
   /* scalarDiffusionSub (subgrid.c:1552-1567) */
   for (long ii = 0; ii < N; ++ii) {

@@ -21,6 +21,9 @@ SPECS = {
     "wet48x40": D.DeckSpec(nx=48, ny=40, steps=30, seed=3),
     "dry40x36": D.DeckSpec(nx=40, ny=36, steps=40, seed=5, dry_frac=0.3),
     "dry37x29": D.DeckSpec(nx=37, ny=29, steps=40, seed=9, dry_frac=0.35, dt=2.0, depth_max=3.0),
+    # TVD (superbee) scalar advection, scalar.c:99-249
+    "tvd44x36": D.DeckSpec(nx=44, ny=36, steps=40, seed=13, dry_frac=0.3, dt=2.0,
+                           scalar_adv=2, scalar_sigma=60.0),
 }
 
 _cache: dict = {}

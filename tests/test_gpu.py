@@ -54,7 +54,8 @@ def test_init_bitwise(name, geometry, scratch):
     assert mismatches(got, ref, POW, exact=False, rtol=1e-15) == []
 
 
-@pytest.mark.parametrize("name,steps", [("wet48x40", 6), ("dry40x36", 25), ("dry37x29", 25)])
+@pytest.mark.parametrize("name,steps", [("wet48x40", 6), ("dry40x36", 25), ("dry37x29", 25),
+                                        ("tvd44x36", 25)])
 def test_phases_bitwise(name, steps, scratch):
     """Each step: the oracle's state is uploaded, then the device's explicit
     phase and update phase (fed the oracle's x) must give the oracle's doubles."""
@@ -101,7 +102,7 @@ def test_solve_matches_oracle(name, schedule, scratch):
 
 
 @pytest.mark.parametrize("schedule", list(SCHEDULES))
-@pytest.mark.parametrize("name", ["wet48x40", "dry40x36", "dry37x29"])
+@pytest.mark.parametrize("name", ["wet48x40", "dry40x36", "dry37x29", "tvd44x36"])
 def test_full_run_matches_oracle(name, schedule, scratch):
     """Whole run against the oracle in the reference's own solver set-up (SSOR-PCG
     from x = 0, which tracks the reference program to ~1e-13)."""

@@ -46,7 +46,7 @@ def _run_batch(names, steps, scratch, cells_per_cta, graph=True):
 def test_batch_matches_single_domain_bitwise(scratch):
     names = list(SPECS)
     got, info = _run_batch(names, 12, scratch, cells_per_cta=1)
-    assert info["domains"] == 3
+    assert info["domains"] == len(names)
     for n in names:
         d, _ = deck_for(n, str(scratch))
         g = native.domain_from_deck(d, geometry="fine")
@@ -85,7 +85,7 @@ def test_served_results_equal_alone(scratch):
     same state as each request's domain stepped alone in a batch."""
     from frehdc_b200 import serve
     names = list(SPECS)
-    steps = {"wet48x40": 7, "dry40x36": 11, "dry37x29": 5}
+    steps = {"wet48x40": 7, "dry40x36": 11, "dry37x29": 5, "tvd44x36": 9}
     results = {}
 
     def done(req):
@@ -96,7 +96,7 @@ def test_served_results_equal_alone(scratch):
         d, _ = deck_for(n, str(scratch))
         reqs.append(serve.Request(k, d, steps[n], arrival=0.002 * k))
     res = serve.serve(reqs, BUDGET, 1e9, on_done=done)
-    assert res["requests"] == 3 and res["failed"] == 0
+    assert res["requests"] == len(names) and res["failed"] == 0
     for k, n in enumerate(names):
         alone, _ = _run_batch([n], steps[n], scratch, cells_per_cta=1e9)
         assert mismatches(results[k], alone[n][0], FIELDS) == [], n

@@ -15,6 +15,7 @@ FIELDS = [
     "tideLocFirstP", "tideLocLengthP", "useScalar", "scalarAdv", "useConstTidePS", "tidePS",
     "useWind", "useEvap", "useRain", "inflowLocLength", "useSubStep", "checkConservation",
     "minDepth", "wtfh", "CFLl", "CFLh", "eps", "maxIter", "offset",
+    "inflowI0", "inflowI1", "inflowJ0", "inflowJ1", "inflowS", "northAngle", "rhoa", "Cw",
 ]
 
 
@@ -67,6 +68,10 @@ def config_from_values(v: list, offset: float = 0.0) -> dict:
         # never assigned by ReadUserSettings; zero under a zeroing allocator
         useEvap=0, useRain=0, useSubStep=0, checkConservation=0,
         inflowLocLength=i(v[26]), offset=offset,
+        # inflowLoc[k] = jj*NX + ii - 1 for ii in [v27, v28), jj in [v29, v30)
+        # (configuration.c:53-60): cells i in [v27 - 1, v28 - 1), j in [v29, v30)
+        inflowI0=i(v[27]) - 1, inflowI1=i(v[28]) - 1, inflowJ0=i(v[29]), inflowJ1=i(v[30]),
+        inflowS=float(v[39]), northAngle=float(v[33]), rhoa=float(v[78]), Cw=float(v[79]),
     )
     return c
 

@@ -53,9 +53,16 @@ int check_config(const frehd_config *c) {
   if (c->useminV == 1 || c->useminV == 2)
     return fail(FREHD_ERR_UNSUPPORTED, "useminV=%d (1 and 2 not implemented)", c->useminV);
   if (c->bcType != 1) return fail(FREHD_ERR_UNSUPPORTED, "bcType=%d (only 1)", c->bcType);
-  if (c->useWind || c->useEvap || c->useRain || c->inflowLocLength || c->useSubStep ||
-      c->checkConservation)
-    return fail(FREHD_ERR_UNSUPPORTED, "wind/evaporation/rain/inflow/sub-stepping not implemented");
+  // ReadUserSettings never assigns useEvap, useRain, useSubStep or
+  // checkConservation (configuration.c:18-159): the reference never runs them
+  if (c->useEvap || c->useRain || c->useSubStep || c->checkConservation)
+    return fail(FREHD_ERR_UNSUPPORTED, "evaporation/rain/sub-stepping/conservation output");
+  if (c->useWind != 0 && c->useWind != 1) return fail(FREHD_ERR_INVALID, "useWind=%d", c->useWind);
+  if (c->inflowLocLength < 0 ||
+      (c->inflowLocLength > 0 &&
+       (c->inflowI0 < 0 || c->inflowJ0 < 0 || c->inflowI1 > c->nx || c->inflowJ1 > c->ny ||
+        (long)(c->inflowI1 - c->inflowI0) * (c->inflowJ1 - c->inflowJ0) != c->inflowLocLength)))
+    return fail(FREHD_ERR_INVALID, "inflow cells must be the rectangle of inflowLocLength interior cells");
   if (c->useScalar && ((c->scalarAdv != 1 && c->scalarAdv != 2) || c->useConstTidePS != 1))
     return fail(FREHD_ERR_UNSUPPORTED, "scalar: scalarAdv 1 or 2 with a constant tidal scalar");
   if (c->tideLocFirstP < 0 || c->tideLocLengthP < 0 || c->tideLocFirstP + c->tideLocLengthP > c->nx)
@@ -86,6 +93,9 @@ View make_view_at(const frehd_domain *d, int cur) {
   w.cellV = d->cellV; w.Sm = d->Sm; w.Fuu = d->Fuu; w.Fvv = d->Fvv;
   w.rmv = d->rmv; w.fix_list = d->fix_list; w.partials = d->partials;
   w.tide = d->tide; w.ntide = d->ntide;
+  w.inflow = d->inflow; w.ninflow = d->ninflow;
+  w.wspd = d->wspd; w.nwspd = d->nwspd; w.wcos = d->wcos; w.wsin = d->wsin; w.nwdir = d->nwdir;
+  w.dXP = d->dXP; w.dYP = d->dYP;
   w.sc = d->sc;
   return w;
 }
@@ -239,6 +249,11 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
   p.Ne = (int)std::lround((cfg->surfmax - cfg->surfmin) / cfg->dsurf);  // subgrid.c:2115
   p.useThinLayer = cfg->useThinLayer; p.useScalar = cfg->useScalar; p.scalarAdv = cfg->scalarAdv;
   p.tideFirst = cfg->tideLocFirstP; p.tideLen = cfg->tideLocLengthP; p.maxIter = cfg->maxIter;
+  p.inflowLen = cfg->inflowLocLength;
+  p.inflowI0 = cfg->inflowI0; p.inflowI1 = cfg->inflowI1;
+  p.inflowJ0 = cfg->inflowJ0; p.inflowJ1 = cfg->inflowJ1;
+  p.inflowS = cfg->inflowS;
+  p.useWind = cfg->useWind; p.rhoa = cfg->rhoa; p.Cw = cfg->Cw; p.CwT = cfg->CwT;
   p.mixed = 0;
   p.eps_inner = 1e-5;
   const long tot = d->gr.total;
@@ -256,6 +271,10 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
   for (auto a : arrs)
     if (!r) r |= dalloc(d, a, tot);
   if (!r) r |= dalloc(d, &d->rmv, tot);
+  if (!r && cfg->useWind) {  // face depths the wind term reads (zero until set)
+    r |= dalloc(d, &d->dXP, tot);
+    if (!r) r |= dalloc(d, &d->dYP, tot);
+  }
   if (!r) r |= dalloc(d, &d->fix_list, d->N);
   if (!r) r |= dalloc(d, &d->stage, d->T);
   if (!r) r |= dalloc(d, &d->stage2, d->T);
@@ -294,6 +313,13 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
   k_fill<<<(unsigned)((tot + 255) / 256), 256, 0, d->stream>>>(d->Ct, tot, -1.0);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaStreamSynchronize(d->stream));
+  if (cfg->useWind) {  // the direction before any series is set: zero plus northAngle
+    const int rc = frehd_domain_set_series(d, FREHD_SERIES_WIND_DIR, 0, nullptr);
+    if (rc) {
+      frehd_domain_destroy(d);
+      return rc;
+    }
+  }
   *out = d;
   return FREHD_OK;
 }
@@ -306,6 +332,8 @@ extern "C" int frehd_domain_destroy(frehd_domain *d) {
   if (d->tables) cudaFree(d->tables);
   if (d->zf) cudaFree(d->zf);
   if (d->tide) cudaFree(d->tide);
+  for (double *a : {d->inflow, d->wspd, d->wcos, d->wsin})
+    if (a) cudaFree(a);
   if (d->out_host) cudaFreeHost(d->out_host);
   for (cudaEvent_t e : d->ev) cudaEventDestroy(e);
   if (d->stream) cudaStreamDestroy(d->stream);
@@ -377,6 +405,56 @@ extern "C" int frehd_domain_set_tide(frehd_domain *d, int n, const double *tideP
   return FREHD_OK;
 }
 
+namespace {
+int upload_series(frehd_domain *d, double **dst, const std::vector<double> &h) {
+  if (*dst) cudaFree(*dst);
+  *dst = nullptr;
+  CUDA_TRY(cudaMalloc(dst, sizeof(double) * std::max<size_t>(h.size(), 1)));
+  if (!h.empty())
+    CUDA_TRY(cudaMemcpy(*dst, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+  return FREHD_OK;
+}
+}  // namespace
+
+extern "C" int frehd_domain_set_series(frehd_domain *d, int kind, int n, const double *values) {
+  if (!d || n < 0 || (n > 0 && !values)) return fail(FREHD_ERR_INVALID, "bad argument");
+  if (d->in_batch) return fail(FREHD_ERR_STATE, "the domain is stepped by a batch (release it first)");
+  CUDA_TRY(cudaSetDevice(d->device));
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  std::vector<double> h(values, values + n);
+  int rc;
+  switch (kind) {
+    case FREHD_SERIES_INFLOW:
+      rc = upload_series(d, &d->inflow, h);
+      if (!rc) d->ninflow = n;
+      return rc;
+    case FREHD_SERIES_WIND_SPEED:
+      rc = upload_series(d, &d->wspd, h);
+      if (!rc) d->nwspd = n;
+      return rc;
+    case FREHD_SERIES_WIND_DIR: {
+      // omega = (winddir[tt] + northAngle) * pi / 180 with the reference's pi
+      // (nsfunctions.c:611-617), its cosine and sine taken here by the host's
+      // libm as the reference takes them; entry n serves the steps past the
+      // series, where the reference reads a zero direction
+      const double pi = 3.1415926;
+      std::vector<double> c(n + 1), s(n + 1);
+      for (int t = 0; t <= n; ++t) {
+        const double phi = (t < n ? h[t] : 0.0) + d->cfg.northAngle;
+        const double omega = phi * pi / 180.0;
+        c[t] = std::cos(omega);
+        s[t] = std::sin(omega);
+      }
+      rc = upload_series(d, &d->wcos, c);
+      if (!rc) rc = upload_series(d, &d->wsin, s);
+      if (!rc) d->nwdir = n;
+      return rc;
+    }
+    default:
+      return fail(FREHD_ERR_INVALID, "unknown series kind %d", kind);
+  }
+}
+
 extern "C" int frehd_domain_set_solver(frehd_domain *d, int x0_mode) {
   if (!d || (x0_mode != FREHD_X0_ZERO && x0_mode != FREHD_X0_SURFACE))
     return fail(FREHD_ERR_INVALID, "bad solver option");
@@ -440,9 +518,10 @@ extern "C" int frehd_domain_upload_state(frehd_domain *d, const frehd_state *st)
       {st->Nx, d->Nx, T}, {st->Oy, d->Oy, T}, {st->Vx, d->Vx, T}, {st->Vy, d->Vy, T},
       {st->Zx, d->Zx, T}, {st->Zy, d->Zy, T}, {st->bottomZ, d->bottomZ, T},
       {st->bottomXP, d->bottomXP, T}, {st->bottomYP, d->bottomYP, T},
+      {st->depthXP, d->dXP, T}, {st->depthYP, d->dYP, T},
   };
   for (auto &it : items)
-    if (it.h) {
+    if (it.h && it.dv) {
       int rc = upload_ref(d, it.dv, it.h, it.n);
       if (rc) return rc;
     }
@@ -490,9 +569,10 @@ extern "C" int frehd_domain_download_state(frehd_domain *d, frehd_state *st) {
       {st->bottomXP, d->bottomXP, T}, {st->bottomYP, d->bottomYP, T},
       {st->surfOld, d->surf[o], T}, {st->EnXP, d->EnXP, T}, {st->EnYP, d->EnYP, T},
       {st->cellV, d->cellV, N}, {st->Sm, d->Sm, N}, {st->Fuu, d->Fuu, T}, {st->Fvv, d->Fvv, T},
+      {st->depthXP, d->dXP, T}, {st->depthYP, d->dYP, T},
   };
   for (auto &it : items)
-    if (it.h) {
+    if (it.h && it.dv) {
       int rc = download_ref(d, it.h, it.dv, it.n);
       if (rc) return rc;
     }
@@ -591,7 +671,7 @@ extern "C" int frehd_domain_init(frehd_domain *d, const double *bottom, const do
     if (dep[ii] < 0) dep[ii] = 0;
   }
   // updateAllFaceDepth (nsfunctions.c:143-236): only the interior face depths
-  // feed thinLayerDrag
+  // feed thinLayerDrag and the wind term
   for (long ii = 0; ii < N; ++ii) {
     const double a = s[ii], bE = s[m.iPjc(ii)], bN = s[m.icjP(ii)];
     hx[ii] = (a > bE ? a : bE) - bx[ii];
@@ -620,6 +700,7 @@ extern "C" int frehd_domain_init(frehd_domain *d, const double *bottom, const do
   st.surf = s.data(); st.uuXP = u.data(); st.vvYP = v.data(); st.S = S.data();
   st.depth = dep.data(); st.CDXP = cdx.data(); st.CDYP = cdy.data();
   st.bottomZ = bz.data(); st.bottomXP = bx.data(); st.bottomYP = by.data(); st.ind = ind.data();
+  st.depthXP = hx.data(); st.depthYP = hy.data();  // held for the wind term only
   int rc = frehd_domain_upload_state(d, &st);
   if (rc) return rc;
   {

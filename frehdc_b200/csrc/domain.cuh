@@ -59,6 +59,11 @@ struct Params {
   double offset, surfmin, dsurf, tidePS, subR, dxf, dyf, eps;
   int Ne, useThinLayer, useScalar, tideFirst, tideLen, maxIter;
   int scalarAdv;      // 1: first-order upwind, 2: TVD with the superbee limiter
+  // inflow cells i in [inflowI0, inflowI1), j in [inflowJ0, inflowJ1) (inflowLen of them)
+  int inflowLen, inflowI0, inflowI1, inflowJ0, inflowJ1;
+  double inflowS;
+  int useWind;        // windTerm (nsfunctions.c:609-648)
+  double rhoa, Cw, CwT;
   int mixed;          // CG: FP32 inner iterations inside FP64 iterative refinement
   double eps_inner;   // relative residual reduction of one FP32 inner solve
   // geometry source
@@ -111,12 +116,30 @@ struct View {
   double *partials;  // per-block partial sums
   const double *tide;
   int ntide;
+  const double *inflow;        // bc->inflow by step
+  int ninflow;
+  const double *wspd;          // bc->windspd by step
+  int nwspd;
+  const double *wcos, *wsin;   // cos/sin of the wind direction by step (nwdir + 1 entries;
+  int nwdir;                   // the last one for steps past the series)
+  double *dXP, *dYP;           // face depths of the last updateAllFaceDepth (wind only)
   Scratch *sc;
 };
 
 __device__ __forceinline__ double tide_value(const View &w) {
   const int tt = w.sc->tt;
   return (tt >= 0 && tt < w.ntide) ? w.tide[tt] : 0.0;
+}
+
+// bc->inflow[tt]; past the end of the series the reference reads its zeroed guard.
+__device__ __forceinline__ double inflow_value(const View &w) {
+  const int tt = w.sc->tt;
+  return (tt >= 0 && tt < w.ninflow) ? w.inflow[tt] : 0.0;
+}
+
+// Inflow cell: inflowLoc[k] = jj*NX + ii - 1 (configuration.c:53-60).
+__device__ __forceinline__ bool is_inflow(const Params &p, int i, int j) {
+  return p.inflowLen > 0 && i >= p.inflowI0 && i < p.inflowI1 && j >= p.inflowJ0 && j < p.inflowJ1;
 }
 
 __device__ __forceinline__ bool is_tidal(const Params &p, int i, int j) {

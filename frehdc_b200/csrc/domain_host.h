@@ -39,6 +39,9 @@ struct frehd_domain {
   long npartials = 0;
   double *tide = nullptr;
   int ntide = 0;
+  double *inflow = nullptr, *wspd = nullptr, *wcos = nullptr, *wsin = nullptr;
+  int ninflow = 0, nwspd = 0, nwdir = 0;
+  double *dXP = nullptr, *dYP = nullptr;  // face depths read by the wind term
   double *tables = nullptr, *zf = nullptr;
   frehd::Scratch *sc = nullptr;
   frehd::StepOut *out = nullptr;

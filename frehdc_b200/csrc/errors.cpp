@@ -81,4 +81,9 @@ extern "C" void frehd_config_defaults(frehd_config *c) {
   c->eps = 1e-8;
   c->maxIter = 10000000;
   c->offset = 0.0;
+  c->inflowI0 = c->inflowI1 = c->inflowJ0 = c->inflowJ1 = 0;
+  c->inflowS = 0.0;
+  c->northAngle = 0.0;
+  c->rhoa = 1.25;
+  c->Cw = 0.0013;
 }

@@ -57,6 +57,32 @@ struct Ex {
   double En, Drag;
 };
 
+// windTerm (nsfunctions.c:609-648) of cell k: the stress (the same for both
+// faces) and the cosine and sine of the step's wind direction, which the host
+// takes with its libm as the reference does (frehd_domain_set_series).
+struct Wind {
+  double tau, c, s;
+};
+
+__device__ __forceinline__ Wind wind_at(const View &w, long k) {
+  const Params &p = w.p;
+  const int tt = w.sc->tt;
+  const double W = (tt >= 0 && tt < w.nwspd) ? w.wspd[tt] : 0.0;
+  const int q = (tt >= 0 && tt < w.nwdir) ? tt : w.nwdir;
+  Wind r;
+  r.c = w.wcos[q];
+  r.s = w.wsin[q];
+  const double a = W - w.u[k] * r.c - w.v[k] * r.s;
+  r.tau = p.rhoa * p.Cw * a * a;
+  return r;
+}
+
+// The face's share: the thin-layer decay below hD (the reference's depth test),
+// no stress on a dry face.
+__device__ __forceinline__ double wind_face(const Params &p, double tau, double h) {
+  return (h < p.hD && p.useThinLayer == 1) ? tau * exp(p.CwT * (h - p.hD) / p.hD) : tau;
+}
+
 // One cell's x-momentum source: explicitVelocity, advectionTerm with the CFL
 // limiter (nsfunctions.c:498-586), diffusionTermSub (subgrid.c:781-812),
 // dragTermSub with staggeredV = 1 (subgrid.c:857-927) and dragInversion
@@ -93,6 +119,11 @@ __device__ Ex explicit_x(const View &w, int i, int j) {
          (p.NUy / Vx) * (w.Oy[k] * (uN - u0) / p.dy - rd(w.Oy, g, i, j - 1) * (-uS + u0) / p.dy);
   }
   En = En + p.dt * fx;
+  if (p.useWind) {
+    const Wind wd = wind_at(w, k);
+    const double h = w.dXP[k];
+    if (h > 0) En = En + p.dt * wind_face(p, wd.tau, h) * wd.c / (h * 1000.0);
+  }
   const double velx = sqrt(u0 * u0 + vX * vX);
   const double hx = Vx > 0 ? w.Zx[k] / Vx : 0;
   Ex r;
@@ -135,6 +166,11 @@ __device__ Ex explicit_y(const View &w, int i, int j) {
          (p.NUy / Vy) * (rd(w.Oy, g, i, j + 1) * (vN - v0) / p.dy - w.Oy[k] * (-vS + v0) / p.dy);
   }
   En = En + p.dt * fy;
+  if (p.useWind) {  // the y term is subtracted (nsfunctions.c:642-645)
+    const Wind wd = wind_at(w, k);
+    const double h = w.dYP[k];
+    if (h > 0) En = En - p.dt * wind_face(p, wd.tau, h) * wd.s / (h * 1000.0);
+  }
   const double vely = sqrt(uY * uY + v0 * v0);
   const double hy = Vy > 0 ? w.Zy[k] / Vy : 0;
   Ex r;
@@ -205,9 +241,10 @@ static __device__ __forceinline__ void explicit_tile(const View &w, int bx, int 
   const double gxe = GnXP, gyn = GnYP;
   const double dxdy = p.dx * p.dy;
   double Ct = w.Z[k] + GnXP + GnYP + GnXM + GnYM;
-  // matrixSourceTermSub (subgrid.c:934-974), no inflow cells
+  // matrixSourceTermSub (subgrid.c:934-974) with its inflow cells (:959-968)
   const double s = w.surf_cur[k];
   double b = s * w.Z[k] - p.dt * (ex.En * w.Nx[k] - EnW * NxW) - p.dt * (ey.En * w.Oy[k] - EnS * OyS);
+  if (is_inflow(p, i, j)) b = b + p.dt * (inflow_value(w) / p.inflowLen);
   if (b == 0 || b == s * p.dx * p.dy) b = s * p.dx * p.dy;
   // matrixCoeffSub singular-row guards (subgrid.c:1061-1078)
   if (Ct == 0.0 || Ct == dxdy) Ct = dxdy;
@@ -778,6 +815,8 @@ static __device__ __forceinline__ void update_vel_tile(const View &w, int bx, in
     // volumeByFluxSub (subgrid.c:1227-1263)
     const double cv_old = w.cellV[k];
     double cv = cv_old + p.dt * (FW - FE + FS - FN);
+    const bool inflow_cell = is_inflow(p, i, j);
+    if (inflow_cell) cv = cv + inflow_value(w) * p.dt;
     if (cv < 0) cv = 0;
     w.cellV[k] = cv;
     vol = cv;
@@ -791,7 +830,7 @@ static __device__ __forceinline__ void update_vel_tile(const View &w, int bx, in
       CDY = coeff / pow(h, 1.0 / 3.0);
     }
     const double dep = w.depth_nxt[k];
-    if (p.useThinLayer && dep > 0) {
+    if ((p.useThinLayer && dep > 0) || p.useWind) {
       double hxp = 0, hyp = 0;
       if (i < g.nx - 1) {
         const double a = sN, c = w.surf_nxt[g.at(i + 1, j)];
@@ -803,8 +842,14 @@ static __device__ __forceinline__ void update_vel_tile(const View &w, int bx, in
         hyp = (a > c ? a : c) - w.bottomYP[k];
         if (hyp < 0) hyp = 0;
       }
-      if (hxp <= p.hD) CDX = coeff / pow(dep, 2.0 / 3.0);
-      if (hyp <= p.hD) CDY = coeff / pow(dep, 2.0 / 3.0);
+      if (p.useThinLayer && dep > 0) {
+        if (hxp <= p.hD) CDX = coeff / pow(dep, 2.0 / 3.0);
+        if (hyp <= p.hD) CDY = coeff / pow(dep, 2.0 / 3.0);
+      }
+      if (p.useWind) {  // updateAllFaceDepth's interior faces, read by the next windTerm
+        w.dXP[k] = hxp;
+        w.dYP[k] = hyp;
+      }
     }
     w.CDXP[k] = CDX;
     w.CDYP[k] = CDY;
@@ -828,6 +873,8 @@ static __device__ __forceinline__ void update_vel_tile(const View &w, int bx, in
       Sm = Sm + p.dt * (-FE * Sd + FW * Su - FN * Sr + FS * Sl);
       Sm = Sm + p.dt * ((p.Kx * w.Nx[k] / p.dx) * (SE - Sc) - (p.Kx * NxW / p.dx) * (Sc - SW) +
                         (p.Ky * w.Oy[k] / p.dy) * (SNn - Sc) - (p.Ky * OyS / p.dy) * (Sc - SS));
+      // scalar from inflow (subgrid.c:1648-1654); inflow cells skip the limiter
+      if (inflow_cell) Sm = Sm + p.inflowS * inflow_value(w) * p.dt / p.inflowLen;
       int cnt = 0;
       double smax = 0, smin = 0;
 #define FREHD_NB(cond, val)                                 \
@@ -844,8 +891,8 @@ static __device__ __forceinline__ void update_vel_tile(const View &w, int bx, in
       FREHD_NB(j > 0 && OyS > 0 && rd(w.surf_cur, g, i, j - 1) - rd(w.bottomZ, g, i, j - 1) > 0, SS);
 #undef FREHD_NB
       double Sn = cv > 0 ? Sm / cv : 0;
-      if (cnt != 0 && Sn > smax) Sn = smax;
-      else if (cnt != 0 && Sn < smin) Sn = smin;
+      if (cnt != 0 && Sn > smax && !inflow_cell) Sn = smax;
+      else if (cnt != 0 && Sn < smin && !inflow_cell) Sn = smin;
       double depf = dep;
       if ((Sn > 100 || Sn < 0) && !(j == 0) && !(j == g.ny - 1 && i > 0)) {
         Sn = 0;

@@ -58,6 +58,17 @@ class DeckSpec:
     scalar_in_window: bool = False  # plume at the centre of the (cropped) window, not the basin
     block_check: bool = False       # checkBlock = 1 face areas (largest wet cluster per block)
     scalar_adv: int = 1             # scalarAdv: 1 first-order upwind, 2 TVD (superbee)
+    # inflow cells (i0, i1, j0, j1), half-open, 0-based; None = none.  The inflow
+    # is inflow_q * (1 + 0.5 sin(2 pi t / 3 h)) m^3/s over all of them, carrying
+    # scalar at concentration inflow_s
+    inflow_cells: tuple | None = None
+    inflow_q: float = 0.0
+    inflow_s: float = 0.0
+    # wind (useWind = 1 when wind_speed > 0): speed wind_speed * (1 + 0.3 sin(.)),
+    # direction wind_dir + 20 sin(.) degrees from north, before north_angle
+    wind_speed: float = 0.0
+    wind_dir: float = 0.0
+    north_angle: float = 0.0
     dsurf: float = 0.01
     eps: float = 1e-12
     max_iter: int = 100000
@@ -95,6 +106,9 @@ class Deck:
     Nt: int                 # steps the data.dat allows (configuration.c:26)
     NT_days: float
     offset: float           # bathymetry offset the model adds (bathymetry.c:98-102)
+    inflow_v: np.ndarray | None = None   # inflow.dat values at tide_t (m^3/s)
+    wspd_v: np.ndarray | None = None     # windspd.dat values at tide_t (m/s)
+    wdir_v: np.ndarray | None = None     # winddir.dat values at tide_t (degrees)
     extra: dict = field(default_factory=dict)
 
     @property
@@ -230,10 +244,15 @@ def make_deck(spec: DeckSpec, start: str = DEFAULT_START, with_tables: bool = Fa
 
     zmin = float(bottom.min())
     offset = 0.0 if zmin >= 0 else -zmin            # bathymetry.c:98-102
+    ph = 2.0 * np.pi * (tide_t - t0) / 10800.0
+    inflow_v = spec.inflow_q * (1.0 + 0.5 * np.sin(ph)) if spec.inflow_cells else None
+    wspd_v = spec.wind_speed * (1.0 + 0.3 * np.sin(ph)) if spec.wind_speed > 0 else None
+    wdir_v = spec.wind_dir + 20.0 * np.sin(0.7 * ph) if spec.wind_speed > 0 else None
     deck = Deck(spec=spec, nx=nx, ny=ny, r=r, zf=zf, bottom=bottom, bottomXP=bxp, bottomYP=byp,
                 surf0=surf0.reshape(-1).copy(), S0=S0.reshape(-1).copy(), surfmin=surfmin,
                 surfmax=surfmax, dsurf=spec.dsurf, Ne=Ne, start=start, tide_t=tide_t,
-                tide_v=tide_v, Nt=Nt, NT_days=NT_days, offset=offset)
+                tide_v=tide_v, Nt=Nt, NT_days=NT_days, offset=offset, inflow_v=inflow_v,
+                wspd_v=wspd_v, wdir_v=wdir_v)
     if with_tables:
         deck.extra["tables"] = build_tables(deck)
     return deck
@@ -249,13 +268,30 @@ def build_tables(deck: Deck) -> np.ndarray:
 
 # --------------------------------------------------------------------------- tide
 def tide_series(deck: Deck) -> np.ndarray:
-    """bc->tideP[0..Nt) as the reference computes it from tideP.dat.
+    """bc->tideP[0..Nt) as the reference computes it from tideP.dat."""
+    return bc_series(deck, deck.tide_v)
+
+
+def forcing_series(deck: Deck) -> dict:
+    """bc->inflow / windspd / winddir[0..Nt) of the deck's forcing (only those
+    its data.dat switches on)."""
+    out = {}
+    if deck.inflow_v is not None:
+        out["inflow"] = bc_series(deck, deck.inflow_v)
+    if deck.wspd_v is not None:
+        out["windspd"] = bc_series(deck, deck.wspd_v)
+        out["winddir"] = bc_series(deck, deck.wdir_v)
+    return out
+
+
+def bc_series(deck: Deck, v: np.ndarray) -> np.ndarray:
+    """One BC array [0..Nt) as the reference computes it from a "t,value" file
+    on the deck's time axis.
 
     Restates readOneBC/searchInd/dataInterp (initialize.c:447-477,
     utilities.c:65-86,129-148) with the same double arithmetic.
     """
     t = deck.tide_t
-    v = deck.tide_v
     dt = deck.spec.dt
     itval = int(t[1] - t[0])
     t_start = float(t[0])
@@ -300,6 +336,11 @@ def data_dat_values(deck: Deck, out_hours: float | None = None) -> list:
         out_hours = (deck.Nt + 1000) * s.dt / 3600.0
     nx, ny = deck.nx, deck.ny
     M = len(deck.tide_t)
+    if s.inflow_cells:  # inflowLoc = jj*NX + ii - 1 for ii in [v27, v28), jj in [v29, v30)
+        i0, i1, j0, j1 = s.inflow_cells
+        inflow_vals = [(i1 - i0) * (j1 - j0), i0 + 1, i1 + 1, j0, j1]
+    else:
+        inflow_vals = [0, 1, 1, 0, 0]
     return [
         deck.start, "input/", "output/", "subdata/",
         s.dx, s.dx, nx, ny, s.dt, deck.NT_days, 0, out_hours,   # 4..11
@@ -307,9 +348,9 @@ def data_dat_values(deck: Deck, out_hours: float | None = None) -> list:
         1,                                                      # 19 bcType: tide on YP
         nx, 0, M,                                               # 20..22 tideP: whole row
         1, 1, M,                                                # 23..25 tideM (unused)
-        0, 1, 1, 0, 0, M,                                       # 26..31 no inflow cells
-        0, 0, M, M,                                             # 32..35 no wind
-        1, s.scalar_adv, 1, 0.0, 1, 0.0, M, 1, 0.0, M,          # 36..45 scalar, tide S = 0
+        *inflow_vals, M,                                        # 26..31 inflow cells
+        1 if s.wind_speed > 0 else 0, s.north_angle, M, M,      # 32..35 wind
+        1, s.scalar_adv, 1, s.inflow_s, 1, 0.0, M, 1, 0.0, M,   # 36..45 scalar, tide S = 0
         0.0, 0.0, 0.0, 0.0, 0, 1, 1, 0,                         # 46..53 IC from files
         1, 0, s.dx / s.r, s.dx / s.r,                           # 54..57 subgrid
         deck.surfmax, deck.surfmin, deck.dsurf,                 # 58..60
@@ -397,9 +438,15 @@ def write_reference_deck(deck: Deck, path: str, tables: np.ndarray | None = None
     with open(os.path.join(inp, "tideP.dat"), "w") as f:
         for t, v in zip(deck.tide_t, deck.tide_v):
             f.write("%s,%s\n" % (_fmt(t), _fmt(v)))
+    inflow = deck.inflow_v if deck.inflow_v is not None else np.zeros(len(deck.tide_t))
     with open(os.path.join(inp, "inflow.dat"), "w") as f:
-        for t in deck.tide_t:
-            f.write("%s,0\n" % _fmt(t))
+        for t, v in zip(deck.tide_t, inflow):
+            f.write("%s,%s\n" % (_fmt(t), _fmt(v)))
+    if deck.wspd_v is not None:
+        for name, vals in (("windspd.dat", deck.wspd_v), ("winddir.dat", deck.wdir_v)):
+            with open(os.path.join(inp, name), "w") as f:
+                for t, v in zip(deck.tide_t, vals):
+                    f.write("%s,%s\n" % (_fmt(t), _fmt(v)))
     return path
 
 

@@ -138,6 +138,34 @@ static int make_config(const Config *s, const Bath *bath, frehd_config *c) {
   c->useEvap = s->useEvap;
   c->useRain = s->useRain;
   c->inflowLocLength = s->inflowLocLength;
+  /* inflow cells: the rectangle configuration.c:53-60 lists (i-index minus one
+   * in its loop) */
+  if (s->inflowLocLength > 0) {
+    int i0 = s->nx, i1 = -1, j0 = s->ny, j1 = -1;
+    for (int k = 0; k < s->inflowLocLength; ++k) {
+      const int i = s->inflowLoc[k] % s->nx, j = s->inflowLoc[k] / s->nx;
+      if (s->inflowLoc[k] < 0 || j >= s->ny) {
+        fprintf(stderr, "frehd_b200: inflow cell %d outside the domain\n", s->inflowLoc[k]);
+        return FREHD_ERR_UNSUPPORTED;
+      }
+      if (i < i0) i0 = i;
+      if (i > i1) i1 = i;
+      if (j < j0) j0 = j;
+      if (j > j1) j1 = j;
+    }
+    c->inflowI0 = i0;
+    c->inflowI1 = i1 + 1;
+    c->inflowJ0 = j0;
+    c->inflowJ1 = j1 + 1;
+    if ((long)(i1 + 1 - i0) * (j1 + 1 - j0) != s->inflowLocLength) {
+      fprintf(stderr, "frehd_b200: inflow cells must form a rectangle\n");
+      return FREHD_ERR_UNSUPPORTED;
+    }
+  }
+  c->inflowS = s->inflowS;
+  c->northAngle = s->northAngle;
+  c->rhoa = s->rhoa;
+  c->Cw = s->Cw;
   c->useSubStep = s->useSubStep;
   c->checkConservation = s->checkConservation;
   c->minDepth = s->minDepth;
@@ -172,6 +200,8 @@ static void persistent_fields(frehd_state *st, Data *data, Sub *sub) {
   st->Zx = sub->Zx;
   st->Zy = sub->Zy;
   st->ind = sub->ind;
+  st->depthXP = data->depthXP;  /* read by the wind term; held only with useWind */
+  st->depthYP = data->depthYP;
 }
 
 int frehd_gpu_init(Data *data, Sub *sub, Bath *bath, BC *bc, Config *setting, int device) {
@@ -198,6 +228,13 @@ int frehd_gpu_init(Data *data, Sub *sub, Bath *bath, BC *bc, Config *setting, in
   free(tables);
   if (rc) return note(rc);
   rc = frehd_domain_set_tide(g_dom, setting->Nt, bc->tideP);
+  if (rc) return note(rc);
+  /* readBC (initialize.c:345-378) loads inflow always, the wind only with useWind */
+  rc = frehd_domain_set_series(g_dom, FREHD_SERIES_INFLOW, setting->Nt, bc->inflow);
+  if (!rc && setting->useWind == 1)
+    rc = frehd_domain_set_series(g_dom, FREHD_SERIES_WIND_SPEED, setting->Nt, bc->windspd);
+  if (!rc && setting->useWind == 1)
+    rc = frehd_domain_set_series(g_dom, FREHD_SERIES_WIND_DIR, setting->Nt, bc->winddir);
   if (rc) return note(rc);
   const char *prec = getenv("FREHD_PRECISION");
   if (prec && !strcmp(prec, "mixed")) {

@@ -60,6 +60,9 @@ class Config(C.Structure):
         ("minDepth", C.c_double), ("wtfh", C.c_double), ("CFLl", C.c_double),
         ("CFLh", C.c_double), ("eps", C.c_double), ("maxIter", C.c_int),
         ("offset", C.c_double),
+        ("inflowI0", C.c_int), ("inflowI1", C.c_int), ("inflowJ0", C.c_int), ("inflowJ1", C.c_int),
+        ("inflowS", C.c_double), ("northAngle", C.c_double), ("rhoa", C.c_double),
+        ("Cw", C.c_double),
     ]
 
 
@@ -68,7 +71,9 @@ STATE_FIELDS = [
     "V", "Z", "Nx", "Oy", "Vx", "Vy", "Zx", "Zy", "ind",
     "bottomZ", "bottomXP", "bottomYP",
     "surfOld", "uuYP", "vvXP", "EnXP", "EnYP", "cellV", "Sm", "Fuu", "Fvv",
+    "depthXP", "depthYP",   # held only with useWind = 1
 ]
+WIND_FIELDS = ("depthXP", "depthYP")
 # arrays carrying the ghost ring (N2ct) vs interior only (N)
 STATE_N = {"depth", "uuYP", "vvXP", "cellV", "Sm"}
 
@@ -140,6 +145,7 @@ X0_ZERO, X0_SURFACE = 0, 1
 CG_SINGLE_SWEEP, CG_TWO_PHASE = 0, 1
 DECOUPLED_AS_ASSEMBLED, DECOUPLED_ELIMINATED = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
+SERIES_INFLOW, SERIES_WIND_SPEED, SERIES_WIND_DIR = 1, 2, 3
 STATUS = {0: "ok", 1: "invalid", 2: "unsupported", 3: "cuda", 4: "nomem", 5: "cg_noconverge",
           6: "cfl", 7: "timeout", 8: "state"}
 
@@ -160,6 +166,7 @@ def _declare_domain(L: C.CDLL) -> None:
     L.frehd_domain_set_fine_bottoms.argtypes = [_vp, C.c_int, _dp, C.c_long]
     L.frehd_domain_set_fine_bottoms_ex.argtypes = [_vp, C.c_int, _dp, C.c_long, C.c_int]
     L.frehd_domain_set_tide.argtypes = [_vp, C.c_int, _dp]
+    L.frehd_domain_set_series.argtypes = [_vp, C.c_int, C.c_int, _dp]
     L.frehd_domain_set_solver.argtypes = [_vp, C.c_int]
     L.frehd_domain_set_cg_schedule.argtypes = [_vp, C.c_int]
     L.frehd_domain_set_decoupled.argtypes = [_vp, C.c_int]
@@ -251,6 +258,11 @@ class Domain:
         t = np.ascontiguousarray(tideP, dtype=np.float64)
         check(lib().frehd_domain_set_tide(self.h, len(t), as_dp(t)), "set_tide")
 
+    def set_series(self, kind: int, values: np.ndarray):
+        """bc->inflow / windspd / winddir by step (SERIES_*)."""
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        check(lib().frehd_domain_set_series(self.h, kind, len(v), as_dp(v)), "set_series")
+
     def set_solver(self, x0: int):
         check(lib().frehd_domain_set_solver(self.h, x0), "set_solver")
 
@@ -293,7 +305,7 @@ class Domain:
         check(lib().frehd_domain_upload_state(self.h, C.byref(st)), "upload_state")
 
     def download(self, names=None) -> dict:
-        names = STATE_FIELDS if names is None else names
+        names = [n for n in STATE_FIELDS if n not in WIND_FIELDS] if names is None else names
         st = State()
         out = {}
         for name in names:
@@ -511,6 +523,9 @@ def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0
             deck.extra["tables"] = tabs
         d.set_tables(tabs)
     d.set_tide(D.tide_series(deck))
+    for kind, series in D.forcing_series(deck).items():
+        d.set_series({"inflow": SERIES_INFLOW, "windspd": SERIES_WIND_SPEED,
+                      "winddir": SERIES_WIND_DIR}[kind], series)
     d.set_solver(x0)
     d.set_cg_schedule(schedule)
     d.set_decoupled(decoupled)

@@ -74,6 +74,13 @@ typedef struct frehd_config {
   double eps;                 /* CG stop: ||r||_2 < eps*||b||_2 (rtc.c:53) */
   int maxIter;
   double offset;              /* bathymetry offset -min(z) (bathymetry.c:98-102) */
+  /* forcing (configuration.c:53-65,71,78-79) */
+  int inflowI0, inflowI1;     /* inflow cells: i in [inflowI0, inflowI1), the data.dat first and
+                                 last i-index minus one (configuration.c:57) ... */
+  int inflowJ0, inflowJ1;     /* ... and j in [inflowJ0, inflowJ1); inflowLocLength cells */
+  double inflowS;             /* scalar concentration of the inflow */
+  double northAngle, rhoa, Cw; /* wind (useWind = 1): direction offset in degrees, air
+                                  density, wind drag coefficient */
 } frehd_config;
 
 void frehd_config_defaults(frehd_config *cfg);
@@ -128,6 +135,9 @@ typedef struct frehd_state {
   double *EnXP, *EnYP;       /* N2ct  explicit velocities after drag inversion */
   double *cellV, *Sm;        /* N     cell volume and scalar mass after the update */
   double *Fuu, *Fvv;         /* N2ct  face flow rates */
+  /* face depths of the last updateAllFaceDepth (nsfunctions.c:143-236), N2ct; held
+   * only with useWind = 1, whose term reads them (otherwise skipped) */
+  double *depthXP, *depthYP;
 } frehd_state;
 
 /* Per-domain counters of the last step. */
@@ -162,6 +172,14 @@ int frehd_domain_set_fine_bottoms_ex(frehd_domain *d, int r, const double *zf, l
 
 /* Tidal elevation series bc->tideP (initialize.h:28-32), indexed by step tt. */
 int frehd_domain_set_tide(frehd_domain *d, int n, const double *tideP);
+/* The other boundary series of BC (initialize.h:28-32, read by readBC,
+ * initialize.c:345-378), indexed by step tt like tideP; past the end of a series
+ * a step reads zero:
+ *   FREHD_SERIES_INFLOW      bc->inflow, m^3/s over all inflow cells
+ *   FREHD_SERIES_WIND_SPEED  bc->windspd, m/s (useWind = 1)
+ *   FREHD_SERIES_WIND_DIR    bc->winddir, degrees from north before northAngle */
+enum { FREHD_SERIES_INFLOW = 1, FREHD_SERIES_WIND_SPEED = 2, FREHD_SERIES_WIND_DIR = 3 };
+int frehd_domain_set_series(frehd_domain *d, int kind, int n, const double *values);
 
 /* Copy state in the reference layout to/from the device (NULL fields skipped). */
 int frehd_domain_upload_state(frehd_domain *d, const frehd_state *st);

@@ -19,8 +19,9 @@
  *
  * Supported Config subset (others are rejected at creation): useSubgrid = 1,
  * staggeredV = 1, useSubDrag = 0, CDnotN = 0, useminA = 0, useminV not in {1,2},
- * bcType = 1, no wind/evaporation/rain/inflow/sub-stepping, scalarAdv = 1 or 2,
- * useConstTidePS = 1, checkConservation = 0.
+ * bcType = 1, no evaporation/rain/sub-stepping, scalarAdv = 1 or 2,
+ * useConstTidePS = 1, checkConservation = 0.  Inflow cells and wind are
+ * supported (their series set with oracle_set_series).
  */
 #include <math.h>
 #include <stdint.h>
@@ -58,6 +59,9 @@ struct oracle_domain {
   /* BC */
   int nt;
   double *tideP;
+  int ninflow, nwind, nwdir;
+  double *inflow, *windspd, *winddir;  /* bc->inflow, windspd, winddir, indexed by tt */
+  int tt;                              /* step of the phase being run */
   /* solver */
   int precond, x0mode, last_iters;
   double last_acc;
@@ -136,8 +140,11 @@ static int check_cfg(oracle_domain *d) {
   if (c->useminA != 0) FAIL("useminA=%d unsupported", c->useminA);
   if (c->useminV == 1 || c->useminV == 2) FAIL("useminV=%d unsupported", c->useminV);
   if (c->bcType != 1) FAIL("bcType=%d unsupported", c->bcType);
-  if (c->useWind || c->useEvap || c->useRain || c->inflowLocLength || c->useSubStep)
-    FAIL("wind/evap/rain/inflow/substep unsupported");
+  if (c->useEvap || c->useRain || c->useSubStep) FAIL("evap/rain/substep unsupported");
+  if (c->inflowLocLength &&
+      (c->inflowI0 < 0 || c->inflowJ0 < 0 || c->inflowI1 > c->nx || c->inflowJ1 > c->ny ||
+       (long)(c->inflowI1 - c->inflowI0) * (c->inflowJ1 - c->inflowJ0) != c->inflowLocLength))
+    FAIL("inflow cells must be the rectangle of inflowLocLength interior cells");
   if (c->useScalar && ((c->scalarAdv != 1 && c->scalarAdv != 2) || c->useConstTidePS != 1))
     FAIL("scalar options unsupported");
   if (c->tideLocFirstP < 0 || c->tideLocFirstP + c->tideLocLengthP > c->nx)
@@ -189,7 +196,7 @@ void oracle_destroy(oracle_domain *d) {
                   d->allSurf, d->V, d->Z, d->Vxp, d->Vyp, d->Vxm, d->Vym, d->Np, d->Nm, d->Op,
                   d->Om, d->Nx, d->Oy, d->Vx, d->Vy, d->Zx, d->Zy, d->ind, d->bottomZ,
                   d->bottomXP, d->bottomYP, d->edgeX, d->edgeY, d->tideP, d->x, d->wr, d->wp,
-                  d->wq, d->wz};
+                  d->wq, d->wz, d->inflow, d->windspd, d->winddir};
   for (size_t k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); ++k) free(ptrs[k]);
   for (int t = 0; t < NTAB; ++t) free(d->tab[t]);
   free(d);
@@ -211,6 +218,29 @@ int oracle_set_tables(oracle_domain *d, int Ne, const double *tables) {
   /* initAllSubVar (subgrid.c:2116-2119) */
   for (int k = 0; k < Ne; ++k) d->allSurf[k] = d->c.surfmin + k * d->c.dsurf + d->c.offset;
   return 0;
+}
+
+/* bc->inflow (kind 1), bc->windspd (2), bc->winddir (3), indexed by tt. */
+int oracle_set_series(oracle_domain *d, int kind, int n, const double *v) {
+  double **dst = kind == 1 ? &d->inflow : kind == 2 ? &d->windspd : kind == 3 ? &d->winddir : NULL;
+  if (!dst || n < 0) return 1;
+  free(*dst);
+  *dst = dz(n);
+  if (n) memcpy(*dst, v, (size_t)n * sizeof(double));
+  if (kind == 1) d->ninflow = n; else if (kind == 2) d->nwind = n; else d->nwdir = n;
+  return 0;
+}
+
+/* A series value at step tt; past its end the reference reads the zeroed guard. */
+static double series_at(const double *a, int n, int tt) {
+  return (a && tt >= 0 && tt < n) ? a[tt] : 0.0;
+}
+
+/* Inflow cell test: inflowLoc[k] = jj*NX + ii - 1 (configuration.c:53-60). */
+static int is_inflow(const oracle_domain *d, long ii) {
+  if (!d->c.inflowLocLength) return 0;
+  const int i = (int)(ii % d->nx), j = (int)(ii / d->nx);
+  return i >= d->c.inflowI0 && i < d->c.inflowI1 && j >= d->c.inflowJ0 && j < d->c.inflowJ1;
 }
 
 int oracle_set_tide(oracle_domain *d, int n, const double *tideP) {
@@ -629,6 +659,35 @@ static void diffusion(oracle_domain *d) {
   }
 }
 
+/* windTerm (nsfunctions.c:609-648): uniform wind stress with the thin-layer
+ * decay, pi and the water density as the reference writes them, on the face
+ * depths of the last updateAllFaceDepth.  Note the sign of the y term. */
+static void wind(oracle_domain *d) {
+  const double pi = 3.1415926, rho = 1000;
+  const double W = series_at(d->windspd, d->nwind, d->tt);
+  const double phi = series_at(d->winddir, d->nwdir, d->tt) + d->c.northAngle;
+  const double omega = phi * pi / 180.0;
+  const double dt = d->c.dt, hD = d->c.hD, CwT = d->c.CwT;
+  for (long ii = 0; ii < d->N; ++ii) {
+    const double tau = d->c.rhoa * d->c.Cw *
+                       (W - d->uuXP[ii] * cos(omega) - d->vvYP[ii] * sin(omega)) *
+                       (W - d->uuXP[ii] * cos(omega) - d->vvYP[ii] * sin(omega));
+    double tauXP, tauYP;
+    if (d->depthXP[ii] < hD && d->c.useThinLayer == 1)
+      tauXP = tau * exp(CwT * (d->depthXP[ii] - hD) / hD);
+    else
+      tauXP = tau;
+    if (d->depthYP[ii] < hD && d->c.useThinLayer == 1)
+      tauYP = tau * exp(CwT * (d->depthYP[ii] - hD) / hD);
+    else
+      tauYP = tau;
+    if (d->depthXP[ii] > 0)
+      d->EnXP[ii] = d->EnXP[ii] + dt * tauXP * cos(omega) / (d->depthXP[ii] * rho);
+    if (d->depthYP[ii] > 0)
+      d->EnYP[ii] = d->EnYP[ii] - dt * tauYP * sin(omega) / (d->depthYP[ii] * rho);
+  }
+}
+
 /* dragTermSub (subgrid.c:857-927, staggeredV = 1) and dragInversion
  * (nsfunctions.c:730-746) */
 static void drag(oracle_domain *d) {
@@ -651,13 +710,22 @@ static void drag(oracle_domain *d) {
   for (int j = 0; j < d->ny; ++j) d->EnYP[d->iMgt[j]] = d->EnYP[d->iMbd[j]];
 }
 
-/* matrixSourceTermSub (subgrid.c:930-975), no inflow cells */
+/* matrixSourceTermSub (subgrid.c:930-975) */
 static void rhs(oracle_domain *d) {
   const double dt = d->c.dt;
   for (long k = 0; k < d->N; ++k) {
     const int c = d->trps[k], w = d->iMjc[c], s = d->icjM[c];
     d->z[k] = d->surf[c] * d->Z[c] - dt * (d->EnXP[c] * d->Nx[c] - d->EnXP[w] * d->Nx[w]) -
               dt * (d->EnYP[c] * d->Oy[c] - d->EnYP[s] * d->Oy[s]);
+  }
+  /* inflow cells (subgrid.c:959-968; bcType != 3) */
+  if (d->c.inflowLocLength) {
+    const double q = series_at(d->inflow, d->ninflow, d->tt);
+    for (long ii = 0; ii < d->N; ++ii)
+      if (is_inflow(d, ii)) {
+        const long k = d->sprt[ii];
+        d->z[k] = d->z[k] + dt * (q / d->c.inflowLocLength);
+      }
   }
   for (long k = 0; k < d->N; ++k) {
     const int c = d->trps[k];
@@ -713,8 +781,10 @@ static void assemble(oracle_domain *d, int tt) {
 }
 
 void oracle_explicit(oracle_domain *d, int tt) {
+  d->tt = tt;
   advection(d);
   diffusion(d);
+  if (d->c.useWind) wind(d);
   drag(d);
   rhs(d);
   assemble(d, tt);
@@ -928,11 +998,13 @@ static void tidal_velocity(oracle_domain *d) {
   }
 }
 
-/* volumeByFluxSub (subgrid.c:1227-1263), no inflow/evaporation/rain */
+/* volumeByFluxSub (subgrid.c:1227-1263), inflow cells, no evaporation/rain */
 static void volume_by_flux(oracle_domain *d) {
+  const double q = series_at(d->inflow, d->ninflow, d->tt);
   for (long ii = 0; ii < d->N; ++ii) {
     d->cellV[ii] = d->cellV[ii] + d->c.dt * (d->Fuu[d->iMjc[ii]] - d->Fuu[ii] +
                                              d->Fvv[d->icjM[ii]] - d->Fvv[ii]);
+    if (is_inflow(d, ii)) d->cellV[ii] = d->cellV[ii] + q * d->c.dt;
     if (d->cellV[ii] < 0) d->cellV[ii] = 0;
   }
 }
@@ -1101,10 +1173,18 @@ static void scalar_transport(oracle_domain *d) {
       smin[ii] = mn;
     }
   }
+  /* scalar from inflow (subgrid.c:1648-1654); inflow cells skip the limiter */
+  if (d->c.inflowLocLength) {
+    const double q = series_at(d->inflow, d->ninflow, d->tt);
+    for (long ii = 0; ii < N; ++ii)
+      if (is_inflow(d, ii))
+        Sm[ii] = Sm[ii] + d->c.inflowS * q * dt / d->c.inflowLocLength;
+  }
   for (long ii = 0; ii < N; ++ii) {
     S[ii] = d->cellV[ii] > 0 ? Sm[ii] / d->cellV[ii] : 0;
-    if (cnt[ii] != 0 && S[ii] > smax[ii]) S[ii] = smax[ii];
-    else if (cnt[ii] != 0 && S[ii] < smin[ii]) S[ii] = smin[ii];
+    const int flag = is_inflow(d, ii);
+    if (cnt[ii] != 0 && S[ii] > smax[ii] && !flag) S[ii] = smax[ii];
+    else if (cnt[ii] != 0 && S[ii] < smin[ii] && !flag) S[ii] = smin[ii];
   }
   free(cnt); free(smax); free(smin);
   for (long ii = 0; ii < N; ++ii)
@@ -1138,6 +1218,7 @@ static double monitor_cfl(oracle_domain *d) {
 /* getFreeSurface .. enforceTidalBC (nsfunctions.c:1020-1031; nssolve.c:169-177),
  * updateData, scalarTransport and monitorCFL.  x: transposed order. */
 double oracle_update(oracle_domain *d, int tt, const double *x) {
+  d->tt = tt;
   for (long k = 0; k < d->T; ++k) d->surfOld[k] = d->surf[k];
   for (long k = 0; k < d->N; ++k) d->surf[d->trps[k]] = x[k];
   zero_neg_surf(d, tt);

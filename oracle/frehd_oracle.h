@@ -25,6 +25,9 @@ typedef struct oracle_cfg {
   double eps;
   int maxIter;
   double offset;
+  int inflowI0, inflowI1, inflowJ0, inflowJ1;
+  double inflowS;
+  double northAngle, rhoa, Cw;
 } oracle_cfg;
 
 typedef struct oracle_domain oracle_domain;
@@ -37,6 +40,8 @@ void oracle_destroy(oracle_domain *d);
 const char *oracle_error(const oracle_domain *d);
 int oracle_set_tables(oracle_domain *d, int Ne, const double *tables);
 int oracle_set_tide(oracle_domain *d, int n, const double *tideP);
+/* bc->inflow (kind 1), bc->windspd (2), bc->winddir (3), indexed by tt. */
+int oracle_set_series(oracle_domain *d, int kind, int n, const double *values);
 void oracle_set_solver(oracle_domain *d, int precond, int x0mode);
 int oracle_init(oracle_domain *d, const double *bottom, const double *bottomXP,
                 const double *bottomYP, const double *surf0, const double *u0,

@@ -57,6 +57,9 @@ class OracleCfg(C.Structure):
         ("minDepth", C.c_double), ("wtfh", C.c_double), ("CFLl", C.c_double),
         ("CFLh", C.c_double), ("eps", C.c_double), ("maxIter", C.c_int),
         ("offset", C.c_double),
+        ("inflowI0", C.c_int), ("inflowI1", C.c_int), ("inflowJ0", C.c_int), ("inflowJ1", C.c_int),
+        ("inflowS", C.c_double), ("northAngle", C.c_double), ("rhoa", C.c_double),
+        ("Cw", C.c_double),
     ]
 
 
@@ -72,6 +75,7 @@ def lib() -> C.CDLL:
         L.oracle_error.argtypes = [C.c_void_p]
         L.oracle_set_tables.argtypes = [C.c_void_p, C.c_int, _dp]
         L.oracle_set_tide.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.oracle_set_series.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
         L.oracle_set_solver.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.oracle_init.argtypes = [C.c_void_p] + [_dp] * 7 + [C.c_int]
         L.oracle_explicit.argtypes = [C.c_void_p, C.c_int]
@@ -117,6 +121,12 @@ class Oracle:
         tideP = np.ascontiguousarray(tideP, dtype=np.float64)
         self._chk(L.oracle_set_tide(h, len(tideP), _p(tideP)))
         L.oracle_set_solver(h, precond, x0)
+
+    def set_series(self, kind: str, values: np.ndarray) -> None:
+        """bc->inflow / windspd / winddir by step."""
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        k = {"inflow": 1, "windspd": 2, "winddir": 3}[kind]
+        self._chk(lib().oracle_set_series(self.h, k, len(v), _p(v)))
 
     def _chk(self, rc):
         if rc != 0:
@@ -180,5 +190,7 @@ def from_deck(deck, precond: int = PRECOND_SSOR, x0: int = X0_ZERO) -> Oracle:
         tables = D.build_tables(deck)
         deck.extra["tables"] = tables
     o = Oracle(cfg, tables, D.tide_series(deck), precond=precond, x0=x0)
+    for kind, series in D.forcing_series(deck).items():
+        o.set_series(kind, series)
     o.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
     return o

@@ -24,6 +24,12 @@ SPECS = {
     # TVD (superbee) scalar advection, scalar.c:99-249
     "tvd44x36": D.DeckSpec(nx=44, ny=36, steps=40, seed=13, dry_frac=0.3, dt=2.0,
                            scalar_adv=2, scalar_sigma=60.0),
+    # inflow cells (configuration.c:53-60, subgrid.c:959-968,1236-1241,1648-1666)
+    # and wind with the thin-layer decay (nsfunctions.c:609-648)
+    "inflow36x30": D.DeckSpec(nx=36, ny=30, steps=30, seed=21, dry_frac=0.3,
+                              inflow_cells=(4, 7, 2, 4), inflow_q=3.0, inflow_s=35.0),
+    "wind40x32": D.DeckSpec(nx=40, ny=32, steps=30, seed=23, dry_frac=0.3,
+                            wind_speed=9.0, wind_dir=60.0, north_angle=15.0),
 }
 
 _cache: dict = {}
@@ -60,6 +66,22 @@ def mismatches(a: dict, b: dict, names, exact: bool = True, rtol: float = 0.0):
     return out
 
 
+def inflow_source(d, tt: int) -> np.ndarray:
+    """Volume each cell receives from the deck's inflow at step tt: every inflow
+    cell gets the whole inflow times dt (subgrid.c:1236-1241), while the
+    continuity equation shares it among them (subgrid.c:959-968)."""
+    N = d.nx * d.ny
+    src = np.zeros(N)
+    if d.spec.inflow_cells:
+        q = D.forcing_series(d)["inflow"]
+        qt = q[tt] if tt < len(q) else 0.0
+        i0, i1, j0, j1 = d.spec.inflow_cells
+        for j in range(j0, j1):
+            for i in range(i0, i1):
+                src[j * d.nx + i] = qt * d.spec.dt
+    return src
+
+
 def max_rel(a, b) -> float:
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
@@ -67,18 +89,22 @@ def max_rel(a, b) -> float:
     return float(np.max(np.abs(a - b))) / scale
 
 
-def ledger_residual(V_old, cellV, Fuu, Fvv, nx: int, ny: int, dt: float) -> float:
+def ledger_residual(V_old, cellV, Fuu, Fvv, nx: int, ny: int, dt: float, source=None) -> float:
     """Relative misclosure of one step's volume ledger (volumeByFluxSub,
     subgrid.c:1227-1263): the cell volumes after the flux update must add up to
     the volumes before it plus dt times the net inflow through the domain's
-    outer faces, plus the water added where a negative volume was clipped to 0.
-    Arrays in the reference layout (ghost ring after the N interior cells)."""
+    outer faces, plus the volume the inflow cells receive (`source`, per cell,
+    added before the clip), plus the water added where a negative volume was
+    clipped to 0.  Arrays in the reference layout (ghost ring after the N
+    interior cells)."""
     N = nx * ny
     ii = np.arange(N)
     i, j = ii % nx, ii // nx
     iM = np.where(i == 0, N + 2 * nx + ny + j, ii - 1)   # iMjc (map.c)
     jM = np.where(j == 0, N + nx + i, ii - nx)           # icjM
     raw = V_old[:N] + dt * (Fuu[iM] - Fuu[:N] + Fvv[jM] - Fvv[:N])
+    src = np.zeros(N) if source is None else np.asarray(source, dtype=np.float64)
+    raw = raw + src
     clip_added = float(np.sum(np.where(raw < 0, -raw, 0.0)))
     # outer faces: west (ghost column), east (i = nx-1), south (ghost row), north (j = ny-1)
     west = Fuu[N + 2 * nx + ny + np.arange(ny)]
@@ -87,5 +113,5 @@ def ledger_residual(V_old, cellV, Fuu, Fvv, nx: int, ny: int, dt: float) -> floa
     north = Fvv[(ny - 1) * nx + np.arange(nx)]
     inflow = float(np.sum(west) - np.sum(east) + np.sum(south) - np.sum(north))
     total = float(np.sum(cellV[:N]))
-    want = float(np.sum(V_old[:N])) + dt * inflow + clip_added
+    want = float(np.sum(V_old[:N])) + dt * inflow + float(np.sum(src)) + clip_added
     return abs(total - want) / max(abs(total), 1e-300)

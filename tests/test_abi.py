@@ -49,7 +49,7 @@ def test_noalloc_rejects_oversize_without_device_work():
 def test_domain_create_rejects_unsupported_option():
     from frehdc_b200 import deck as D
     cfg = D.config_dict(D.make_deck(D.DeckSpec(nx=16, ny=12, steps=2)))
-    cfg["useWind"] = 1
+    cfg["useminA"] = 1
     with pytest.raises(native.FrehdError) as e:
         native.Domain(cfg)
     assert e.value.status == 2

@@ -55,7 +55,7 @@ def test_init_bitwise(name, geometry, scratch):
 
 
 @pytest.mark.parametrize("name,steps", [("wet48x40", 6), ("dry40x36", 25), ("dry37x29", 25),
-                                        ("tvd44x36", 25)])
+                                        ("tvd44x36", 25), ("inflow36x30", 20)])
 def test_phases_bitwise(name, steps, scratch):
     """Each step: the oracle's state is uploaded, then the device's explicit
     phase and update phase (fed the oracle's x) must give the oracle's doubles."""
@@ -80,6 +80,34 @@ def test_phases_bitwise(name, steps, scratch):
         assert mismatches(got, ref, POW, exact=False, rtol=1e-15) == [], tt
 
 
+def test_phases_with_wind(scratch):
+    """Wind (nsfunctions.c:609-648): the direction's cosine and sine are taken on
+    the host as the reference takes them, so only the thin-layer decay's exp()
+    may differ from glibc's in the last place; the phases match to 1e-15."""
+    d, _ = deck_for("wind40x32", str(scratch))
+    o = port.from_deck(d, precond=port.PRECOND_JACOBI, x0=port.X0_ZERO)
+    g = native.domain_from_deck(d, geometry="fine")
+    up = UPLOAD + ["depthXP", "depthYP"]
+    names = ["GnCt", "GnXP", "GnXM", "GnYP", "GnYM", "z", "EnXP", "EnYP"]
+    for tt in range(1, 16):
+        g.upload(_oracle_state(o, up))
+        o.explicit(tt)
+        g.phase(native.PHASE_EXPLICIT, tt)
+        sysg = {**g.system(), **g.download(["EnXP", "EnYP"])}
+        assert mismatches(sysg, _oracle_state(o, names), names, exact=False, rtol=1e-15) == [], tt
+        o.solve()
+        x = o.get("x")
+        o.update(tt, x)
+        g.phase(native.PHASE_UPDATE, tt, x_ext=x)
+        got = g.download(EXACT + POW + ["depthXP", "depthYP"])
+        ref = _oracle_state(o, EXACT + POW + ["depthXP", "depthYP"])
+        assert mismatches(got, ref, EXACT + POW, exact=False, rtol=1e-13) == [], tt
+        # the face depths the next wind term reads are the update's own doubles
+        N = d.nx * d.ny
+        assert np.array_equal(got["depthXP"][:N], ref["depthXP"][:N]), tt
+        assert np.array_equal(got["depthYP"][:N], ref["depthYP"][:N]), tt
+
+
 SCHEDULES = {"single_sweep": native.CG_SINGLE_SWEEP, "two_phase": native.CG_TWO_PHASE}
 
 
@@ -102,7 +130,8 @@ def test_solve_matches_oracle(name, schedule, scratch):
 
 
 @pytest.mark.parametrize("schedule", list(SCHEDULES))
-@pytest.mark.parametrize("name", ["wet48x40", "dry40x36", "dry37x29", "tvd44x36"])
+@pytest.mark.parametrize("name", ["wet48x40", "dry40x36", "dry37x29", "tvd44x36", "inflow36x30",
+                                  "wind40x32"])
 def test_full_run_matches_oracle(name, schedule, scratch):
     """Whole run against the oracle in the reference's own solver set-up (SSOR-PCG
     from x = 0, which tracks the reference program to ~1e-13)."""

@@ -61,7 +61,8 @@ def test_init_bitwise(name, scratch):
 
 
 @pytest.mark.parametrize("name,steps", [("wet48x40", 8), ("dry40x36", 30), ("dry37x29", 40),
-                                        ("tvd44x36", 40)])
+                                        ("tvd44x36", 40), ("inflow36x30", 30),
+                                        ("wind40x32", 30)])
 def test_phases_bitwise(name, steps, scratch):
     """Each phase of each step from the reference's own pre-phase state."""
     d, path = deck_for(name, str(scratch))

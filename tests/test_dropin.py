@@ -94,7 +94,7 @@ def _read_outputs(folder: str) -> dict:
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("output", ["host", "device"])
-@pytest.mark.parametrize("name", ["wet48x40", "dry40x36"])
+@pytest.mark.parametrize("name", ["wet48x40", "dry40x36", "inflow36x30", "wind40x32"])
 def test_dropin_matches_reference_program(name, output, tmp_path):
     if native.device_count() < 1:
         pytest.fail("no CUDA device visible: the GPU tests need a B200")

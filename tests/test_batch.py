@@ -85,8 +85,8 @@ def test_served_results_equal_alone(scratch):
     same state as each request's domain stepped alone in a batch."""
     from frehdc_b200 import serve
     names = list(SPECS)
-    steps = {"wet48x40": 7, "dry40x36": 11, "dry37x29": 5, "tvd44x36": 9, "inflow36x30": 6,
-             "wind40x32": 8}
+    steps = {"wet48x40": 7, "dry40x36": 11, "dry37x29": 5, "tvd44x36": 9, "tvdwet44x36": 4,
+             "inflow36x30": 6, "wind40x32": 8}
     results = {}
 
     def done(req):

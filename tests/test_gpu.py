@@ -130,8 +130,8 @@ def test_solve_matches_oracle(name, schedule, scratch):
 
 
 @pytest.mark.parametrize("schedule", list(SCHEDULES))
-@pytest.mark.parametrize("name", ["wet48x40", "dry40x36", "dry37x29", "tvd44x36", "inflow36x30",
-                                  "wind40x32"])
+@pytest.mark.parametrize("name", ["wet48x40", "dry40x36", "dry37x29", "tvdwet44x36",
+                                  "inflow36x30", "wind40x32"])
 def test_full_run_matches_oracle(name, schedule, scratch):
     """Whole run against the oracle in the reference's own solver set-up (SSOR-PCG
     from x = 0, which tracks the reference program to ~1e-13)."""

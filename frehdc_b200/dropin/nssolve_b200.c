@@ -258,6 +258,8 @@ int frehd_gpu_run(int t0, int nsteps) {
   return note(frehd_domain_run(g_dom, t0, nsteps));
 }
 
+int frehd_gpu_step(int tt) { return frehd_gpu_run(tt, 1); }
+
 int frehd_gpu_sync_to_host(Data *data, Sub *sub) {
   if (!g_dom) return note(FREHD_ERR_STATE);
   if (!data || !sub) return note(FREHD_ERR_INVALID);

@@ -45,6 +45,8 @@ int frehd_gpu_init(struct Data *data, struct Sub *sub, struct Bath *bath, struct
  * the host arrays are not touched.  FREHD_ERR_CFL: the device stopped after the
  * step whose max CFL exceeded 20 (frehd_gpu_last_step). */
 int frehd_gpu_run(int t0, int nsteps);
+/* One step tt on the device (frehd_gpu_run(tt, 1)). */
+int frehd_gpu_step(int tt);
 /* Copy the device state into the host's Data and Sub arrays (every field the
  * step writes), so the reference's output and monitoring code can read them. */
 int frehd_gpu_sync_to_host(struct Data *data, struct Sub *sub);

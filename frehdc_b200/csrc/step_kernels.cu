@@ -942,7 +942,9 @@ static __device__ __forceinline__ void update_vel_tile(const View &w, int bx, in
   }
 }
 
-__global__ void __launch_bounds__(TBX *TBY) k_update_vel(View w) {
+// Four blocks per SM (64 registers): 1.78 -> 1.49 ms per step at 4096 x 4096
+// against the unconstrained 72 registers and three blocks.
+__global__ void __launch_bounds__(TBX *TBY, 4) k_update_vel(View w) {
   if (*(volatile int *)&w.sc->status != FREHD_OK) return;
   update_vel_tile<false>(w, blockIdx.x, blockIdx.y, gridDim.x);
 }

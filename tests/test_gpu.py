@@ -6,11 +6,11 @@ go through pow(), where CUDA and glibc may differ in the last place, so they
 are compared to a few ulp.  The linear solve is compared to the CG tolerance.
 
 Whole runs: the surface and the scalar to 1e-9 relative (max norm).  Face
-velocities are compared to 3e-9: two solves that both meet ||r|| < 1e-12 ||b||
+velocities are compared to 6e-9.  Two solves that both meet ||r|| < 1e-12 ||b||
 (the reference's own SSOR-PCG and a Jacobi-PCG, both on the CPU) already differ
-by 1.2e-9 in the velocities of the 30%-dry deck, because u = En - g dt (Nx/Vx)
-d(eta) amplifies the solver's eta error on thin-water faces; the surface itself
-agrees to ~1e-11.
+in the velocities: by 1.2e-9 on the 30%-dry deck and 3.3e-9 after 40 steps of
+the 15%-dry TVD deck.  u = En - g dt (Nx/Vx) d(eta) amplifies the solver's eta
+error on thin-water faces; the surface itself agrees to ~1e-11.
 """
 import os
 
@@ -27,7 +27,7 @@ pytestmark = pytest.mark.gpu
 EXACT = ["surf", "uuXP", "vvYP", "S", "depth", "V", "Z", "Nx", "Oy", "Vx", "Vy", "Zx", "Zy", "ind",
          "surfOld", "cellV", "Sm", "Fuu", "Fvv", "CFLx", "CFLy", "uuYP", "vvXP"]
 POW = ["CDXP", "CDYP"]
-RUN_TOL = {"surf": 1e-9, "S": 1e-9, "uuXP": 3e-9, "vvYP": 3e-9}
+RUN_TOL = {"surf": 1e-9, "S": 1e-9, "uuXP": 6e-9, "vvYP": 6e-9}
 UPLOAD = ["surf", "uuXP", "vvYP", "S", "depth", "CDXP", "CDYP", "CFLx", "CFLy", "V", "Z", "Nx",
           "Oy", "Vx", "Vy", "Zx", "Zy", "ind", "bottomZ", "bottomXP", "bottomYP"]
 

@@ -455,6 +455,40 @@ extern "C" int frehd_domain_set_series(frehd_domain *d, int kind, int n, const d
   }
 }
 
+extern "C" int frehd_domain_update_series(frehd_domain *d, int kind, int t0, int n,
+                                          const double *values) {
+  if (!d || t0 < 0 || n < 0 || (n > 0 && !values)) return fail(FREHD_ERR_INVALID, "bad argument");
+  if (n == 0) return FREHD_OK;
+  double *dst = nullptr;
+  int len = 0;
+  switch (kind) {
+    case FREHD_SERIES_TIDE: dst = d->tide; len = d->ntide; break;
+    case FREHD_SERIES_INFLOW: dst = d->inflow; len = d->ninflow; break;
+    case FREHD_SERIES_WIND_SPEED: dst = d->wspd; len = d->nwspd; break;
+    case FREHD_SERIES_WIND_DIR: len = d->nwdir; break;
+    default: return fail(FREHD_ERR_INVALID, "unknown series kind %d", kind);
+  }
+  if ((long)t0 + n > len)
+    return fail(FREHD_ERR_INVALID, "entries %d..%d past the series' %d (set it first)", t0,
+                t0 + n - 1, len);
+  CUDA_TRY(cudaSetDevice(d->device));
+  if (kind != FREHD_SERIES_WIND_DIR) {
+    CUDA_TRY(cudaMemcpyAsync(dst + t0, values, sizeof(double) * n, cudaMemcpyHostToDevice, d->stream));
+    return FREHD_OK;
+  }
+  const double pi = 3.1415926;  // as in frehd_domain_set_series
+  std::vector<double> c(n), s(n);
+  for (int t = 0; t < n; ++t) {
+    const double omega = (values[t] + d->cfg.northAngle) * pi / 180.0;
+    c[t] = std::cos(omega);
+    s[t] = std::sin(omega);
+  }
+  CUDA_TRY(cudaMemcpyAsync(d->wcos + t0, c.data(), sizeof(double) * n, cudaMemcpyHostToDevice, d->stream));
+  CUDA_TRY(cudaMemcpyAsync(d->wsin + t0, s.data(), sizeof(double) * n, cudaMemcpyHostToDevice, d->stream));
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return FREHD_OK;
+}
+
 extern "C" int frehd_domain_set_solver(frehd_domain *d, int x0_mode) {
   if (!d || (x0_mode != FREHD_X0_ZERO && x0_mode != FREHD_X0_SURFACE))
     return fail(FREHD_ERR_INVALID, "bad solver option");

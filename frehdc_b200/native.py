@@ -145,7 +145,7 @@ X0_ZERO, X0_SURFACE = 0, 1
 CG_SINGLE_SWEEP, CG_TWO_PHASE = 0, 1
 DECOUPLED_AS_ASSEMBLED, DECOUPLED_ELIMINATED = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
-SERIES_INFLOW, SERIES_WIND_SPEED, SERIES_WIND_DIR = 1, 2, 3
+SERIES_TIDE, SERIES_INFLOW, SERIES_WIND_SPEED, SERIES_WIND_DIR = 0, 1, 2, 3
 STATUS = {0: "ok", 1: "invalid", 2: "unsupported", 3: "cuda", 4: "nomem", 5: "cg_noconverge",
           6: "cfl", 7: "timeout", 8: "state"}
 
@@ -167,6 +167,7 @@ def _declare_domain(L: C.CDLL) -> None:
     L.frehd_domain_set_fine_bottoms_ex.argtypes = [_vp, C.c_int, _dp, C.c_long, C.c_int]
     L.frehd_domain_set_tide.argtypes = [_vp, C.c_int, _dp]
     L.frehd_domain_set_series.argtypes = [_vp, C.c_int, C.c_int, _dp]
+    L.frehd_domain_update_series.argtypes = [_vp, C.c_int, C.c_int, C.c_int, _vp]
     L.frehd_domain_set_solver.argtypes = [_vp, C.c_int]
     L.frehd_domain_set_cg_schedule.argtypes = [_vp, C.c_int]
     L.frehd_domain_set_decoupled.argtypes = [_vp, C.c_int]
@@ -257,6 +258,13 @@ class Domain:
     def set_tide(self, tideP: np.ndarray):
         t = np.ascontiguousarray(tideP, dtype=np.float64)
         check(lib().frehd_domain_set_tide(self.h, len(t), as_dp(t)), "set_tide")
+
+    def update_series(self, kind: int, t0: int, n: int, ptr: int):
+        """Overwrite entries t0..t0+n-1 of a series from host memory at address
+        ptr (queued on the domain's stream; from pinned memory the values must
+        stay untouched until the next synchronisation)."""
+        check(lib().frehd_domain_update_series(self.h, kind, t0, n, C.c_void_p(ptr)),
+              "update_series")
 
     def set_series(self, kind: int, values: np.ndarray):
         """bc->inflow / windspd / winddir by step (SERIES_*)."""

@@ -178,8 +178,16 @@ int frehd_domain_set_tide(frehd_domain *d, int n, const double *tideP);
  *   FREHD_SERIES_INFLOW      bc->inflow, m^3/s over all inflow cells
  *   FREHD_SERIES_WIND_SPEED  bc->windspd, m/s (useWind = 1)
  *   FREHD_SERIES_WIND_DIR    bc->winddir, degrees from north before northAngle */
-enum { FREHD_SERIES_INFLOW = 1, FREHD_SERIES_WIND_SPEED = 2, FREHD_SERIES_WIND_DIR = 3 };
+enum { FREHD_SERIES_TIDE = 0, FREHD_SERIES_INFLOW = 1, FREHD_SERIES_WIND_SPEED = 2,
+       FREHD_SERIES_WIND_DIR = 3 };
 int frehd_domain_set_series(frehd_domain *d, int kind, int n, const double *values);
+/* Overwrite entries t0 .. t0+n-1 of a series already set (FREHD_SERIES_TIDE is
+ * bc->tideP), for forcing that arrives while the model runs.  The copy is queued
+ * on the domain's stream, ahead of the steps queued after it, and allocates
+ * nothing; from pinned host memory it returns before the copy is done, so the
+ * values must stay untouched until the domain's next synchronisation (a
+ * FREHD_SERIES_WIND_DIR update waits for its copy). */
+int frehd_domain_update_series(frehd_domain *d, int kind, int t0, int n, const double *values);
 
 /* Copy state in the reference layout to/from the device (NULL fields skipped). */
 int frehd_domain_upload_state(frehd_domain *d, const frehd_state *st);

@@ -108,6 +108,29 @@ def test_phases_with_wind(scratch):
         assert np.array_equal(got["depthYP"][:N], ref["depthYP"][:N]), tt
 
 
+def test_update_series_equals_set_series(scratch):
+    """Forcing streamed in while the model runs (frehd_domain_update_series,
+    queued before each step) gives the doubles of the same series set up front."""
+    d, _ = deck_for("wind40x32", str(scratch))
+    alt_tide = D.tide_series(d) + 0.03 * np.sin(np.arange(d.Nt))
+    alt_dir = D.forcing_series(d)["winddir"] + 25.0
+    whole = native.domain_from_deck(d)
+    whole.set_tide(alt_tide)
+    whole.set_series(native.SERIES_WIND_DIR, alt_dir)
+    streamed = native.domain_from_deck(d)
+    for tt in range(1, 9):
+        for kind, arr in ((native.SERIES_TIDE, alt_tide), (native.SERIES_WIND_DIR, alt_dir)):
+            streamed.update_series(kind, tt, 1, arr.ctypes.data + 8 * tt)
+        assert streamed.step(tt) == 0
+    assert whole.run(1, 8) == 0
+    a = whole.download(["surf", "uuXP", "vvYP", "S"])
+    b = streamed.download(["surf", "uuXP", "vvYP", "S"])
+    for n in a:
+        assert np.array_equal(a[n], b[n]), n
+    with pytest.raises(native.FrehdError):
+        streamed.update_series(native.SERIES_TIDE, d.Nt, 1, alt_tide.ctypes.data)
+
+
 SCHEDULES = {"single_sweep": native.CG_SINGLE_SWEEP, "two_phase": native.CG_TWO_PHASE}
 
 

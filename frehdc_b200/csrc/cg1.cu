@@ -68,7 +68,9 @@ constexpr int kRing = 2 * (kTW + 2) + 2 * kTH;   // cells of the one-cell halo r
 constexpr int kRedStride = 8;                    // partial sums per block in grid_allreduce
 constexpr int kMaxOuter = 8;                     // refinements of one mixed-precision solve
 static_assert(kTH == kCgThreads / 32, "one warp per tile row");
-static_assert(kRing <= kCgThreads, "one thread per halo-ring cell");
+constexpr int kRingPer = (kRing + kCgThreads - 1) / kCgThreads;  // halo-ring cells per thread
+// resident CTAs per SM the launch bounds ask for: 128 registers per thread either way
+constexpr int kCg1MinBlocks = kCgThreads >= 512 ? 1 : 512 / kCgThreads;
 
 // Box geometry of an element type: the tile sits kLeft cells into a box with a
 // two-cell halo at least, kLeft chosen so that the box's first column is
@@ -283,12 +285,19 @@ __device__ __forceinline__ bool sweep(const SweepMaps &m, T *rn_out, T *pn_out, 
           red[4] += (double)s.P[q] * (double)sv;
         }
       }
-      T rring = 0;
-      const int qr = threadIdx.x < kRing ? B::ring(threadIdx.x) : 0;
-      if (threadIdx.x < kRing) rring = s.R[qr] - alpha * apply<T>(s.P, s.HX, s.HY, qr);
+      T rring[kRingPer];
+      int qr[kRingPer];
+#pragma unroll
+      for (int t = 0; t < kRingPer; ++t) {
+        const int e = threadIdx.x + t * kCgThreads;
+        qr[t] = e < kRing ? B::ring(e) : 0;
+        rring[t] = e < kRing ? s.R[qr[t]] - alpha * apply<T>(s.P, s.HX, s.HY, qr[t]) : T(0);
+      }
 #pragma unroll
       for (int c = 0; c < CPT; ++c) s.R[B::q(c * 32 + tx, ty)] = rb[c];
-      if (threadIdx.x < kRing) s.R[qr] = rring;
+#pragma unroll
+      for (int t = 0; t < kRingPer; ++t)
+        if (threadIdx.x + t * kCgThreads < kRing) s.R[qr[t]] = rring[t];
     }
     __syncthreads();
 
@@ -752,7 +761,7 @@ static __device__ __forceinline__ bool cg1_smem(unsigned char *smem_raw, unsigne
   return true;
 }
 
-__global__ void __launch_bounds__(kCgThreads, 1)
+__global__ void __launch_bounds__(kCgThreads, kCg1MinBlocks)
     k_cg1(View w, const Cg1Maps *__restrict__ m, int x0_surface, int eliminate) {
   if (*(volatile int *)&w.sc->status != FREHD_OK) return;
   extern __shared__ unsigned char smem_raw[];
@@ -780,7 +789,7 @@ __global__ void __launch_bounds__(kCgThreads, 1)
 // one CTA's share of one domain's solve (rank `rank` of a group of `nb` CTAs,
 // all co-resident in this cooperative launch; a CTA of a multi-CTA group runs
 // no other job).  Each domain's view is taken at its current parity.
-__global__ void __launch_bounds__(kCgThreads, 1)
+__global__ void __launch_bounds__(kCgThreads, kCg1MinBlocks)
     k_cg1_batch(const View *__restrict__ views2, const Cg1Maps *const *__restrict__ maps,
                 const int *__restrict__ job_start, const CgJob *__restrict__ jobs) {
   extern __shared__ unsigned char smem_raw[];

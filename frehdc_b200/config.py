@@ -16,6 +16,7 @@ FIELDS = [
     "useWind", "useEvap", "useRain", "inflowLocLength", "useSubStep", "checkConservation",
     "minDepth", "wtfh", "CFLl", "CFLh", "eps", "maxIter", "offset",
     "inflowI0", "inflowI1", "inflowJ0", "inflowJ1", "inflowS", "northAngle", "rhoa", "Cw",
+    "nscalar",
 ]
 
 
@@ -72,6 +73,7 @@ def config_from_values(v: list, offset: float = 0.0) -> dict:
         # (configuration.c:53-60): cells i in [v27 - 1, v28 - 1), j in [v29, v30)
         inflowI0=i(v[27]) - 1, inflowI1=i(v[28]) - 1, inflowJ0=i(v[29]), inflowJ1=i(v[30]),
         inflowS=float(v[39]), northAngle=float(v[33]), rhoa=float(v[78]), Cw=float(v[79]),
+        nscalar=1,  # the reference carries one scalar, S
     )
     return c
 

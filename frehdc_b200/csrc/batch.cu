@@ -270,6 +270,7 @@ extern "C" int frehd_domain_footprint(const frehd_config *cfg, int r, long long 
   const long long nvel = (long long)((cfg->nx + 31) / 32) * ((cfg->ny + 7) / 8);
   long long b = 0;
   b += 2 * (3 * 8 + 4) * tot;       // surf, depth, S (double) and ind (int), both halves
+  if (cfg->useScalar && cfg->nscalar > 1) b += 2 * 8 * tot * (long long)(cfg->nscalar - 1);  // tracers
   b += 36 * 8 * tot;                // persistent, per-step and CG arrays
   b += tot;                         // rmv flags
   b += 4 * N + 2 * 8 * T;           // fix list, staging

@@ -65,6 +65,8 @@ int check_config(const frehd_config *c) {
     return fail(FREHD_ERR_INVALID, "inflow cells must be the rectangle of inflowLocLength interior cells");
   if (c->useScalar && ((c->scalarAdv != 1 && c->scalarAdv != 2) || c->useConstTidePS != 1))
     return fail(FREHD_ERR_UNSUPPORTED, "scalar: scalarAdv 1 or 2 with a constant tidal scalar");
+  if (c->nscalar < 0 || c->nscalar > FREHD_MAX_SCALARS)
+    return fail(FREHD_ERR_INVALID, "nscalar=%d (0 .. %d)", c->nscalar, FREHD_MAX_SCALARS);
   if (c->tideLocFirstP < 0 || c->tideLocLengthP < 0 || c->tideLocFirstP + c->tideLocLengthP > c->nx)
     return fail(FREHD_ERR_INVALID, "tidal cells outside the YP row");
   if (!(c->dsurf > 0) || !(c->dx > 0) || !(c->dy > 0) || !(c->dt > 0))
@@ -80,6 +82,7 @@ View make_view_at(const frehd_domain *d, int cur) {
   w.surf_cur = d->surf[c]; w.surf_nxt = d->surf[n];
   w.depth_cur = d->depth[c]; w.depth_nxt = d->depth[n];
   w.S_cur = d->S[c]; w.S_nxt = d->S[n];
+  for (int s = 0; s < FREHD_MAX_SCALARS - 1; ++s) { w.Tr_cur[s] = d->Tr[s][c]; w.Tr_nxt[s] = d->Tr[s][n]; }
   w.ind_cur = d->ind[c]; w.ind_nxt = d->ind[n];
   w.u = d->u; w.v = d->v; w.CDXP = d->CDXP; w.CDYP = d->CDYP; w.CFLx = d->CFLx; w.CFLy = d->CFLy;
   w.V = d->V; w.Z = d->Z; w.Nx = d->Nx; w.Oy = d->Oy; w.Vx = d->Vx; w.Vy = d->Vy; w.Zx = d->Zx;
@@ -248,6 +251,7 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
   p.subR = cfg->subR; p.dxf = cfg->dxf; p.dyf = cfg->dyf; p.eps = cfg->eps;
   p.Ne = (int)std::lround((cfg->surfmax - cfg->surfmin) / cfg->dsurf);  // subgrid.c:2115
   p.useThinLayer = cfg->useThinLayer; p.useScalar = cfg->useScalar; p.scalarAdv = cfg->scalarAdv;
+  p.nscalar = cfg->useScalar ? std::max(cfg->nscalar, 1) : 0;
   p.tideFirst = cfg->tideLocFirstP; p.tideLen = cfg->tideLocLengthP; p.maxIter = cfg->maxIter;
   p.inflowLen = cfg->inflowLocLength;
   p.inflowI0 = cfg->inflowI0; p.inflowI1 = cfg->inflowI1;
@@ -263,6 +267,7 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
     r |= dalloc(d, &d->depth[a], tot);
     r |= dalloc(d, &d->S[a], tot);
     r |= dalloc(d, &d->ind[a], tot);
+    for (int s = 0; s + 1 < p.nscalar && !r; ++s) r |= dalloc(d, &d->Tr[s][a], tot);
   }
   double **arrs[] = {&d->u, &d->v, &d->CDXP, &d->CDYP, &d->CFLx, &d->CFLy, &d->V, &d->Z, &d->Nx,
                      &d->Oy, &d->Vx, &d->Vy, &d->Zx, &d->Zy, &d->bottomZ, &d->bottomXP,
@@ -627,6 +632,59 @@ extern "C" int frehd_domain_download_state(frehd_domain *d, frehd_state *st) {
   }
   CUDA_TRY(cudaStreamSynchronize(d->stream));
   return FREHD_OK;
+}
+
+// Device buffers of scalar s at the current half (h = 0) or the other one (h = 1).
+static double *scalar_buf(frehd_domain *d, int s, int h) {
+  const int half = d->cur ^ h;
+  return s == 0 ? d->S[half] : d->Tr[s - 1][half];
+}
+
+static int check_scalar(const frehd_domain *d, int s) {
+  if (d->in_batch) return fail(FREHD_ERR_STATE, "the domain is stepped by a batch (release it first)");
+  if (!d->p.useScalar || s < 0 || s >= d->p.nscalar)
+    return fail(FREHD_ERR_INVALID, "scalar %d of a domain with %d", s, d->p.nscalar);
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_upload_scalar(frehd_domain *d, int s, const double *values) {
+  if (!d || !values) return fail(FREHD_ERR_INVALID, "null argument");
+  int rc = check_scalar(d, s);
+  if (rc) return rc;
+  CUDA_TRY(cudaSetDevice(d->device));
+  // both halves, as frehd_domain_upload_state does for S
+  for (int h = 0; h < 2 && !rc; ++h) rc = upload_ref(d, scalar_buf(d, s, h), values, d->T);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_download_scalar(frehd_domain *d, int s, double *values) {
+  if (!d || !values) return fail(FREHD_ERR_INVALID, "null argument");
+  int rc = check_scalar(d, s);
+  if (rc) return rc;
+  CUDA_TRY(cudaSetDevice(d->device));
+  rc = download_ref(d, values, scalar_buf(d, s, 0), d->T);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_init_scalar(frehd_domain *d, int s, const double *S0) {
+  if (!d) return fail(FREHD_ERR_INVALID, "null argument");
+  int rc = check_scalar(d, s);
+  if (rc) return rc;
+  if (!d->ready) return fail(FREHD_ERR_STATE, "domain has no state (frehd_domain_init first)");
+  CUDA_TRY(cudaSetDevice(d->device));
+  const long N = d->N;
+  std::vector<double> dep(N), S(d->T, 0.0);
+  rc = download_ref(d, dep.data(), d->depth[d->cur], N);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
+  // initFieldValues (initialize.c:410-430), then the dry-cell zeroing of Init
+  // (initialize.c:149); the ghost ring stays zero
+  for (long ii = 0; ii < N; ++ii) S[ii] = (S0 && dep[ii] > 0) ? S0[ii] : 0.0;
+  return frehd_domain_upload_scalar(d, s, S.data());
 }
 
 // ---------------------------------------------------------------- init

@@ -59,6 +59,7 @@ struct Params {
   double offset, surfmin, dsurf, tidePS, subR, dxf, dyf, eps;
   int Ne, useThinLayer, useScalar, tideFirst, tideLen, maxIter;
   int scalarAdv;      // 1: first-order upwind, 2: TVD with the superbee limiter
+  int nscalar;        // scalars transported (S and nscalar - 1 tracers)
   // inflow cells i in [inflowI0, inflowI1), j in [inflowJ0, inflowJ1) (inflowLen of them)
   int inflowLen, inflowI0, inflowI1, inflowJ0, inflowJ1;
   double inflowS;
@@ -99,6 +100,7 @@ struct View {
   Grid gr;
   // persistent state
   double *surf_cur, *surf_nxt, *depth_cur, *depth_nxt, *S_cur, *S_nxt;
+  double *Tr_cur[FREHD_MAX_SCALARS - 1], *Tr_nxt[FREHD_MAX_SCALARS - 1];  // tracers 1 ..
   int *ind_cur, *ind_nxt;
   double *u, *v, *CDXP, *CDYP, *CFLx, *CFLy;
   double *V, *Z, *Nx, *Oy, *Vx, *Vy, *Zx, *Zy;

@@ -20,6 +20,7 @@ struct frehd_domain {
   frehd::Params p;
   long N = 0, T = 0;
   double *surf[2] = {}, *depth[2] = {}, *S[2] = {};
+  double *Tr[FREHD_MAX_SCALARS - 1][2] = {};  // tracers 1 .. nscalar-1 (both halves)
   int *ind[2] = {};
   double *u = nullptr, *v = nullptr, *CDXP = nullptr, *CDYP = nullptr, *CFLx = nullptr,
          *CFLy = nullptr;

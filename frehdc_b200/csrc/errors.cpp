@@ -86,4 +86,5 @@ extern "C" void frehd_config_defaults(frehd_config *c) {
   c->northAngle = 0.0;
   c->rhoa = 1.25;
   c->Cw = 0.0013;
+  c->nscalar = 1;
 }

@@ -313,6 +313,14 @@ extern "C" int frehd_domain_write_output(frehd_domain *d, const char *prefix, in
     if (!rc) rc = frehd::write_file(prefix, it.name, tt, s);
     if (rc) return rc;
   }
+  // the tracers beside the scalar file: scalar1_<tt>.dat ...
+  for (int t = 1; (fields & FREHD_OUT_SCALAR) && t < d->p.nscalar; ++t) {
+    char name[16];
+    std::snprintf(name, sizeof(name), "scalar%d", t);
+    int rc = frehd::format_values(Values{d->Tr[t - 1][c], nx, pitch, 0.0}, N, d->stream, fs, &s);
+    if (!rc) rc = frehd::write_file(prefix, name, tt, s);
+    if (rc) return rc;
+  }
   // DataOutput always round-trips the interior surface through the datum
   frehd::k_surf_round_trip<<<(unsigned)((N + 255) / 256), 256, 0, d->stream>>>(d->surf[c], nx,
                                                                               d->gr.ny, pitch, off);

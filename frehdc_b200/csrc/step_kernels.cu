@@ -666,12 +666,11 @@ __device__ __forceinline__ double superbee(double r) {
 // stop at the ghost ring; icjMM of the second row (j = 1) is never assigned by
 // the reference and reads 0 (cell (0, 0)) under the zero-filled allocation the
 // parity build uses.  The YM Courant number uses dx, as the reference's does.
-__device__ void tvd_faces(const View &w, int i, int j, double FE, double FW, double FN, double FS,
-                          double uE, double uW, double vst, double vS, double *Sd_, double *Su_,
-                          double *Sr_, double *Sl_) {
+__device__ void tvd_faces(const View &w, const double *S, int i, int j, double FE, double FW,
+                          double FN, double FS, double uE, double uW, double vst, double vS,
+                          double *Sd_, double *Su_, double *Sr_, double *Sl_) {
   const Params &p = w.p;
   const Grid &g = w.gr;
-  const double *S = w.S_cur;
   const double dSmin = 0.00001;
   const long k = g.at(i, j);
   const double Sc = S[k], SE = S[g.at(i + 1, j)], SW = S[g.at(i - 1, j)];
@@ -752,6 +751,80 @@ __device__ void tvd_faces(const View &w, int i, int j, double FE, double FW, dou
 
 __device__ __forceinline__ unsigned long long dbits(double x) {
   return (unsigned long long)__double_as_longlong(x);
+}
+
+// What one cell's scalar update needs besides the scalar itself: the step's
+// face flows and velocities, volumes and depth, and which neighbours the
+// limiter may take its bounds from.
+struct ScalarCell {
+  double cv_old, cv, dep, FE, FW, FN, FS, uE, uW, vst, vS, NxW, OyS;
+  bool inflow, wE, wW, wN, wS;
+};
+
+// scalarTransport (scalar.c:30-57) of one scalar in cell (i, j): upwind or TVD
+// advection (scalar.c:72-249), scalarDiffusionSub (subgrid.c:1552-1567),
+// updateScalarSub (subgrid.c:1570-1713), enforceScalarBC (scalar.c:419-471).
+// `primary` is the reference's S: it stores Sm and, in the singularity branch
+// (S outside [0, 100], subgrid.c:1700-1712), queues the cell for the surface and
+// depth fix-up.  A tracer only takes the branch's zero, so the hydrodynamics
+// stay those of S.
+template <bool kTVD>
+static __device__ __forceinline__ void transport_scalar(const View &w, const double *S, double *Snx,
+                                                        bool primary, int i, int j, long k,
+                                                        const ScalarCell &c) {
+  const Params &p = w.p;
+  const Grid &g = w.gr;
+  const double Sc = S[k], SE = rd(S, g, i + 1, j), SW = rd(S, g, i - 1, j);
+  const double SNn = rd(S, g, i, j + 1), SS = rd(S, g, i, j - 1);
+  double Sm = Sc * c.cv_old;  // computeVolumeSub: Sm = S * cellV
+  double Sd, Su, Sr, Sl;
+  if (kTVD) {
+    tvd_faces(w, S, i, j, c.FE, c.FW, c.FN, c.FS, c.uE, c.uW, c.vst, c.vS, &Sd, &Su, &Sr, &Sl);
+  } else {
+    Sd = c.FE > 0 ? Sc : SE;
+    Su = c.FW > 0 ? SW : Sc;
+    Sr = c.FN > 0 ? Sc : SNn;
+    Sl = c.FS > 0 ? SS : Sc;
+  }
+  Sm = Sm + p.dt * (-c.FE * Sd + c.FW * Su - c.FN * Sr + c.FS * Sl);
+  Sm = Sm + p.dt * ((p.Kx * w.Nx[k] / p.dx) * (SE - Sc) - (p.Kx * c.NxW / p.dx) * (Sc - SW) +
+                    (p.Ky * w.Oy[k] / p.dy) * (SNn - Sc) - (p.Ky * c.OyS / p.dy) * (Sc - SS));
+  // scalar from inflow (subgrid.c:1648-1654); inflow cells skip the limiter
+  if (c.inflow) Sm = Sm + p.inflowS * inflow_value(w) * p.dt / p.inflowLen;
+  int cnt = 0;
+  double smax = 0, smin = 0;
+#define FREHD_NB(cond, val)                                 \
+  if (cond) {                                               \
+    const double v_ = (val);                                \
+    if (cnt == 0) { smax = v_; smin = v_; }                 \
+    else { if (v_ > smax) smax = v_; if (v_ < smin) smin = v_; } \
+    ++cnt;                                                  \
+  }
+  FREHD_NB(c.wE, SE);
+  FREHD_NB(c.wW, SW);
+  FREHD_NB(c.wN, SNn);
+  FREHD_NB(c.wS, SS);
+#undef FREHD_NB
+  double Sn = c.cv > 0 ? Sm / c.cv : 0;
+  if (cnt != 0 && Sn > smax && !c.inflow) Sn = smax;
+  else if (cnt != 0 && Sn < smin && !c.inflow) Sn = smin;
+  double depf = c.dep;
+  if ((Sn > 100 || Sn < 0) && !(j == 0) && !(j == g.ny - 1 && i > 0)) {
+    Sn = 0;
+    if (primary) {
+      depf = 0;
+      const int slot = atomicAdd(&w.sc->n_fix, 1);
+      w.fix_list[slot] = (int)k;
+    }
+  }
+  if (i == 0) Snx[g.at(-1, j)] = Sn;
+  if (i == g.nx - 1) Snx[g.at(g.nx, j)] = Sn;
+  if (j == 0) Snx[g.at(i, -1)] = Sn;
+  if (j == g.ny - 1) Snx[g.at(i, g.ny)] = Sn;
+  if (is_tidal(p, i, j)) Sn = p.tidePS;
+  if (depf <= 0) Sn = 0;
+  Snx[k] = Sn;
+  if (primary) w.Sm[k] = Sm;
 }
 
 // gx: the domain's tile-grid width (the block's partial-sum slot is by*gx + bx)
@@ -853,61 +926,23 @@ static __device__ __forceinline__ void update_vel_tile(const View &w, int bx, in
     }
     w.CDXP[k] = CDX;
     w.CDYP[k] = CDY;
-    // scalarTransport: upwind or TVD advection (scalar.c:72-249), scalarDiffusionSub
-    // (subgrid.c:1552-1567), updateScalarSub (subgrid.c:1570-1713), enforceScalarBC
-    // (scalar.c:419-471)
+    // scalarTransport for S and the tracers
     if (p.useScalar) {
-      const double *S = w.S_cur;
-      const double Sc = S[k], SE = rd(S, g, i + 1, j), SW = rd(S, g, i - 1, j);
-      const double SNn = rd(S, g, i, j + 1), SS = rd(S, g, i, j - 1);
-      double Sm = Sc * cv_old;  // computeVolumeSub: Sm = S * cellV
-      double Sd, Su, Sr, Sl;
-      if (kTVD) {
-        tvd_faces(w, i, j, FE, FW, FN, FS, uE, uW, vstore, vS, &Sd, &Su, &Sr, &Sl);
-      } else {
-        Sd = FE > 0 ? Sc : SE;
-        Su = FW > 0 ? SW : Sc;
-        Sr = FN > 0 ? Sc : SNn;
-        Sl = FS > 0 ? SS : Sc;
-      }
-      Sm = Sm + p.dt * (-FE * Sd + FW * Su - FN * Sr + FS * Sl);
-      Sm = Sm + p.dt * ((p.Kx * w.Nx[k] / p.dx) * (SE - Sc) - (p.Kx * NxW / p.dx) * (Sc - SW) +
-                        (p.Ky * w.Oy[k] / p.dy) * (SNn - Sc) - (p.Ky * OyS / p.dy) * (Sc - SS));
-      // scalar from inflow (subgrid.c:1648-1654); inflow cells skip the limiter
-      if (inflow_cell) Sm = Sm + p.inflowS * inflow_value(w) * p.dt / p.inflowLen;
-      int cnt = 0;
-      double smax = 0, smin = 0;
-#define FREHD_NB(cond, val)                                 \
-  if (cond) {                                               \
-    const double v_ = (val);                                \
-    if (cnt == 0) { smax = v_; smin = v_; }                 \
-    else { if (v_ > smax) smax = v_; if (v_ < smin) smin = v_; } \
-    ++cnt;                                                  \
-  }
-      FREHD_NB(w.Nx[k] > 0 && rd(w.surf_cur, g, i + 1, j) - rd(w.bottomZ, g, i + 1, j) > 0, SE);
-      FREHD_NB(NxW > 0 && rd(w.surf_cur, g, i - 1, j) - rd(w.bottomZ, g, i - 1, j) > 0, SW);
-      FREHD_NB((j < g.ny - 1 || i == 0) && w.Oy[k] > 0 &&
-                   rd(w.surf_cur, g, i, j + 1) - rd(w.bottomZ, g, i, j + 1) > 0, SNn);
-      FREHD_NB(j > 0 && OyS > 0 && rd(w.surf_cur, g, i, j - 1) - rd(w.bottomZ, g, i, j - 1) > 0, SS);
-#undef FREHD_NB
-      double Sn = cv > 0 ? Sm / cv : 0;
-      if (cnt != 0 && Sn > smax && !inflow_cell) Sn = smax;
-      else if (cnt != 0 && Sn < smin && !inflow_cell) Sn = smin;
-      double depf = dep;
-      if ((Sn > 100 || Sn < 0) && !(j == 0) && !(j == g.ny - 1 && i > 0)) {
-        Sn = 0;
-        depf = 0;
-        const int slot = atomicAdd(&w.sc->n_fix, 1);
-        w.fix_list[slot] = (int)k;
-      }
-      if (i == 0) w.S_nxt[g.at(-1, j)] = Sn;
-      if (i == g.nx - 1) w.S_nxt[g.at(g.nx, j)] = Sn;
-      if (j == 0) w.S_nxt[g.at(i, -1)] = Sn;
-      if (j == g.ny - 1) w.S_nxt[g.at(i, g.ny)] = Sn;
-      if (is_tidal(p, i, j)) Sn = p.tidePS;
-      if (depf <= 0) Sn = 0;
-      w.S_nxt[k] = Sn;
-      w.Sm[k] = Sm;
+      ScalarCell c;
+      c.cv_old = cv_old; c.cv = cv; c.dep = dep;
+      c.FE = FE; c.FW = FW; c.FN = FN; c.FS = FS;
+      c.uE = uE; c.uW = uW; c.vst = vstore; c.vS = vS; c.NxW = NxW; c.OyS = OyS;
+      c.inflow = inflow_cell;
+      // connected wet neighbours of the limiter (updateScalarSub, subgrid.c:1582-1640)
+      c.wE = w.Nx[k] > 0 && rd(w.surf_cur, g, i + 1, j) - rd(w.bottomZ, g, i + 1, j) > 0;
+      c.wW = NxW > 0 && rd(w.surf_cur, g, i - 1, j) - rd(w.bottomZ, g, i - 1, j) > 0;
+      c.wN = (j < g.ny - 1 || i == 0) && w.Oy[k] > 0 &&
+             rd(w.surf_cur, g, i, j + 1) - rd(w.bottomZ, g, i, j + 1) > 0;
+      c.wS = j > 0 && OyS > 0 && rd(w.surf_cur, g, i, j - 1) - rd(w.bottomZ, g, i, j - 1) > 0;
+      transport_scalar<kTVD>(w, w.S_cur, w.S_nxt, true, i, j, k, c);
+#pragma unroll
+      for (int t = 0; t < FREHD_MAX_SCALARS - 1; ++t)
+        if (t + 1 < p.nscalar) transport_scalar<kTVD>(w, w.Tr_cur[t], w.Tr_nxt[t], false, i, j, k, c);
     }
     // monitorCFL (nsfunctions.c:1196-1223)
     cflx = fabs(uE) * p.dt / p.dx;

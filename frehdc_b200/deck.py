@@ -69,6 +69,9 @@ class DeckSpec:
     wind_speed: float = 0.0
     wind_dir: float = 0.0
     north_angle: float = 0.0
+    # scalars carried (nscalar): S plus n_scalars - 1 tracers, plumes like S's
+    # placed around it (see _tracer_fields)
+    n_scalars: int = 1
     dsurf: float = 0.01
     eps: float = 1e-12
     max_iter: int = 100000
@@ -109,6 +112,7 @@ class Deck:
     inflow_v: np.ndarray | None = None   # inflow.dat values at tide_t (m^3/s)
     wspd_v: np.ndarray | None = None     # windspd.dat values at tide_t (m/s)
     wdir_v: np.ndarray | None = None     # winddir.dat values at tide_t (degrees)
+    tracers: list = field(default_factory=list)  # (N,) initial fields of tracers 1 ..
     extra: dict = field(default_factory=dict)
 
     @property
@@ -223,6 +227,8 @@ def make_deck(spec: DeckSpec, start: str = DEFAULT_START, with_tables: bool = Fa
         xcen = ((ii + i0) + 0.5) * spec.dx - 0.5 * nxf * spec.dx
         ycen = ((jj + j0) + 0.5) * spec.dx - 0.5 * nyf * spec.dx
     S0 = spec.scalar_peak * np.exp(-(xcen ** 2 + ycen ** 2) / (2.0 * spec.scalar_sigma ** 2))
+    W, H = (nx, ny) if spec.scalar_in_window else (nxf, nyf)
+    tracers = _tracer_fields(spec, xcen, ycen, W * spec.dx, H * spec.dx)
 
     lo_eta = min(-spec.tide_amp, -spec.eta0_amp)
     hi_eta = max(spec.tide_amp, spec.eta0_amp)
@@ -252,7 +258,7 @@ def make_deck(spec: DeckSpec, start: str = DEFAULT_START, with_tables: bool = Fa
                 surf0=surf0.reshape(-1).copy(), S0=S0.reshape(-1).copy(), surfmin=surfmin,
                 surfmax=surfmax, dsurf=spec.dsurf, Ne=Ne, start=start, tide_t=tide_t,
                 tide_v=tide_v, Nt=Nt, NT_days=NT_days, offset=offset, inflow_v=inflow_v,
-                wspd_v=wspd_v, wdir_v=wdir_v)
+                wspd_v=wspd_v, wdir_v=wdir_v, tracers=tracers)
     if with_tables:
         deck.extra["tables"] = build_tables(deck)
     return deck
@@ -461,6 +467,27 @@ def _write_table(path: str, tab: np.ndarray, binary: bool) -> None:
         _write_column(path, tab)
 
 
+def _tracer_fields(spec: DeckSpec, xcen, ycen, width: float, height: float) -> list:
+    """Initial fields of the tracers: tracer t is S's plume moved a quarter of
+    the basin from its centre, at angle 2 pi t / n_scalars, with peak
+    scalar_peak * (1 - 0.2 t); all values stay inside [0, 100]."""
+    out = []
+    for t in range(1, spec.n_scalars):
+        a = 2.0 * np.pi * t / spec.n_scalars
+        cx, cy = 0.25 * width * np.cos(a), 0.25 * height * np.sin(a)
+        peak = spec.scalar_peak * (1.0 - 0.2 * t)
+        f = peak * np.exp(-((xcen - cx) ** 2 + (ycen - cy) ** 2) / (2.0 * spec.scalar_sigma ** 2))
+        out.append(f.reshape(-1).copy())
+    return out
+
+
+def with_scalar(deck: Deck, S0: np.ndarray) -> Deck:
+    """The same deck with S starting from another field: the reference run that a
+    tracer with that initial field must reproduce."""
+    return dataclasses.replace(deck, S0=np.asarray(S0, dtype=np.float64).copy(), tracers=[],
+                               extra=dict(deck.extra))
+
+
 def config_dict(deck: Deck) -> dict:
     """frehd_config fields of a deck, read back through the data.dat mapping."""
     from .config import config_from_values
@@ -469,4 +496,6 @@ def config_dict(deck: Deck) -> dict:
     txt = [v if isinstance(v, str) else (_fmt(v) if isinstance(v, float) else str(v)) for v in vals]
     from .config import _strtod
     parsed = txt[:4] + [_strtod(t) for t in txt[4:]]
-    return config_from_values(parsed, offset=deck.offset)
+    c = config_from_values(parsed, offset=deck.offset)
+    c["nscalar"] = 1 + len(deck.tracers)
+    return c

@@ -62,7 +62,7 @@ class Config(C.Structure):
         ("offset", C.c_double),
         ("inflowI0", C.c_int), ("inflowI1", C.c_int), ("inflowJ0", C.c_int), ("inflowJ1", C.c_int),
         ("inflowS", C.c_double), ("northAngle", C.c_double), ("rhoa", C.c_double),
-        ("Cw", C.c_double),
+        ("Cw", C.c_double), ("nscalar", C.c_int),
     ]
 
 
@@ -175,6 +175,9 @@ def _declare_domain(L: C.CDLL) -> None:
     L.frehd_domain_upload_state.argtypes = [_vp, C.POINTER(State)]
     L.frehd_domain_download_state.argtypes = [_vp, C.POINTER(State)]
     L.frehd_domain_init.argtypes = [_vp] + [_dp] * 7 + [C.c_int]
+    L.frehd_domain_upload_scalar.argtypes = [_vp, C.c_int, _dp]
+    L.frehd_domain_download_scalar.argtypes = [_vp, C.c_int, _dp]
+    L.frehd_domain_init_scalar.argtypes = [_vp, C.c_int, _dp]
     L.frehd_domain_step.argtypes = [_vp, C.c_int]
     L.frehd_domain_run.argtypes = [_vp, C.c_int, C.c_int]
     L.frehd_domain_phase.argtypes = [_vp, C.c_int, C.c_int, _dp]
@@ -290,6 +293,23 @@ class Domain:
                 for a in (bottom, bottomXP, bottomYP, surf0, u0, v0, S0)]
         check(lib().frehd_domain_init(self.h, *[as_dp(a) for a in arrs], int(round_trip_output)),
               "init")
+
+    def init_scalar(self, s: int, S0=None):
+        """Init's setup of scalar s (a tracer for s >= 1) from its initial field (N values)."""
+        a = None if S0 is None else np.ascontiguousarray(S0, dtype=np.float64)
+        assert a is None or a.size == self.N
+        check(lib().frehd_domain_init_scalar(self.h, s, None if a is None else as_dp(a)),
+              "init_scalar")
+
+    def upload_scalar(self, s: int, values: np.ndarray):
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        assert a.size == self.T
+        check(lib().frehd_domain_upload_scalar(self.h, s, as_dp(a)), "upload_scalar")
+
+    def download_scalar(self, s: int) -> np.ndarray:
+        a = np.empty(self.T)
+        check(lib().frehd_domain_download_scalar(self.h, s, as_dp(a)), "download_scalar")
+        return a
 
     # state
     def _len(self, name: str) -> int:
@@ -472,6 +492,15 @@ class Batch:
         check(lib().frehd_batch_info(self.h, C.byref(i)), "frehd_batch_info")
         return {n: getattr(i, n) for n, _ in BatchInfo._fields_}
 
+    @staticmethod
+    def capacity(device: int = 0) -> int:
+        """Co-resident CTAs of the batched CG on this device."""
+        b = Batch(1 << 20, 1.0, device)
+        try:
+            return int(b.info()["cg_capacity"])
+        finally:
+            b.close()
+
     def stream(self) -> int:
         s = _vp()
         check(lib().frehd_batch_stream(self.h, C.byref(s)), "frehd_batch_stream")
@@ -540,4 +569,6 @@ def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0
     if precision != PRECISION_FP64:
         d.set_precision(precision, eps_inner)
     d.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
+    for s, field in enumerate(deck.tracers, start=1):
+        d.init_scalar(s, field)
     return d

@@ -81,7 +81,14 @@ typedef struct frehd_config {
   double inflowS;             /* scalar concentration of the inflow */
   double northAngle, rhoa, Cw; /* wind (useWind = 1): direction offset in degrees, air
                                   density, wind drag coefficient */
+  int nscalar;                /* scalars transported when useScalar = 1, 1 .. FREHD_MAX_SCALARS
+                                 (0 counts as 1).  Scalar 0 is the reference's S; the others are
+                                 passive tracers with S's transport, boundary and inflow values
+                                 (tidePS, inflowS), each one what the reference computes for S
+                                 when S starts from that tracer's field. */
 } frehd_config;
+
+#define FREHD_MAX_SCALARS 4
 
 void frehd_config_defaults(frehd_config *cfg);
 
@@ -192,6 +199,15 @@ int frehd_domain_update_series(frehd_domain *d, int kind, int t0, int n, const d
 /* Copy state in the reference layout to/from the device (NULL fields skipped). */
 int frehd_domain_upload_state(frehd_domain *d, const frehd_state *st);
 int frehd_domain_download_state(frehd_domain *d, frehd_state *st);
+/* Scalar s (0 .. nscalar-1; 0 is frehd_state.S) in the layout of the reference's
+ * S: Nt = (nx+2)(ny+2) doubles, interior row-major with the ghost ring appended. */
+int frehd_domain_upload_scalar(frehd_domain *d, int s, const double *values);
+int frehd_domain_download_scalar(frehd_domain *d, int s, double *values);
+/* The reference Init's setup of scalar s from its initial field S0 (N doubles,
+ * NULL for zeros; initFieldValues, initialize.c:410-430): the interior from S0,
+ * zero on the ghost ring and in dry cells (initialize.c:149).  After
+ * frehd_domain_init, for the tracers 1 .. nscalar-1. */
+int frehd_domain_init_scalar(frehd_domain *d, int s, const double *S0);
 
 /*
  * Run the reference's initialisation sequence on the device (initialize.c:40-155,
@@ -245,8 +261,9 @@ int frehd_domain_sync(frehd_domain *d);
  * the host.
  *   frehd_domain_write_output: the files of DataOutput (fileio.c:62-122) and
  *     SubOutput (fileio.c:125-155) selected by `fields`: uVelocity, vVelocity,
- *     surfaceZ (surf - offset), depth, cdxp and cdyp, scalar; SubNx, SubOy,
- *     SubVx, SubVy, SubV, SubZ.  Like DataOutput it then round-trips the
+ *     surfaceZ (surf - offset), depth, cdxp and cdyp, scalar (and scalar1 ..
+ *     scalar<nscalar-1> for the tracers); SubNx, SubOy, SubVx, SubVy, SubV, SubZ.
+ *     Like DataOutput it then round-trips the
  *     interior surface through the output datum (surf = (surf - offset) + offset),
  *     which the next step starts from.
  *   frehd_domain_write_restart: restart_<tt>.dat of writeRestartFile

@@ -53,3 +53,33 @@ def test_domain_create_rejects_unsupported_option():
     with pytest.raises(native.FrehdError) as e:
         native.Domain(cfg)
     assert e.value.status == 2
+
+
+def test_domain_create_rejects_too_many_scalars():
+    from frehdc_b200 import deck as D
+    cfg = D.config_dict(D.make_deck(D.DeckSpec(nx=16, ny=12, steps=2)))
+    cfg["nscalar"] = 5
+    with pytest.raises(native.FrehdError) as e:
+        native.Domain(cfg)
+    assert e.value.status == 1 and "nscalar" in str(e.value)
+
+
+def test_config_mirror_matches_the_c_struct(tmp_path):
+    """The ctypes mirror of frehd_config has the C compiler's size and offsets."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    fields = [n for n, _ in native.Config._fields_]
+    src = "#include <stdio.h>\n#include <stddef.h>\n#include \"frehd_b200.h\"\nint main(void){\n"
+    src += 'printf("%zu\\n", sizeof(frehd_config));\n'
+    src += "".join(f'printf("%zu\\n", offsetof(frehd_config, {n}));\n' for n in fields)
+    src += "return 0;}\n"
+    c = tmp_path / "probe.c"
+    c.write_text(src)
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-I", os.path.dirname(HEADER), str(c), "-o", str(exe)], check=True)
+    out = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    assert out[0] == C.sizeof(native.Config)
+    assert out[1:] == [getattr(native.Config, n).offset for n in fields]

@@ -14,18 +14,38 @@ import itertools
 
 from . import native
 
-CELLS_PER_CTA = (8192.0, 16384.0, 32768.0, 65536.0, 131072.0)
+CELLS_PER_CTA = (8192.0, 16384.0, 32768.0, 65536.0, 131072.0, 196608.0, 262144.0, 393216.0,
+                 524288.0)
 EPS_INNER = (1e-4, 1e-5, 1e-6)
+CTX, CTY = 128, 16   # CG tile of k_cg1
 
 
-def time_batch(decks, cells_per_cta: float, steps: int, warmup: int, budget: int,
+def ctas_needed(sizes, cells_per_cta: float, capacity: int = 148) -> int:
+    """CTAs of the batched CG for domains of these (nx, ny): each domain's
+    group is round(cells / cells_per_cta) CTAs (at least 1, at most its tile
+    count), multi-CTA groups get CTAs of their own and the single-CTA domains
+    share the rest (batch.cu, group_size / ctas_needed)."""
+    dedicated, singles = 0, 0
+    for nx, ny in sizes:
+        ntiles = ((nx + CTX - 1) // CTX) * ((ny + CTY - 1) // CTY)
+        g = max(1, min(int(round(nx * ny / cells_per_cta)), ntiles, capacity))
+        if g > 1:
+            dedicated += g
+        else:
+            singles += 1
+    return dedicated + (1 if singles else 0)
+
+
+def time_batch(doms, cells_per_cta: float, steps: int, warmup: int, budget: int,
                precision: int = native.PRECISION_FP64, eps_inner: float = 1e-5,
                device: int = 0) -> float:
-    """Device milliseconds of `steps` batch steps of the decks' domains, or None
-    when the mix does not fit the batch (memory budget or CG CTA capacity)."""
+    """Device milliseconds of `steps` batch steps of the domains (set to the
+    given precision; their state advances), or None when the mix does not fit
+    the batch (memory budget or CG CTA capacity)."""
     import torch
-    doms = [native.domain_from_deck(dk, device=device, precision=precision, eps_inner=eps_inner)
-            for dk in decks]
+    if precision != native.PRECISION_FP64:
+        for g in doms:
+            g.set_precision(precision, eps_inner)
     b = native.Batch(budget, cells_per_cta, device)
     try:
         for g in doms:
@@ -46,21 +66,30 @@ def time_batch(decks, cells_per_cta: float, steps: int, warmup: int, budget: int
         for sl in list(b.members):
             b.release(sl)
         b.close()
-        for g in doms:
-            g.close()
 
 
 def tune(decks, budget: int, precision: int = native.PRECISION_FP64, steps: int = 4,
          warmup: int = 2, cells_candidates=CELLS_PER_CTA, eps_candidates=EPS_INNER,
          device: int = 0) -> dict:
-    """The fastest (cells_per_cta, eps_inner) on this mix, and every timing."""
+    """The fastest (cells_per_cta, eps_inner) on this mix, and every timing.
+    Granularities whose CG would need more co-resident CTAs than the device
+    holds are skipped before any domain is built; the domains are built once
+    and stepped by every candidate in turn."""
     eps_list = eps_candidates if precision == native.PRECISION_MIXED else (1e-5,)
+    capacity = native.Batch.capacity(device)
+    sizes = [(dk.nx, dk.ny) for dk in decks]
+    fits = [c for c in cells_candidates if ctas_needed(sizes, c, capacity) <= capacity]
     results = []
-    for cpc, ein in itertools.product(cells_candidates, eps_list):
-        ms = time_batch(decks, cpc, steps, warmup, budget, precision, ein, device)
-        if ms is None:  # the mix does not fit with this granularity
-            continue
-        results.append({"cells_per_cta": cpc, "eps_inner": ein, "ms_per_step": ms / steps})
+    doms = [native.domain_from_deck(dk, device=device) for dk in decks] if fits else []
+    try:
+        for cpc, ein in itertools.product(fits, eps_list):
+            ms = time_batch(doms, cpc, steps, warmup, budget, precision, ein, device)
+            if ms is None:  # the mix does not fit with this granularity
+                continue
+            results.append({"cells_per_cta": cpc, "eps_inner": ein, "ms_per_step": ms / steps})
+    finally:
+        for g in doms:
+            g.close()
     if not results:
         raise RuntimeError("no candidate packing fits the mix")
     best = min(results, key=lambda r: r["ms_per_step"])

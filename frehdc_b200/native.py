@@ -433,7 +433,25 @@ def _declare_batch(L: C.CDLL) -> None:
     L.frehd_batch_info.argtypes = [_vp, C.POINTER(BatchInfo)]
     L.frehd_batch_stream.argtypes = [_vp, C.POINTER(_vp)]
     L.frehd_batch_set_graph.argtypes = [_vp, C.c_int]
+    L.frehd_server_create.argtypes = [C.c_int, C.c_longlong, C.c_double, C.POINTER(_vp)]
+    L.frehd_server_submit.argtypes = [_vp, _vp, C.c_int, C.c_int, C.POINTER(C.c_longlong)]
+    L.frehd_server_poll.argtypes = [_vp, C.POINTER(ServerDone), C.c_int, C.c_int, _ip]
+    L.frehd_server_info.argtypes = [_vp, C.POINTER(ServerInfo)]
+    L.frehd_server_destroy.argtypes = [_vp]
     L._batch_declared = True
+
+
+class ServerDone(C.Structure):
+    """Mirror of frehd_server_done."""
+    _fields_ = [("ticket", C.c_longlong), ("domain", _vp), ("status", C.c_int), ("steps", C.c_int),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double)]
+
+
+class ServerInfo(C.Structure):
+    """Mirror of frehd_server_info_t."""
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("waiting", C.c_int),
+                ("active", C.c_int), ("max_active", C.c_int), ("batch_steps", C.c_longlong),
+                ("cell_steps", C.c_longlong), ("clock", C.c_double), ("status", C.c_int)]
 
 
 def footprint(cfg: dict, r: int) -> int:
@@ -514,6 +532,61 @@ class Batch:
             lib().frehd_batch_destroy(self.h)
             self.h = None
             self.members.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """frehd_server_*: a native continuous-batching loop on its own host thread.
+    Submitted domains stay owned by the caller (and by this object's table
+    until polled back)."""
+
+    def __init__(self, budget_bytes: int, cells_per_cta: float, device: int = 0):
+        L = lib()
+        _declare_batch(L)
+        h = _vp()
+        check(L.frehd_server_create(device, int(budget_bytes), float(cells_per_cta), C.byref(h)),
+              "frehd_server_create")
+        self.h = h
+        self.held: dict[int, "Domain"] = {}
+
+    def submit(self, dom: "Domain", nsteps: int, t0: int = 1) -> int:
+        t = C.c_longlong()
+        check(lib().frehd_server_submit(self.h, dom.h, t0, nsteps, C.byref(t)), "frehd_server_submit")
+        self.held[t.value] = dom
+        return t.value
+
+    def poll(self, timeout_ms: int = 0, cap: int = 64) -> list:
+        """Completed requests: dicts with ticket, domain (the Domain object),
+        status, steps and the server-clock times."""
+        arr = (ServerDone * cap)()
+        n = C.c_int()
+        check(lib().frehd_server_poll(self.h, arr, cap, int(timeout_ms), C.byref(n)),
+              "frehd_server_poll")
+        out = []
+        for k in range(n.value):
+            r = {f: getattr(arr[k], f) for f, _ in ServerDone._fields_}
+            r["domain"] = self.held.pop(r["ticket"])
+            out.append(r)
+        return out
+
+    def info(self) -> dict:
+        i = ServerInfo()
+        check(lib().frehd_server_info(self.h, C.byref(i)), "frehd_server_info")
+        return {n: getattr(i, n) for n, _ in ServerInfo._fields_}
+
+    def clock(self) -> float:
+        return self.info()["clock"]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().frehd_server_destroy(self.h)
+            self.h = None
+            self.held.clear()
 
     def __del__(self):
         try:

@@ -405,6 +405,47 @@ int frehd_batch_stream(frehd_batch *b, void **stream);
 /* Replay steps from a captured CUDA graph (default 1) or launch them directly. */
 int frehd_batch_set_graph(frehd_batch *b, int on);
 
+/* ------------------------------------------------------------ serving */
+/*
+ * Continuous batching (the served form; the reference's driver loop, FREHD.c,
+ * runs one domain to the end instead).  A server owns a batch and one host
+ * thread that steps it while it holds domains.  Callers prepare each domain on
+ * their own thread (create, geometry, series, init), then submit it for nsteps
+ * steps from tt = t0.  Between two batch steps the thread admits waiting
+ * domains in submission order while the memory budget and the CG's CTA
+ * capacity allow, and releases each domain that has run its steps; poll
+ * returns them (the domain's state and statistics are readable again).  A
+ * domain that cannot fit even an empty batch completes with FREHD_ERR_NOMEM.
+ * The caller keeps ownership of every domain and must not touch one between
+ * its submit and the poll that returns it.  Times are seconds on the server's
+ * monotonic clock (frehd_server_info_t.clock is "now").
+ */
+typedef struct frehd_server frehd_server;
+typedef struct frehd_server_done {
+  long long ticket;          /* from frehd_server_submit */
+  frehd_domain *domain;
+  int status;                /* FREHD_OK, or the step's or admission's error */
+  int steps;                 /* steps the domain ran */
+  double t_submit, t_admit, t_done;  /* t_admit < 0: never admitted */
+} frehd_server_done;
+typedef struct frehd_server_info_t {
+  long long submitted, completed;
+  int waiting, active, max_active;
+  long long batch_steps, cell_steps;
+  double clock;              /* the server's clock now */
+  int status;                /* FREHD_OK, or the error that stopped the server */
+} frehd_server_info_t;
+
+int frehd_server_create(int device, long long hbm_budget_bytes, double cells_per_cta,
+                        frehd_server **out);
+int frehd_server_submit(frehd_server *s, frehd_domain *d, int t0, int nsteps, long long *ticket);
+/* Up to cap completed requests into out (*n of them); waits up to timeout_ms
+ * for the first one when none is ready (0: return at once). */
+int frehd_server_poll(frehd_server *s, frehd_server_done *out, int cap, int timeout_ms, int *n);
+int frehd_server_info(frehd_server *s, frehd_server_info_t *out);
+/* Stop the thread; domains still held go back to their owners unfinished. */
+int frehd_server_destroy(frehd_server *s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -83,3 +83,10 @@ def test_config_mirror_matches_the_c_struct(tmp_path):
                                           check=True).stdout.split()]
     assert out[0] == C.sizeof(native.Config)
     assert out[1:] == [getattr(native.Config, n).offset for n in fields]
+
+
+def test_server_create_fails_loudly_without_a_device():
+    if native.device_count() > 0:
+        pytest.skip("a CUDA device is visible")
+    with pytest.raises(native.FrehdError):
+        native.Server(1 << 30, 65536.0)

@@ -101,3 +101,41 @@ def test_served_results_equal_alone(scratch):
     for k, n in enumerate(names):
         alone, _ = _run_batch([n], steps[n], scratch, cells_per_cta=1e9)
         assert mismatches(results[k], alone[n][0], FIELDS) == [], n
+
+
+def test_server_waits_for_room_and_refuses_what_never_fits(scratch):
+    """The native server admits a request only when the budget has room (with
+    room for one domain at a time they run one after another, each with its
+    single-domain result) and completes a request larger than the whole budget
+    with FREHD_ERR_NOMEM without running it."""
+    names = ["wet48x40", "dry40x36", "dry37x29"]
+    decks = {n: deck_for(n, str(scratch))[0] for n in names}
+    need = max(native.footprint(native.domain_from_deck(d).cfg, d.r) for d in decks.values())
+    srv = native.Server(int(1.2 * need), 1e9)
+    doms = {n: native.domain_from_deck(d) for n, d in decks.items()}
+    tickets = {srv.submit(g, 6): n for n, g in doms.items()}
+    big_deck = deck_for("tvd44x36", str(scratch))[0]
+    big = native.domain_from_deck(big_deck)
+    small_srv = native.Server(native.footprint(big.cfg, big_deck.r) // 2, 1e9)
+    t_big = small_srv.submit(big, 3)
+    got = []
+    while len(got) < len(names):
+        got += srv.poll(timeout_ms=200)
+    assert srv.info()["max_active"] == 1
+    for r in got:
+        n = tickets[r["ticket"]]
+        assert r["status"] == 0 and r["steps"] == 6 and r["t_admit"] >= r["t_submit"]
+        alone, _ = _run_batch([n], 6, scratch, cells_per_cta=1e9)
+        assert mismatches(r["domain"].download(FIELDS), alone[n][0], FIELDS) == [], n
+    # admitted one after another: each waited for the previous one's release
+    order = sorted(got, key=lambda r: r["t_admit"])
+    for a, b in zip(order, order[1:]):
+        assert b["t_admit"] >= a["t_done"] - 1e-3
+    refused = []
+    while not refused:
+        refused = small_srv.poll(timeout_ms=200)
+    assert refused[0]["ticket"] == t_big and refused[0]["status"] == 4
+    assert refused[0]["steps"] == 0 and refused[0]["t_admit"] < 0
+    assert big.run(1, 2) == 0  # handed back untouched, usable alone
+    srv.close()
+    small_srv.close()

@@ -13,8 +13,9 @@ Printed JSON line (rank 0):
                and initialisation, K steps each returning its monitorCFL
                statistics to the host, final state download
   roofline     the CG kernel (the dominant one): algorithmic bytes per launch
-               (48 B/cell set-up + 72 B/cell per iteration) over its mean
-               event-timed launch duration, against the measured HBM copy peak
+               (cg_bytes_per_cell: 48 B/cell set-up + 72 B/cell per iteration)
+               over its mean event-timed launch duration, against the measured
+               HBM copy peak
   cpu_baseline the reference program itself (oracle/_ref, one core) on a
                256 x 256 window of the same deck
 With --gpus N (torchrun) every rank steps its own replica domain (the step does
@@ -361,21 +362,31 @@ def run_e2e(args, deck, cfg, tide, dev, ws, N):
             "final_state_d2h_bytes": sum(a.nbytes for a in out.values())}
 
 
+def cg_bytes_per_cell(iters: float, fp64: bool = True) -> float:
+    """Compulsory DRAM bytes per cell of one single-sweep solve of `iters`
+    iterations: set-up 48 B, then per iteration read r~, p, Hx, Hy, x~ and |Ct|
+    and write r~, p and x~ (72 B in FP64; the FP32 inner iteration of the mixed
+    form moves r~, p, d~, Hx, Hy in FP32, 32 B)."""
+    return 48.0 + (72.0 if fp64 else 32.0) * iters
+
+
 def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk, errors=None):
     N = n * n
     peak, peak_kind = measured_hbm_peak()
     cg_launch_ms = kt["cg_ms"] / kt["steps"]
-    per_it = 72.0 if args.precision == "fp64" else 32.0
-    cg_bytes = N * (48.0 + per_it * iters)
+    fp64 = args.precision == "fp64"
+    cg_cell = cg_bytes_per_cell(iters, fp64)
+    cg_bytes = N * cg_cell
     achieved = cg_bytes / (cg_launch_ms / 1e3) / 1e9
     kname = {"single_sweep": "k_cg1 (persistent single-sweep Jacobi-PCG, one launch per step)",
              "two_phase": "k_cg (persistent two-phase Jacobi-PCG, one launch per step)"}
     roof = {"kernel": kname[args.cg_schedule], "bound": "hbm",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_kind": peak_kind, "traffic": None,
-            "bytes_model": ("48 B/cell set-up + 72 B/cell per CG iteration" if per_it == 72.0 else
+            "bytes_model": ("48 B/cell set-up + 72 B/cell per CG iteration" if fp64 else
                             "48 B/cell set-up + 32 B/cell per FP32 inner iteration (FP64 "
                             "refinement sweeps not counted)"),
+            "bytes_per_cell": cg_cell,
             "cg_iters_per_step": iters, "launch_ms": cg_launch_ms}
     # DRAM traffic of one launch from the committed ncu summary (scaled from a
     # smaller capture; it describes the 4096^2 single-sweep solve only)
@@ -386,7 +397,9 @@ def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk, erro
         if m:
             roof["traffic"] = float(m.group(1))
             roof["traffic_source"] = "profiles/k_cg1_2048x2048_fp64.md (ncu, scaled by cells x iterations)"
-    step_bytes = N * (456.0 + 72.0 * iters)
+    # the step: explicit + assembly 200 B, post-solve + scalar 208 B per cell, and the solve
+    step_cell = 408.0 + cg_cell
+    step_bytes = N * step_cell
     whole = step_bytes * args.steps / (t_max / 1e3) / 1e9
     cpu = None if args.no_cpu else cpu_baseline_reference(args.cpu_steps, n)
     line = {
@@ -404,7 +417,7 @@ def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk, erro
                    "cg_schedule": args.cg_schedule},
         "e2e": e2e,
         "roofline": roof,
-        "step_roofline": {"bytes_per_cell_step": 456.0 + 72.0 * iters, "achieved": whole,
+        "step_roofline": {"bytes_per_cell_step": step_cell, "achieved": whole,
                           "peak": peak, "unit": "GB/s", "frac": whole / peak},
         "per_kernel_ms_per_step": {k: kt[k] / kt["steps"] for k in
                                    ("explicit_ms", "cg_ms", "update_geo_ms", "update_vel_ms",
@@ -421,14 +434,16 @@ def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk, erro
 
 
 # ---------------------------------------------------------------- batched / served forms
-def mix_specs(n: int, seed: int, smin: int, smax: int, steps: int):
+def mix_specs(n: int, seed: int, smin: int, smax: int, steps: int, scalars=(1, 1)):
     """Seeded mix of basins: sides log-uniform in [smin, smax] (multiples of 8),
     square or 1:4 (fair coin), depth 0.3-8 m, 0-40 % dry at low tide, tide
-    amplitude 0.1-0.5 m, Manning n 0.02-0.04, dt 1 s, dx 10 m, 4x4 subgrid."""
+    amplitude 0.1-0.5 m, Manning n 0.02-0.04, dt 1 s, dx 10 m, 4x4 subgrid;
+    each basin carries a number of scalars uniform in scalars = (lo, hi)."""
     import numpy as np
 
     from frehdc_b200 import deck as D
     rng = np.random.default_rng(seed)
+    n_sc = np.random.default_rng(seed + 1).integers(scalars[0], scalars[1] + 1, size=n)
     out = []
     for k in range(n):
         side = float(np.exp(rng.uniform(np.log(smin), np.log(smax))))
@@ -441,7 +456,8 @@ def mix_specs(n: int, seed: int, smin: int, smax: int, steps: int):
                               depth_min=0.3, depth_max=8.0,
                               dry_frac=float(rng.uniform(0.0, 0.4)) or None,
                               tide_amp=float(rng.uniform(0.1, 0.5)),
-                              manning_n=float(rng.uniform(0.02, 0.04))))
+                              manning_n=float(rng.uniform(0.02, 0.04)),
+                              n_scalars=int(n_sc[k])))
     return out
 
 
@@ -477,7 +493,8 @@ def run_batched_form(args):
     from frehdc_b200 import deck as D
     from frehdc_b200 import native, shard
     ws, rank, dev = _dist_init()
-    specs_all = mix_specs(args.mix, 77, args.mix_min, args.mix_max, args.steps + args.warmup + 5)
+    specs_all = mix_specs(args.mix, 77, args.mix_min, args.mix_max, args.steps + args.warmup + 5,
+                          (args.scalars, args.scalars))
     mine = shard.balance([sp.nx * sp.ny for sp in specs_all], ws)[rank]
     specs = [specs_all[i] for i in mine]
     t0 = time.time()
@@ -536,7 +553,8 @@ def run_batched_form(args):
     errors = None
     if args.precision == "mixed":  # every domain against its FP64 run of the same steps
         import numpy as np
-        worst = {"eta_max_abs_m": 0.0, "u_max_rel": 0.0, "v_max_rel": 0.0, "volume_rel": 0.0}
+        worst = {"eta_max_abs_m": 0.0, "u_max_rel": 0.0, "v_max_rel": 0.0, "volume_rel": 0.0,
+                 "scalar_max_abs": 0.0}
         for g, dk in zip(doms, decks):
             r = native.domain_from_deck(dk, device=dev)
             r.run(1, args.warmup + K)
@@ -547,6 +565,9 @@ def run_batched_form(args):
             for f, key in (("uuXP", "u_max_rel"), ("vvYP", "v_max_rel")):
                 sc = max(float(np.max(np.abs(c[f][:n_]))), 1e-300)
                 worst[key] = max(worst[key], float(np.max(np.abs(a[f][:n_] - c[f][:n_]))) / sc)
+            for s_ in range(1 + len(dk.tracers)):   # S and the tracers
+                worst["scalar_max_abs"] = max(worst["scalar_max_abs"], float(np.max(np.abs(
+                    g.download_scalar(s_)[:n_] - r.download_scalar(s_)[:n_]))))
             va, vc = g.stats()["volume"], r.stats()["volume"]
             worst["volume_rel"] = max(worst["volume_rel"], abs(va - vc) / abs(vc))
             r.close()
@@ -572,7 +593,7 @@ def run_batched_form(args):
                        "workload": f"{len(specs_all)} seeded basins, sides log-uniform "
                                    f"{args.mix_min}-{args.mix_max} (square or 1:4), dx 10 m, "
                                    "dt 1 s, depth 0.3-8 m, 0-40% dry, tide 0.1-0.5 m, "
-                                   "n 0.02-0.04, 4x4 subgrid, 1 scalar",
+                                   f"n 0.02-0.04, 4x4 subgrid, {args.scalars} scalar(s)",
                        "cells": int(total_cells), "cells_per_cta": args.cells_per_cta,
                        "sharding": "by cell count over ranks" if ws > 1 else None,
                        "deck_gen_s": round(max(p["gen_s"] for p in parts), 1)},
@@ -606,7 +627,7 @@ def run_served_form(args):
     from frehdc_b200 import native, serve, shard
     ws, rank, dev = _dist_init()
     rng = np.random.default_rng(5)
-    specs = mix_specs(args.requests, 91, args.mix_min, args.mix_max, 10)
+    specs = mix_specs(args.requests, 91, args.mix_min, args.mix_max, 10, (1, args.scalars_max))
     steps = rng.integers(args.req_steps_min, args.req_steps_max + 1, size=len(specs))
     arr = serve.poisson_arrivals(len(specs), args.rate, 17)
     owner = shard.assign_stream(arr, [sp.nx * sp.ny * int(k) for sp, k in zip(specs, steps)], ws)
@@ -638,7 +659,8 @@ def run_served_form(args):
             "p50_latency_s": merged["p50_s"], "p99_latency_s": merged["p99_s"],
             "config": {"workload": f"{len(specs)} requests, Poisson arrivals {args.rate}/s, sides "
                                    f"log-uniform {args.mix_min}-{args.mix_max}, steps "
-                                   f"{args.req_steps_min}-{args.req_steps_max}, 1 scalar, {args.precision}",
+                                   f"{args.req_steps_min}-{args.req_steps_max}, 1-{args.scalars_max} scalars, "
+                                   f"{args.precision}",
                        "cells_per_cta": args.cells_per_cta,
                        "sharding": "least assigned work, arrival order" if ws > 1 else None,
                        "deck_gen_s": round(max(p["gen_s"] for p in parts), 1)},
@@ -673,6 +695,9 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: FP32 inner CG iterations inside FP64 iterative refinement")
     ap.add_argument("--eps-inner", type=float, default=1e-5)
+    ap.add_argument("--scalars", type=int, default=2, help="batched form: scalars per basin")
+    ap.add_argument("--scalars-max", type=int, default=3,
+                    help="served form: scalars per request uniform in 1..this")
     ap.add_argument("--requests", type=int, default=120)
     ap.add_argument("--rate", type=float, default=50.0)
     ap.add_argument("--req-steps-min", type=int, default=50)

@@ -152,6 +152,46 @@ def test_solve_matches_oracle(name, schedule, scratch):
         o.update(tt, o.get("x"))
 
 
+def _true_residual(sysm: dict, x_t: np.ndarray, nx: int, ny: int) -> float:
+    """||z - A x|| / ||z|| of the assembled 5-point system (setupMatrix,
+    nsfunctions.c:927-1001: row entries -GnXM, -GnYM, GnCt, -GnYP, -GnXP; z and x
+    in the transposed order k = i*ny + j, the coefficients row-major)."""
+    def rm(v):  # transposed -> row-major (ny, nx)
+        return v.reshape(nx, ny).T
+    x = rm(x_t)
+    z = rm(sysm["z"])
+    c = {n: sysm[n].reshape(ny, nx) for n in ("GnCt", "GnXP", "GnXM", "GnYP", "GnYM")}
+    ax = c["GnCt"] * x
+    ax[:, :-1] -= c["GnXP"][:, :-1] * x[:, 1:]
+    ax[:, 1:] -= c["GnXM"][:, 1:] * x[:, :-1]
+    ax[:-1, :] -= c["GnYP"][:-1, :] * x[1:, :]
+    ax[1:, :] -= c["GnYM"][1:, :] * x[:-1, :]
+    return float(np.linalg.norm(z - ax) / np.linalg.norm(z))
+
+
+def test_true_residual_of_the_solution(scratch):
+    """The device's x meets the stopping rule on the true residual z - A x of the
+    assembled system, not only on the residual the CG recurrence carries (the
+    scaled solve updates x~ apart from r~), over several stopping tolerances and
+    iteration counts of both parities."""
+    parities = set()
+    for name in ("dry40x36", "tvdwet44x36"):
+        for eps in (1e-12, 3e-12, 1e-11, 3e-11):
+            d = D.make_deck(SPECS[name].replace(eps=eps))
+            g = native.domain_from_deck(d, geometry="fine")
+            for tt in range(1, 9):
+                g.phase(native.PHASE_EXPLICIT, tt)
+                g.phase(native.PHASE_SOLVE, tt)
+                res = _true_residual(g.system(), g.solution(), d.nx, d.ny)
+                g.phase(native.PHASE_UPDATE, tt)
+                st = g.stats()
+                if st["cg_fallback"]:
+                    continue
+                assert res < 2 * eps, (name, eps, tt, res, st["cg_iters"])
+                parities.add(st["cg_iters"] % 2)
+    assert parities == {0, 1}
+
+
 @pytest.mark.parametrize("schedule", list(SCHEDULES))
 @pytest.mark.parametrize("name", ["wet48x40", "dry40x36", "dry37x29", "tvdwet44x36",
                                   "inflow36x30", "wind40x32"])

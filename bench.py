@@ -664,7 +664,8 @@ def run_served_form(args):
                        "cells_per_cta": args.cells_per_cta,
                        "sharding": "least assigned work, arrival order" if ws > 1 else None,
                        "deck_gen_s": round(max(p["gen_s"] for p in parts), 1)},
-            "serving": merged, "clocks": parts[0]["clocks"]}
+            "serving": merged, "clocks": parts[0]["clocks"],
+            "gpu_launches": 5 * sum(int(p.get("batch_steps", 0)) for p in parts)}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -831,15 +831,17 @@ __global__ void __launch_bounds__(kCgThreads, kCg1MinBlocks)
 
 namespace {
 
+// Looked up once; the initialisation of a function-local static is thread-safe,
+// so domains may be set up on several host threads (the server's callers).
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  if (!fn) {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
     void *f = nullptr;
     cudaDriverEntryPointQueryResult q{};
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
-  }
+      return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    return (PFN_cuTensorMapEncodeTiled_v12000) nullptr;
+  }();
   return fn;
 }
 

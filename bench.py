@@ -686,7 +686,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=4096)
-    ap.add_argument("--cpu-steps", type=int, default=60)
+    ap.add_argument("--cpu-steps", type=int, default=300,
+                    help="steps of the reference program on one core for cpu_baseline (about 13 s)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU reference baseline")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end C-ABI leg")
     ap.add_argument("--cg-schedule", default="single_sweep", choices=list(SCHEDULES),

@@ -7,6 +7,7 @@ only in the initial S end with the same surface, velocities and volumes, bit
 for bit.  The generated tracer fields are different plumes inside [0, 1].
 """
 import numpy as np
+import pytest
 
 from frehdc_b200 import deck as D
 from oracle import port
@@ -25,9 +26,12 @@ def test_tracer_fields_are_distinct_plumes():
     assert D.make_deck(D.DeckSpec(nx=24, ny=20, steps=3, seed=4)).tracers == []
 
 
-def test_hydrodynamics_do_not_read_the_scalar():
-    deck = D.make_deck(D.DeckSpec(nx=20, ny=16, steps=8, seed=6, dry_frac=0.3, n_scalars=2),
-                       with_tables=True)
+@pytest.mark.parametrize("extra", [dict(), dict(scalar_adv=2),
+                                   dict(inflow_cells=(3, 5, 2, 4), inflow_q=2.0, inflow_s=30.0)],
+                         ids=["upwind", "tvd", "inflow"])
+def test_hydrodynamics_do_not_read_the_scalar(extra):
+    deck = D.make_deck(D.DeckSpec(nx=20, ny=16, steps=8, seed=6, dry_frac=0.3, n_scalars=2,
+                                  **extra), with_tables=True)
     runs = []
     for field in (deck.S0, deck.tracers[0]):
         o = port.from_deck(D.with_scalar(deck, field), precond=port.PRECOND_JACOBI,

@@ -90,6 +90,10 @@ struct frehd_batch {
   DevArray<CgJob> jobs;
   long ntiles = 0;
   int nfin = 0, nctas = 0;
+  // per-slot device status after each step, written by k_finish_batch into
+  // host-mapped pinned memory (read by the server between steps)
+  int *status_host = nullptr, *status_dev = nullptr;
+  int status_cap = 0;
   // captured launches
   int use_graph = 1;
   cudaGraphExec_t graph = nullptr;
@@ -122,6 +126,27 @@ int ctas_needed(const frehd_batch *b, const frehd_domain *extra) {
   return dedicated + (singles ? 1 : 0);
 }
 
+// Room for `n` slot statuses; growing waits for the queued steps, which may
+// still write the old array.
+int reserve_status(frehd_batch *b, int n) {
+  if (n <= b->status_cap) return FREHD_OK;
+  const int cap = std::max(n, std::max(64, 2 * b->status_cap));
+  BATCH_TRY(cudaStreamSynchronize(b->stream));
+  int *h = nullptr, *dv = nullptr;
+  if (cudaHostAlloc(&h, sizeof(int) * cap, cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer(&dv, h, 0) != cudaSuccess) {
+    cudaGetLastError();
+    if (h) cudaFreeHost(h);
+    return fail(FREHD_ERR_NOMEM, "batch status array: %d slots", cap);
+  }
+  for (int k = 0; k < cap; ++k) h[k] = k < b->status_cap ? b->status_host[k] : FREHD_OK;
+  if (b->status_host) cudaFreeHost(b->status_host);
+  b->status_host = h;
+  b->status_dev = dv;
+  b->status_cap = cap;
+  return FREHD_OK;
+}
+
 void drop_graph(frehd_batch *b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   b->graph = nullptr;
@@ -144,6 +169,10 @@ int launch_step(frehd_batch *b) {
 int rebuild(frehd_batch *b) {
   drop_graph(b);
   const int nslot = (int)b->slots.size();
+  {
+    const int rc = reserve_status(b, nslot);
+    if (rc) return rc;
+  }
   std::vector<View> views(2 * (size_t)std::max(nslot, 1));
   std::vector<const Cg1Maps *> maps(std::max(nslot, 1), nullptr);
   std::vector<BatchTile> tiles;
@@ -162,14 +191,18 @@ int rebuild(frehd_batch *b) {
     const int gx = (d->gr.nx + 31) / 32, gy = (d->gr.ny + 7) / 8;
     for (int by = 0; by < gy; ++by)
       for (int bx = 0; bx < gx; ++bx) tiles.push_back(BatchTile{s, bx, by, gx});
-    fins.push_back(FinishJob{s, gx * gy, d->out});
+    fins.push_back(FinishJob{s, gx * gy, d->out, b->status_dev + s});
     doms.push_back(Dom{s, group_size(b, d), (double)d->gr.nx * d->gr.ny});
   }
-  b->ntiles = (long)tiles.size();
-  b->nfin = (int)fins.size();
+  // the launch sizes describe the device tables: they stay zero (no launch) and
+  // the batch stays dirty until every table of this composition is uploaded
+  b->ntiles = 0;
+  b->nfin = 0;
   b->nctas = 0;
-  b->dirty = false;
-  if (doms.empty()) return FREHD_OK;
+  if (doms.empty()) {
+    b->dirty = false;
+    return FREHD_OK;
+  }
 
   // CTA packing: multi-CTA groups on CTAs of their own, then single-CTA domains
   // longest first onto the least loaded remaining CTA.
@@ -210,7 +243,6 @@ int rebuild(frehd_batch *b) {
     jobs.insert(jobs.end(), per_cta[c].begin(), per_cta[c].end());
   }
   start[per_cta.size()] = (int)jobs.size();
-  b->nctas = (int)per_cta.size();
 
   int rc = 0;
   rc = rc ? rc : b->views2.reserve(views.size());
@@ -228,6 +260,10 @@ int rebuild(frehd_batch *b) {
   BATCH_TRY(cudaMemcpyAsync(b->jobs.p, jobs.data(), sizeof(CgJob) * jobs.size(), cudaMemcpyHostToDevice, b->stream));
   // the host vectors go out of scope: the copies must have left them
   BATCH_TRY(cudaStreamSynchronize(b->stream));
+  b->ntiles = (long)tiles.size();
+  b->nfin = (int)fins.size();
+  b->nctas = (int)per_cta.size();
+  b->dirty = false;
   return FREHD_OK;
 }
 
@@ -261,6 +297,11 @@ void capture(frehd_batch *b) {
 }
 
 }  // namespace
+
+int frehd::batch_slot_status(const frehd_batch *b, int slot) {
+  if (!b || slot < 0 || slot >= b->status_cap) return FREHD_OK;
+  return *(volatile int *)&b->status_host[slot];
+}
 
 extern "C" int frehd_domain_footprint(const frehd_config *cfg, int r, long long *bytes) {
   if (!cfg || !bytes || r < 1 || cfg->nx < 2 || cfg->ny < 2) return fail(FREHD_ERR_INVALID, "bad argument");
@@ -313,6 +354,7 @@ extern "C" int frehd_batch_destroy(frehd_batch *b) {
       s.d->in_batch = 0;
     }
   drop_graph(b);
+  if (b->status_host) cudaFreeHost(b->status_host);
   b->views2.release();
   b->maps.release();
   b->tiles.release();
@@ -353,6 +395,8 @@ extern "C" int frehd_batch_admit(frehd_batch *b, frehd_domain *d, int t0, int *s
   }
   b->slots[s].d = d;
   b->slots[s].steps = 0;
+  // the slot's previous occupant was released after its steps ended
+  if (s < b->status_cap) b->status_host[s] = FREHD_OK;
   b->used += d->bytes;
   d->in_batch = 1;
   b->dirty = true;

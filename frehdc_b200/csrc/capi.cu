@@ -111,6 +111,26 @@ dim3 tile_grid(const frehd_domain *d) {
 
 __global__ void k_set_tt(Scratch *sc, int tt) { sc->tt = tt; }
 
+// A new state clears what a stopped step left behind: the device status (after
+// CFL > 20 or a wait that gave up), a half-counted grid barrier, the per-step
+// counters and the failure-path test settings.
+__global__ void k_reset_scratch(Scratch *sc) {
+  sc->status = FREHD_OK;
+  sc->bar_count = 0;
+  sc->n_fix = 0;
+  sc->n_cfl_warn = 0;
+  sc->max_cflx_bits = 0;
+  sc->max_cfly_bits = 0;
+  sc->cg_noconv = 0;
+  sc->skip_barrier_rank1 = 0;
+  sc->wait_limit_ns = 0;
+}
+
+__global__ void k_set_wait_test(Scratch *sc, unsigned long long limit_ns, int skip_rank1) {
+  sc->wait_limit_ns = limit_ns;
+  sc->skip_barrier_rank1 = skip_rank1;
+}
+
 // host copies in the reference layout: index helpers (map.c:45-143)
 struct RefMap {
   int nx, ny;
@@ -161,7 +181,14 @@ int read_stats(frehd_domain *d) {
   d->last.max_cfly = o.max_cfly;
   d->last.n_cfl_warn = o.n_cfl_warn;
   d->last.volume = o.volume;
+  d->last.cg_noconverge = o.cg_noconv;
   return FREHD_OK;
+}
+
+long long take_noconv(frehd_domain *d) {
+  const long long n = d->out_host->cg_noconv_steps - d->noconv_seen;
+  d->noconv_seen = d->out_host->cg_noconv_steps;
+  return n;
 }
 
 int launch_cg(frehd_domain *d, const View &w) {
@@ -211,6 +238,7 @@ int launch_update(frehd_domain *d, const View &w, cudaEvent_t *ev = nullptr) {
 
 View frehd::domain_view(const frehd_domain *d, int cur) { return make_view_at(d, cur); }
 int frehd::domain_read_stats(frehd_domain *d) { return read_stats(d); }
+long long frehd::domain_take_noconv(frehd_domain *d) { return take_noconv(d); }
 
 // ---------------------------------------------------------------- lifecycle
 extern "C" int frehd_device_count(int *count) {
@@ -331,6 +359,8 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
 
 extern "C" int frehd_domain_destroy(frehd_domain *d) {
   if (!d) return FREHD_OK;
+  // an admitted domain's arrays are referenced by its batch's tables and graph
+  if (d->in_batch) return fail(FREHD_ERR_STATE, "domain is in a batch: release it first");
   cudaSetDevice(d->device);
   if (d->stream) cudaStreamSynchronize(d->stream);
   for (void *p : d->allocs) cudaFree(p);
@@ -546,6 +576,8 @@ extern "C" int frehd_domain_upload_state(frehd_domain *d, const frehd_state *st)
   CUDA_TRY(cudaSetDevice(d->device));
   const long N = d->N, T = d->T;
   const int c = d->cur;
+  k_reset_scratch<<<1, 1, 0, d->stream>>>(d->sc);
+  CUDA_TRY(cudaGetLastError());
   struct Item {
     const double *h;
     double *dv;
@@ -886,9 +918,26 @@ extern "C" int frehd_domain_run(frehd_domain *d, int t0, int nsteps) {
   // buffer parity from the last completed step
   const int done = d->last.step - t0 + 1;
   if (done != nsteps) d->cur = cur0 ^ (done & 1);
+  const long long noconv = take_noconv(d);
   if (d->last.status == FREHD_ERR_CFL) return fail(FREHD_ERR_CFL, "max CFL > 20 at step %d", d->last.step);
   if (d->last.status != FREHD_OK)
     return fail(d->last.status, "step %d: %s", d->last.step, frehd_status_string(d->last.status));
+  if (noconv > 0)  // reported, not fatal: the steps ran on, as laspack's CGIter does
+    return fail(FREHD_ERR_CG_NOCONVERGE, "CG reached maxIter = %d in %lld of steps %d..%d",
+                d->p.maxIter, noconv, t0, t0 + nsteps - 1);
+  return FREHD_OK;
+}
+
+extern "C" int frehd_domain_set_wait_test(frehd_domain *d, long long wait_limit_ns,
+                                          int skip_barrier_rank) {
+  if (d && d->in_batch) return fail(FREHD_ERR_STATE, "the domain is stepped by a batch (release it first)");
+  if (!d || wait_limit_ns < 0 || skip_barrier_rank < -1)
+    return fail(FREHD_ERR_INVALID, "bad argument");
+  CUDA_TRY(cudaSetDevice(d->device));
+  k_set_wait_test<<<1, 1, 0, d->stream>>>(d->sc, (unsigned long long)wait_limit_ns,
+                                          skip_barrier_rank + 1);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaStreamSynchronize(d->stream));
   return FREHD_OK;
 }
 

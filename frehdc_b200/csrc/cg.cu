@@ -44,6 +44,10 @@ namespace frehd {
 __global__ void __launch_bounds__(kCgThreads, 1) k_cg(View w, int x0_surface, int eliminate) {
   Scratch *sc = w.sc;
   if (*(volatile int *)&sc->status != FREHD_OK) return;
+  if (test_skip_barrier(sc, blockIdx.x)) {  // a lone CTA has no partner whose wait could run out
+    if (gridDim.x == 1 && threadIdx.x == 0) set_status(sc, FREHD_ERR_TIMEOUT);
+    return;
+  }
   const Grid g = w.gr;
   const Params &p = w.p;
   const int nx = g.nx, ny = g.ny;
@@ -62,7 +66,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(View w, int x0_surface, in
   // falling above eps*||b|| and laspack's CGIter runs on to maxIter.  When ||r||
   // has not halved for kStallIters iterations the solve starts again in the
   // eliminated (symmetric positive definite) form, and the step reports it.
-  int it = 0, it_all = 0, fallback = 0;
+  int it = 0, it_all = 0, fallback = 0, noconv = 0;
   double rr = 0.0, bnorm = 0.0;
   for (int attempt = 0;; ++attempt) {
     const int elim = eliminate | (attempt > 0);
@@ -226,12 +230,15 @@ __global__ void __launch_bounds__(kCgThreads, 1) k_cg(View w, int x0_surface, in
       }
     }
     it_all += it;
+    // maxIter reached first: laspack's CGIter stops there silently; the step reports it
+    noconv = !stalled && !converged(rr);
     if (!stalled) break;
     fallback = 1;
   }  // attempt
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     sc->cg_iters = it_all;
     sc->cg_fallback = fallback;
+    sc->cg_noconv = noconv;
     sc->cg_rr = rr;
     sc->cg_bb = bnorm * bnorm;
   }

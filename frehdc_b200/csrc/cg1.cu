@@ -405,7 +405,7 @@ static __device__ __forceinline__ bool cg1_fp64(const View &w, const Cg1Maps *__
   // read by all between grid reductions)
   __shared__ double s_best;
   __shared__ int s_best_it, s_it_all, s_fallback;
-  int it = 0;
+  int it = 0, noconv = 0;
   double rr = 0.0, bnorm = 0.0;
   if (threadIdx.x == 0) {
     s_it_all = 0;
@@ -539,6 +539,8 @@ static __device__ __forceinline__ bool cg1_fp64(const View &w, const Cg1Maps *__
       }
     }
     if (threadIdx.x == 0) s_it_all += it;
+    // maxIter reached first: laspack's CGIter stops there silently; the step reports it
+    noconv = !stalled && !converged(rr);
     if (!stalled) break;
     if (threadIdx.x == 0) s_fallback = 1;
   }  // attempt
@@ -560,6 +562,7 @@ static __device__ __forceinline__ bool cg1_fp64(const View &w, const Cg1Maps *__
   if (rank == 0 && threadIdx.x == 0) {
     sc->cg_iters = s_it_all;
     sc->cg_fallback = s_fallback;
+    sc->cg_noconv = noconv;
     sc->cg_rr = rr;
     sc->cg_bb = bnorm * bnorm;
   }
@@ -722,6 +725,7 @@ static __device__ __forceinline__ int cg1_mixed(const View &w, const Cg1Maps *__
   if (rank == 0 && threadIdx.x == 0) {
     sc->cg_iters = it_all;
     sc->cg_fallback = 0;
+    sc->cg_noconv = 0;
     sc->cg_rr = rr;
     sc->cg_bb = bnorm * bnorm;
   }
@@ -733,6 +737,10 @@ static __device__ __forceinline__ bool cg1_solve(const View &w, const Cg1Maps *_
                                                  int x0_surface, int eliminate, unsigned rank,
                                                  unsigned nb, unsigned char *smem,
                                                  unsigned long long *bars, unsigned &seq) {
+  if (test_skip_barrier(w.sc, rank)) {  // a lone CTA has no partner whose wait could run out
+    if (nb == 1 && threadIdx.x == 0) set_status(w.sc, FREHD_ERR_TIMEOUT);
+    return false;
+  }
   if (w.p.mixed) {
     const int r = cg1_mixed(w, m, x0_surface, eliminate, rank, nb, smem, bars, seq);
     if (r != 2) return r == 1;

@@ -88,9 +88,10 @@ static __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], Scratch *
     }
   } else if (threadIdx.x == 0) {
     volatile unsigned *gen = &sc->bar_gen;
+    const unsigned long long lim = sc->wait_limit_ns ? sc->wait_limit_ns : kBarrierTimeoutNs;
     const unsigned long long t0 = gtimer_ns();
     while (*gen == my_gen) {
-      if (gtimer_ns() - t0 > kBarrierTimeoutNs) {
+      if (gtimer_ns() - t0 > lim) {
         set_status(sc, FREHD_ERR_TIMEOUT);
         s_ok = 0;
         break;
@@ -104,6 +105,14 @@ static __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], Scratch *
 #pragma unroll
   for (int m = 0; m < NV; ++m) v[m] = ld(totals, m);
   return true;
+}
+
+// Failure-path testing (frehd_domain_set_wait_test): true in the one CTA of a
+// solve that is to leave before its first grid barrier without arriving, so that
+// its partners' bounded wait runs out and the solve reports FREHD_ERR_TIMEOUT.
+// Nothing is in flight at that point (no TMA load, no partial sum).
+static __device__ __forceinline__ bool test_skip_barrier(const Scratch *sc, unsigned rank) {
+  return *(const volatile int *)&sc->skip_barrier_rank1 == (int)rank + 1;
 }
 
 struct TileIt {

@@ -90,7 +90,11 @@ struct Scratch {
   unsigned long long max_cflx_bits, max_cfly_bits;  // positive doubles as ordered bits
   double volume;
   long long cg_iters_total;  // running sum over completed steps
-  double pad1[2];
+  int cg_noconv;             // 1: the last solve stopped at maxIter with ||r|| >= eps*||b||
+  int skip_barrier_rank1;    // failure-path testing: 1 + the rank of the CTA that leaves the
+                             // next solve's first grid barrier without arriving (0: none)
+  long long cg_noconv_steps; // running count of completed steps whose solve stopped at maxIter
+  unsigned long long wait_limit_ns;  // bound of the grid-barrier waits (0: kBarrierTimeoutNs)
 };
 
 // Device pointers of the state and work arrays for one step.  `cur`/`nxt`

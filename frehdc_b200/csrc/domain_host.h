@@ -67,6 +67,7 @@ struct frehd_domain {
   std::vector<cudaEvent_t> ev;
   frehd_kernel_times times{};
   long long iters_at_prof_start = 0;
+  long long noconv_seen = 0;  // steps stopped at maxIter already reported to the caller
 };
 
 namespace frehd {
@@ -74,6 +75,17 @@ namespace frehd {
 View domain_view(const frehd_domain *d, int cur);
 // Read the last step's statistics (StepOut) into d->last; synchronises d->stream.
 int domain_read_stats(frehd_domain *d);
+// Steps whose solve stopped at maxIter since the last call (from the statistics
+// last read); the count is then marked as reported.
+long long domain_take_noconv(frehd_domain *d);
+}  // namespace frehd
+
+struct frehd_batch;
+namespace frehd {
+// Device status of the domain in `slot` after the latest completed batch step
+// (FREHD_OK while it steps normally); valid once the caller has waited for
+// that step.
+int batch_slot_status(const frehd_batch *b, int slot);
 }  // namespace frehd
 
 #endif

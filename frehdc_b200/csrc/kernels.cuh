@@ -11,6 +11,8 @@ struct StepOut {
   int step, cg_iters, status, n_cfl_warn, n_fix, cg_fallback;
   double cg_rr, cg_bb, max_cflx, max_cfly, volume;
   long long cg_iters_total;
+  int cg_noconv, pad;
+  long long cg_noconv_steps;  // running count of steps whose solve stopped at maxIter
 };
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -45,6 +47,7 @@ struct BatchTile {
 struct FinishJob {
   int d, nblocks_vel;  // domain slot, its k_update_vel tile count
   StepOut *out;
+  int *status;         // the domain's device status after the step, in host-mapped memory
 };
 __global__ void k_explicit_batch(const View *views2, const BatchTile *tiles);
 __global__ void k_update_geo_batch(const View *views2, const BatchTile *tiles);

@@ -13,6 +13,13 @@
 // are in flight on the device, so a domain admitted now joins within two steps
 // instead of behind a long queue of launches.
 //
+// A domain whose step fails on the device (CFL > 20, where the reference
+// exits, nsfunctions.c:1225-1231; a device wait that gave up) is evicted as
+// soon as the server has waited for that step: it completes with the failure
+// status and the steps it ran, and its slot and memory go to waiting requests
+// at once.  A domain whose solves stopped at maxIter completes normally with
+// FREHD_ERR_CG_NOCONVERGE as a warning.
+//
 // A domain's result does not depend on what shares the batch with it (the
 // batch's guarantee), so the server only changes when results arrive.  The
 // caller owns every domain throughout: the server neither creates nor
@@ -71,13 +78,13 @@ struct frehd_server {
 
 namespace {
 
-void finish(frehd_server *s, const Req &r, int status) {
+void finish(frehd_server *s, const Req &r, int status, int steps) {
   frehd_server_done o;
   std::memset(&o, 0, sizeof(o));
   o.ticket = r.ticket;
   o.domain = r.d;
   o.status = status;
-  o.steps = r.taken;
+  o.steps = steps;
   o.t_submit = r.submitted;
   o.t_admit = r.admitted;
   o.t_done = s->now();
@@ -93,10 +100,10 @@ void fail_all(frehd_server *s, int rc) {
   std::snprintf(s->fatal_msg, sizeof(s->fatal_msg), "%s", frehd_last_error());
   for (auto &kv : s->active) {
     frehd_batch_release(s->batch, kv.first, nullptr);
-    finish(s, kv.second, rc);
+    finish(s, kv.second, rc, kv.second.taken);
   }
   s->active.clear();
-  for (const Req &r : s->waiting) finish(s, r, rc);
+  for (const Req &r : s->waiting) finish(s, r, rc, 0);
   s->waiting.clear();
   s->stop = true;
   s->cv_done.notify_all();
@@ -120,7 +127,7 @@ void loop(frehd_server *s) {
         const int rc = frehd_batch_admit(s->batch, r.d, r.t0, &slot);
         if (rc == FREHD_ERR_NOMEM && !s->active.empty()) break;  // wait for room
         if (rc != FREHD_OK) {  // cannot fit even an empty batch, or a bad domain
-          finish(s, r, rc);
+          finish(s, r, rc, 0);
           s->waiting.pop_front();
           s->cv_done.notify_all();
           continue;
@@ -135,9 +142,34 @@ void loop(frehd_server *s) {
     }
     // one step of every admitted domain; at most kInFlight steps queued
     cudaEvent_t &e = s->ev[issued % kInFlight];
-    if (issued >= kInFlight && cudaEventSynchronize(e) != cudaSuccess) {
-      fail_all(s, fail(FREHD_ERR_CUDA, "server thread: step event failed"));
-      return;
+    if (issued >= kInFlight) {
+      if (cudaEventSynchronize(e) != cudaSuccess) {
+        fail_all(s, fail(FREHD_ERR_CUDA, "server thread: step event failed"));
+        return;
+      }
+      // evict the domains whose step failed on the device; their later queued
+      // steps are skipped on the device, and the release waits for them
+      std::lock_guard<std::mutex> lk(s->mu);
+      bool any = false;
+      for (auto it = s->active.begin(); it != s->active.end();) {
+        const int st = batch_slot_status(s->batch, it->first);
+        if (st == FREHD_OK) {
+          ++it;
+          continue;
+        }
+        Req &r = it->second;
+        frehd_domain *d = nullptr;
+        const int rr = frehd_batch_release(s->batch, it->first, &d);
+        // the failing step is the last one the domain completed or began
+        const int ran = rr ? r.taken : r.d->last.step - r.t0 + 1;
+        s->cell_steps -= (long long)(r.taken - ran) * r.d->gr.nx * r.d->gr.ny;
+        finish(s, r, rr ? rr : st, ran);
+        any = true;
+        it = s->active.erase(it);
+      }
+      if (any) s->cv_done.notify_all();
+      if (any && s->active.empty()) continue;  // nothing left to step: admit first
+
     }
     int rc = frehd_batch_step(s->batch);
     void *stream = nullptr;
@@ -163,7 +195,9 @@ void loop(frehd_server *s) {
       // release waits for the queued steps; the domain's last status comes with it
       frehd_domain *d = nullptr;
       const int rr = frehd_batch_release(s->batch, it->first, &d);
-      finish(s, r, rr ? rr : r.d->last.status);
+      int st = rr ? rr : r.d->last.status;
+      if (st == FREHD_OK && domain_take_noconv(r.d) > 0) st = FREHD_ERR_CG_NOCONVERGE;
+      finish(s, r, st, rr ? r.taken : r.d->last.step - r.t0 + 1);
       any = true;
       it = s->active.erase(it);
     }

@@ -1033,6 +1033,11 @@ static __device__ __forceinline__ bool finish_block(const View &w, int nblocks_v
     out->n_fix = nfix;
     sc->cg_iters_total += sc->cg_iters;
     out->cg_iters_total = sc->cg_iters_total;
+    // a solve that stopped at maxIter is reported, not fatal (laspack goes on, itersolv.c:399-418)
+    out->cg_noconv = sc->cg_noconv;
+    sc->cg_noconv_steps += sc->cg_noconv;
+    out->cg_noconv_steps = sc->cg_noconv_steps;
+    sc->cg_noconv = 0;
     // monitorCFL's exit condition (nsfunctions.c:1226-1231)
     if (fabs(out->max_cflx) > 20 || fabs(out->max_cfly) > 20) out->status = FREHD_ERR_CFL;
     // reset the per-step counters for the next step
@@ -1101,6 +1106,9 @@ __global__ void k_finish_batch(const View *views2, const FinishJob *jobs) {
   stage_view(views2, f.d, &sv, &s_cur, threadIdx.x, blockDim.x);
   const bool ran = finish_block(sv, f.nblocks_vel, f.out);
   if (ran && threadIdx.x == 0) sv.sc->cur = s_cur ^ 1;
+  // the batch's owner sees a failed domain (CFL > 20, a wait that gave up) after
+  // this step without reading the domain's statistics
+  if (threadIdx.x == 0) *(volatile int *)f.status = *(volatile int *)&sv.sc->status;
 }
 
 // ---------------------------------------------------------------- layout

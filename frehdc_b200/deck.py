@@ -199,7 +199,16 @@ def _fine_noise(seed: int, fj: int, nxf_fine: int, lo: int, hi: int, rough: floa
     return rng.uniform(-rough, rough, size=nxf_fine)[lo:hi]
 
 
-def make_deck(spec: DeckSpec, start: str = DEFAULT_START, with_tables: bool = False) -> Deck:
+def _host(host):
+    """The pre-processing builders (build_bottoms, build_tables): this library's
+    by default; any module with the same two functions may stand in."""
+    if host is None:
+        from . import native as host
+    return host
+
+
+def make_deck(spec: DeckSpec, start: str = DEFAULT_START, with_tables: bool = False,
+              host=None) -> Deck:
     """Generate a deck (fine bottoms, coarse bottoms, initial fields, tide series)."""
     r = spec.r
     if spec.crop is None:
@@ -212,8 +221,7 @@ def make_deck(spec: DeckSpec, start: str = DEFAULT_START, with_tables: bool = Fa
     for fj in range(ny * r):
         zf[fj] += _fine_noise(spec.seed, j0 * r + fj, nxf * r, i0 * r, (i0 + nx) * r, spec.roughness)
     zf = np.ascontiguousarray(zf)
-    from . import native
-    bottom, bxp, byp = native.build_bottoms(zf, nx, ny, r)
+    bottom, bxp, byp = _host(host).build_bottoms(zf, nx, ny, r)
 
     # initial surface: eta0 sine along the basin, scalar plume at the basin centre
     jj, ii = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
@@ -260,16 +268,15 @@ def make_deck(spec: DeckSpec, start: str = DEFAULT_START, with_tables: bool = Fa
                 tide_v=tide_v, Nt=Nt, NT_days=NT_days, offset=offset, inflow_v=inflow_v,
                 wspd_v=wspd_v, wdir_v=wdir_v, tracers=tracers)
     if with_tables:
-        deck.extra["tables"] = build_tables(deck)
+        deck.extra["tables"] = build_tables(deck, host)
     return deck
 
 
-def build_tables(deck: Deck) -> np.ndarray:
+def build_tables(deck: Deck, host=None) -> np.ndarray:
     """(10, Ne, N) subgrid tables of a deck (frehd_build_tables)."""
-    from . import native
-    return native.build_tables(deck.zf, deck.nx, deck.ny, deck.r, deck.spec.dx / deck.r,
-                               deck.spec.dx / deck.r, deck.surfmin, deck.dsurf, deck.Ne,
-                               block_check=deck.spec.block_check)
+    return _host(host).build_tables(deck.zf, deck.nx, deck.ny, deck.r, deck.spec.dx / deck.r,
+                                    deck.spec.dx / deck.r, deck.surfmin, deck.dsurf, deck.Ne,
+                                    block_check=deck.spec.block_check)
 
 
 # --------------------------------------------------------------------------- tide
@@ -402,13 +409,15 @@ DATA_DAT_LABELS = [
 
 
 def write_reference_deck(deck: Deck, path: str, tables: np.ndarray | None = None,
-                         binary_tables: bool = False, out_steps: int | None = None) -> str:
+                         binary_tables: bool = False, out_steps: int | None = None,
+                         host=None) -> str:
     """Write data.dat + input/ for the reference model under ``path``.
 
     binary_tables additionally writes each subgrid table as raw little-endian
     doubles (``<name>.dat.bin``); the oracle harness reads those when present
     instead of parsing hundreds of millions of text values.  out_steps sets the
-    output interval OutItvl in steps (default: beyond the last step).
+    output interval OutItvl in steps (default: beyond the last step).  host:
+    the table builder when the deck carries no tables (see make_deck).
     """
     os.makedirs(os.path.join(path, "input", "subdata"), exist_ok=True)
     os.makedirs(os.path.join(path, "output"), exist_ok=True)
@@ -429,7 +438,7 @@ def write_reference_deck(deck: Deck, path: str, tables: np.ndarray | None = None
     if tables is None:
         tables = deck.extra.get("tables")
         if tables is None:
-            tables = build_tables(deck)
+            tables = build_tables(deck, host)
     names = list(TABLE_NAMES)
     # useminV = 3 makes the reference load the minV* tables (subgrid.c:2186-2204)
     # without using them (subgrid.c:378,409); they repeat the half-cell volumes.

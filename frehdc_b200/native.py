@@ -87,6 +87,7 @@ class StepStats(C.Structure):
         ("step", C.c_int), ("cg_iters", C.c_int), ("status", C.c_int),
         ("cg_rel_residual", C.c_double), ("max_cflx", C.c_double), ("max_cfly", C.c_double),
         ("n_cfl_warn", C.c_int), ("volume", C.c_double), ("cg_fallback", C.c_int),
+        ("cg_noconverge", C.c_int),
     ]
 
 
@@ -180,6 +181,7 @@ def _declare_domain(L: C.CDLL) -> None:
     L.frehd_domain_init_scalar.argtypes = [_vp, C.c_int, _dp]
     L.frehd_domain_step.argtypes = [_vp, C.c_int]
     L.frehd_domain_run.argtypes = [_vp, C.c_int, C.c_int]
+    L.frehd_domain_set_wait_test.argtypes = [_vp, C.c_longlong, C.c_int]
     L.frehd_domain_phase.argtypes = [_vp, C.c_int, C.c_int, _dp]
     L.frehd_domain_download_system.argtypes = [_vp] + [_dp] * 6
     L.frehd_domain_download_solution.argtypes = [_vp, _dp]
@@ -370,17 +372,29 @@ class Domain:
             check(rc, "phase")
         return rc
 
+    # statuses a step returns without raising: FREHD_OK, FREHD_ERR_CG_NOCONVERGE
+    # (a warning: the solve stopped at maxIter) and FREHD_ERR_CFL (the reference
+    # stops there)
+    STEP_STATUSES = (0, 5, 6)
+
     def step(self, tt: int) -> int:
         rc = lib().frehd_domain_step(self.h, tt)
-        if rc not in (0, 6):
+        if rc not in self.STEP_STATUSES:
             check(rc, "step")
         return rc
 
     def run(self, t0: int, nsteps: int) -> int:
         rc = lib().frehd_domain_run(self.h, t0, nsteps)
-        if rc not in (0, 6):
+        if rc not in self.STEP_STATUSES:
             check(rc, "run")
         return rc
+
+    def set_wait_test(self, wait_limit_ns: int, skip_barrier_rank: int = -1):
+        """Failure-path testing (frehd_domain_set_wait_test): bounded grid-barrier
+        waits of wait_limit_ns, and one CTA that skips the next solve's first
+        barrier so that the others' wait runs out."""
+        check(lib().frehd_domain_set_wait_test(self.h, int(wait_limit_ns), int(skip_barrier_rank)),
+              "frehd_domain_set_wait_test")
 
     def stats(self) -> dict:
         s = StepStats()

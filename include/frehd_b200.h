@@ -159,11 +159,16 @@ typedef struct frehd_step_stats {
   int cg_fallback;           /* 1: the solve of the assembled matrix stalled (||r|| did not
                                 halve in 400 iterations) and was redone with decoupled rows
                                 eliminated; laspack would run on to maxIter */
+  int cg_noconverge;         /* 1: the solve stopped at maxIter with ||r|| >= eps*||b|| (laspack's
+                                CGIter stops there silently, itersolv.c:399-418; the step went on
+                                with that solution) */
 } frehd_step_stats;
 
 /* Create an empty domain on CUDA device `device`.  Unsupported Config options
  * give FREHD_ERR_UNSUPPORTED. */
 int frehd_domain_create(const frehd_config *cfg, int device, frehd_domain **out);
+/* Free a domain.  Refused with FREHD_ERR_STATE while the domain is admitted to
+ * a batch (frehd_batch_release hands it back first). */
 int frehd_domain_destroy(frehd_domain *d);
 
 /* Geometry source, one of the two:
@@ -196,7 +201,10 @@ int frehd_domain_set_series(frehd_domain *d, int kind, int n, const double *valu
  * FREHD_SERIES_WIND_DIR update waits for its copy). */
 int frehd_domain_update_series(frehd_domain *d, int kind, int t0, int n, const double *values);
 
-/* Copy state in the reference layout to/from the device (NULL fields skipped). */
+/* Copy state in the reference layout to/from the device (NULL fields skipped).
+ * An upload (and frehd_domain_init, which uploads) also clears the device status
+ * a stopped step left behind (FREHD_ERR_CFL, FREHD_ERR_TIMEOUT): after such a
+ * step the domain refuses further steps until its state is set again. */
 int frehd_domain_upload_state(frehd_domain *d, const frehd_state *st);
 int frehd_domain_download_state(frehd_domain *d, frehd_state *st);
 /* Scalar s (0 .. nscalar-1; 0 is frehd_state.S) in the layout of the reference's
@@ -224,11 +232,27 @@ int frehd_domain_init(frehd_domain *d, const double *bottom, const double *botto
 
 /* One complete step tt (oneCompleteStep, nssolve.c:110-118) followed by
  * monitorCFL (nsfunctions.c:1192-1232).  Returns FREHD_ERR_CFL when the max CFL
- * exceeds 20 (the state is left as the reference leaves it before exiting). */
+ * exceeds 20 (the state is left as the reference leaves it before exiting).
+ * Returns FREHD_ERR_CG_NOCONVERGE, a warning, when the solve stopped at maxIter
+ * before ||r|| < eps*||b||: the step completed with that solution, as the
+ * reference's does. */
 int frehd_domain_step(frehd_domain *d, int tt);
 /* Steps t0 .. t0+nsteps-1 back to back without host synchronisation; the status
- * is checked once at the end.  Stops early (and reports) on CFL > 20. */
+ * is checked once at the end.  Stops early (and reports) on CFL > 20; reports
+ * FREHD_ERR_CG_NOCONVERGE, after running every step, when any of their solves
+ * stopped at maxIter. */
 int frehd_domain_run(frehd_domain *d, int t0, int nsteps);
+
+/* Failure-path testing of the bounded device waits (no counterpart in the
+ * reference).  The grid-barrier waits of this domain's solves give up after
+ * wait_limit_ns (0: the default of 2 s) and then end the step with
+ * FREHD_ERR_TIMEOUT; with skip_barrier_rank >= 0, the CTA of that rank in the
+ * next solve leaves before its first grid barrier without arriving, so that the
+ * other CTAs' wait runs out (skip_barrier_rank = -1: none).  Nothing faults or
+ * hangs: every wait is bounded, and no load or partial sum is in flight at that
+ * barrier.  frehd_domain_upload_state / frehd_domain_init clear both settings
+ * together with the status. */
+int frehd_domain_set_wait_test(frehd_domain *d, long long wait_limit_ns, int skip_barrier_rank);
 
 /* Phases of one step, for parity testing against the reference's functions:
  *   FREHD_PHASE_EXPLICIT  solveSourceTerm + matrixCoeffSub/adjust*Boundary (nssolve.c:121-166)

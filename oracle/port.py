@@ -1,8 +1,9 @@
-"""ctypes wrapper of the C restatement oracle (oracle/frehd_oracle.c).
+"""ctypes wrapper of the C restatement oracle (oracle/frehd_oracle.c) and of
+the deck pre-processing for runs of the reference program (oracle/deckprep.c).
 
 TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__ (build/smoke) and
-bench.py's cpu_baseline leg.  build() compiles the oracle with plain gcc (no FMA
-contraction, IEEE doubles) into oracle/_build/libfrehd_oracle.so.
+bench.py's cpu_baseline and reference legs.  build() compiles both with plain
+gcc (no FMA contraction, IEEE doubles) into oracle/_build/libfrehd_oracle.so.
 """
 from __future__ import annotations
 
@@ -17,6 +18,10 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(BUILD, "libfrehd_oracle.so")
 SRC = os.path.join(HERE, "frehd_oracle.c")
 HDR = os.path.join(HERE, "frehd_oracle.h")
+PREP = os.path.join(HERE, "deckprep.c")
+# the pre-processor's formulas (one inline definition shared with the library)
+LEVELS_DIR = os.path.join(os.path.dirname(HERE), "frehdc_b200", "csrc")
+LEVELS = os.path.join(LEVELS_DIR, "subgrid_levels.h")
 
 PRECOND_JACOBI, PRECOND_SSOR = 0, 1
 X0_ZERO, X0_SURFACE = 0, 1
@@ -26,10 +31,11 @@ _lib = None
 
 def build(force: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
+    deps = (SRC, HDR, PREP, LEVELS)
     if force or not os.path.exists(LIB) or \
-            max(os.path.getmtime(SRC), os.path.getmtime(HDR)) > os.path.getmtime(LIB):
+            max(os.path.getmtime(d) for d in deps) > os.path.getmtime(LIB):
         subprocess.run(["gcc", "-O2", "-fPIC", "-shared", "-fno-fast-math", "-ffp-contract=off",
-                        "-o", LIB, SRC, "-lm"], check=True)
+                        "-fopenmp", "-I", LEVELS_DIR, "-o", LIB, SRC, PREP, "-lm"], check=True)
     return LIB
 
 
@@ -91,12 +97,40 @@ def lib() -> C.CDLL:
         L.oracle_field_len.restype = C.c_long
         L.oracle_get.argtypes = [C.c_void_p, C.c_char_p, _dp, C.c_long]
         L.oracle_set.argtypes = [C.c_void_p, C.c_char_p, _dp, C.c_long]
+        L.oracle_build_tables.argtypes = [_dp, C.c_long, C.c_int, C.c_int, C.c_int, C.c_double,
+                                          C.c_double, C.c_double, C.c_double, C.c_int, C.c_int,
+                                          _dp]
+        L.oracle_build_bottoms.argtypes = [_dp, C.c_long, C.c_int, C.c_int, C.c_int, _dp, _dp,
+                                           _dp]
         _lib = L
     return _lib
 
 
 def _p(a: np.ndarray):
     return a.ctypes.data_as(_dp)
+
+
+# ---- deck pre-processing (the same interface as frehdc_b200.native's builders)
+def build_tables(zf: np.ndarray, nx: int, ny: int, r: int, dxf: float, dyf: float,
+                 surfmin: float, dsurf: float, Ne: int, block_check: bool = False) -> np.ndarray:
+    """(10, Ne, N) subgrid tables of fine bottoms zf ((ny*r, nx*r))."""
+    zf = np.ascontiguousarray(zf, dtype=np.float64)
+    out = np.empty((10, Ne, nx * ny), dtype=np.float64)
+    rc = lib().oracle_build_tables(_p(zf), zf.shape[1], nx, ny, r, dxf, dyf, surfmin, dsurf, Ne,
+                                   int(bool(block_check)), _p(out))
+    if rc:
+        raise ValueError(f"oracle_build_tables: bad arguments ({rc})")
+    return out
+
+
+def build_bottoms(zf: np.ndarray, nx: int, ny: int, r: int):
+    """Coarse bottom, bottomXP and bottomYP (N doubles each) of fine bottoms zf."""
+    zf = np.ascontiguousarray(zf, dtype=np.float64)
+    N = nx * ny
+    b, bx, by = np.empty(N), np.empty(N), np.empty(N)
+    if lib().oracle_build_bottoms(_p(zf), zf.shape[1], nx, ny, r, _p(b), _p(bx), _p(by)):
+        raise ValueError("oracle_build_bottoms: bad arguments")
+    return b, bx, by
 
 
 class Oracle:

@@ -372,12 +372,19 @@ int main(int argc, char **argv) {
   } else if (!strcmp(mode, "phases")) {
     for (int tt = 1; tt <= steps; ++tt) phased_step(tt, out, want(tt, at, nat));
   } else if (!strcmp(mode, "time")) {
+    /* the CG iterations of each step (laspack's count of the last solve, rtc.c:74)
+     * are summed outside the timed loop body's work */
+    long iters = 0;
     double t0 = now();
-    for (int tt = 1; tt <= steps; ++tt) solveall_step(tt);
+    for (int tt = 1; tt <= steps; ++tt) {
+      solveall_step(tt);
+      iters += GetLastNoIter();
+    }
     double t1 = now();
     double cs = (double)setting->N2ci * steps / (t1 - t0);
-    printf("{\"steps\": %d, \"cells\": %d, \"seconds\": %.6f, \"cell_steps_per_s\": %.6e}\n",
-           steps, setting->N2ci, t1 - t0, cs);
+    printf("{\"steps\": %d, \"cells\": %d, \"seconds\": %.6f, \"cell_steps_per_s\": %.6e, "
+           "\"cg_iters_per_step\": %.3f}\n",
+           steps, setting->N2ci, t1 - t0, cs, (double)iters / steps);
     if (out[0]) dump_state(out, steps, NULL);
   } else {
     fprintf(stderr, "frehd_ref: unknown mode %s\n", mode);

@@ -18,7 +18,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 RECIPE = os.path.join(HERE, "ref")
-REF_SRC = os.environ.get("FREHD_REFERENCE", "/root/reference")
+# The reference checkout: $FREHD_REFERENCE, else a directory named "reference"
+# beside this repository's root (where the build machine keeps it).
+REF_SRC = os.environ.get("FREHD_REFERENCE") or os.path.join(
+    os.path.dirname(os.path.dirname(HERE)), "reference")
 
 PARITY_BIN = os.path.join(REF_DIR, "frehd_ref")
 # the parity build with laspack's JacobiPrecond in place of SSORPrecond

@@ -16,11 +16,13 @@ A fixture keeps, for the final state of the run:
 Cases:
   c1_128      128 x 128, dx 10 m, dt 1 s, 200 steps, n 0.03 (the CPU case)
   c2crop_512  the 512 x 512 window of the 4096 x 4096 deck (dx 2 m, dt 0.5 s,
-              ~30 % dry, n 0.025) along its tidal edge, 100 steps, with the
-              scalar plume centred in the window
+              ~30 % dry, n 0.025) along its tidal edge, 1000 steps (the step
+              count of the 4096 x 4096 workload), with the scalar plume
+              centred in the window
 
-Run from the repository root where the reference sources are present:
-    python tests/golden/make_golden.py
+Run from the repository root where the reference sources are present (the two
+reference runs of a case run side by side; the 512 x 512 case takes minutes):
+    python tests/golden/make_golden.py [case ...]
 """
 from __future__ import annotations
 
@@ -49,7 +51,7 @@ def c1_spec() -> D.DeckSpec:
 
 
 def c2crop_spec() -> D.DeckSpec:
-    full = D.DeckSpec(nx=4096, ny=4096, dx=2.0, dt=0.5, steps=100, seed=2024, dry_frac=0.3,
+    full = D.DeckSpec(nx=4096, ny=4096, dx=2.0, dt=0.5, steps=1000, seed=2024, dry_frac=0.3,
                       manning_n=0.025)
     return full.replace(nx=512, ny=512, crop=(0, 4096 - 512, 4096, 4096), scalar_in_window=True)
 
@@ -84,21 +86,29 @@ def load(case: str, precond: str) -> dict:
         return {k: z[k] for k in z.files}
 
 
-def main() -> int:
+def main(cases: list[str]) -> int:
+    from concurrent.futures import ThreadPoolExecutor
+
     from oracle import refrun
     if not refrun.build():
         print("the reference oracle binaries are not available", file=sys.stderr)
         return 1
-    for case, make_spec in CASES.items():
-        spec = make_spec()
+    for case in cases or list(CASES):
+        spec = CASES[case]()
         deck = D.make_deck(spec)
         N = spec.nx * spec.ny
         idx = sample_index(N)
+        with tempfile.TemporaryDirectory() as tmp:
+            path = os.path.join(tmp, case)
+            D.write_reference_deck(deck, path)
+
+            def one(precond):
+                return refrun.run(path, spec.steps, os.path.join(tmp, f"final_{precond}.bin"),
+                                  precond=precond)
+            with ThreadPoolExecutor(len(PRECONDS)) as ex:
+                states = dict(zip(PRECONDS, ex.map(one, PRECONDS)))
         for precond in PRECONDS:
-            with tempfile.TemporaryDirectory() as tmp:
-                path = os.path.join(tmp, case)
-                D.write_reference_deck(deck, path)
-                st = refrun.run(path, spec.steps, os.path.join(tmp, "final.bin"), precond=precond)
+            st = states[precond]
             out = {"fingerprint": np.array(fingerprint(deck)), "steps": np.array(spec.steps),
                    "idx": idx, "precond": np.array(precond)}
             for f in FIELDS:
@@ -111,4 +121,4 @@ def main() -> int:
 
 
 if __name__ == "__main__":
-    sys.exit(main())
+    sys.exit(main(sys.argv[1:]))

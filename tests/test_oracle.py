@@ -126,3 +126,16 @@ def test_full_run_jacobi_matches_reference(scratch):
         o.step(tt)
     for n in ["surf", "uuXP", "vvYP", "S"]:
         assert max_rel(o.get(n), ref[n]) <= 1e-9, n
+
+
+@pytest.mark.parametrize("block_check", [False, True])
+def test_oracle_deck_builders_match_library(block_check):
+    """The deck pre-processing of runs of the reference program alone
+    (oracle/deckprep.c, used by bench.py's reference arm so that it loads no
+    library of the product) gives the library's tables and bottoms bit for bit."""
+    from frehdc_b200 import deck as D
+    spec = D.DeckSpec(nx=40, ny=36, steps=5, seed=3, dry_frac=0.3, block_check=block_check)
+    a, b = D.make_deck(spec), D.make_deck(spec, host=port)
+    for f in ("bottom", "bottomXP", "bottomYP"):
+        assert getattr(a, f).tobytes() == getattr(b, f).tobytes(), f
+    assert D.build_tables(a).tobytes() == D.build_tables(a, host=port).tobytes()

@@ -18,9 +18,22 @@ Printed JSON line (rank 0):
                HBM copy peak
   cpu_baseline the reference program itself (oracle/_ref, one core) on a
                256 x 256 window of the same deck
+and the other forms of the metric, each a sub-record with its own config:
+  mixed        the same 4096^2 deck in mixed precision (FP32 inner CG in FP64
+               refinement): device rate, and eta/u/v/scalar/volume errors against
+               the FP64 run after 1000 steps
+  batched      256 seeded basins, sides 64-1024, 2 scalars, mixed precision, one
+               batch (five launches per step, graph-replayed), autotuned packing:
+               rate, the same mix stepped one domain at a time in FP64, the
+               speed-up, and errors against FP64 after 500 steps
+  served       the head of a 2000-request stream (Poisson arrivals 50/s, sides
+               64-2048, 100-2000 steps, 1-3 scalars), continuous batching in mixed
+               precision: cell-steps/s, p50/p99 latency, errors of a sample of
+               requests against FP64
 With --gpus N (torchrun) every rank steps its own replica domain (the step does
 not shard: one domain lives on one GPU), value sums them, time is the max over
-ranks.  --impl reference times the reference program on all host cores.
+ranks; the batched mix and the request stream are partitioned over the ranks.
+--impl reference times the reference program on all host cores.
 """
 from __future__ import annotations
 
@@ -215,7 +228,6 @@ def run_reference_arm(args):
 
 # ---------------------------------------------------------------- GPU arm
 def run_gpu_arm(args):
-    import numpy as np
     import torch
 
     from frehdc_b200 import deck as D
@@ -226,10 +238,11 @@ def run_gpu_arm(args):
         import datetime
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     dev = local
     n = args.n
-    spec = c2_spec(n, steps=max(args.steps + args.warmup + 5, 20))
+    extras = args.extras.split(",") if args.extras and args.extras != "none" else []
+    spec = c2_spec(n, steps=max(args.steps + args.warmup, args.mixed_steps) + 5)
     t0 = time.time()
     deck = D.make_deck(spec)
     gen_s = time.time() - t0
@@ -244,9 +257,8 @@ def run_gpu_arm(args):
     dom.set_solver(native.X0_ZERO)
     dom.set_cg_schedule(SCHEDULES[args.cg_schedule])
     if args.precision == "mixed":
-        if args.eps_inner is None:
-            args.eps_inner = 1e-5
-        dom.set_precision(native.PRECISION_MIXED, args.eps_inner)
+        dom.set_precision(native.PRECISION_MIXED,
+                          args.eps_inner if args.eps_inner is not None else 1e-5)
     dom.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
     rc = dom.run(1, args.warmup)
     if rc != 0:
@@ -263,8 +275,7 @@ def run_gpu_arm(args):
         raise RuntimeError(f"timed steps returned status {rc}")
     kt = dom.kernel_times()
     st = dom.stats()
-    dev_ms = sum(kt[k] for k in ("explicit_ms", "cg_ms", "update_geo_ms", "update_vel_ms",
-                                 "finish_ms"))
+    dev_ms = _step_ms(kt)
     t_max = dev_ms
     if ws > 1:
         tt = torch.tensor([dev_ms], device=f"cuda:{dev}", dtype=torch.float64)
@@ -273,47 +284,97 @@ def run_gpu_arm(args):
     value = ws * N * args.steps / (t_max / 1e3)
     iters = kt["cg_iters"] / max(kt["steps"], 1)
     dom.set_profiling(False)
-    errors = None
-    if args.precision == "mixed":
-        errors = mixed_errors(dom, deck, cfg, tide, dev, args.warmup + args.steps, N)
-    dom.close()
 
     # ---- e2e: through the C ABI from host buffers
-    if args.no_e2e:
-        e2e = None
-    else:
-        e2e = run_e2e(args, deck, cfg, tide, dev, ws, N)
+    e2e = None if args.no_e2e else run_e2e(args, deck, cfg, tide, dev, ws, N)
+
+    # ---- the other forms of the metric, each its own sub-record
+    sub = {}
+    if "mixed" in extras and args.precision == "fp64":
+        sub["mixed"] = _guard(lambda: measure_mixed_domain(args, deck, cfg, tide, dev, ws, dom))
+    dom.close()
+    del deck
+    if "batched" in extras:
+        sub["batched"] = _guard(lambda: measure_batched(
+            args, ws, rank, dev, 256, 64, 1024, 2, args.batched_total, "mixed",
+            args.batched_steps, args.warmup))
+    if "served" in extras:
+        sub["served"] = _guard(lambda: measure_served(
+            args, ws, rank, dev, 2000, args.served_requests, 64, 2048, 100, 2000, 3, 50.0,
+            "mixed", args.served_cells_per_cta, 1e-4, 10))
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     if rank != 0:
         return 0
-    return report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk, errors)
+    return report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk, sub)
 
 
-def mixed_errors(dom, deck, cfg, tide, dev, steps, N):
-    """The mixed-precision domain's state after `steps` steps against an FP64
-    run of the same deck and steps."""
-    import numpy as np
+def _guard(fn):
+    """A sub-measurement's record, or its error: a failure there must not cost
+    the headline line.  (Every rank takes the same collective steps either way:
+    the sub-measurements gather only at their end.)"""
+    try:
+        return fn()
+    except Exception as e:  # reported in the JSON line
+        import traceback
+        traceback.print_exc(file=sys.stderr)
+        return {"error": f"{type(e).__name__}: {e}"}
+
+
+def measure_mixed_domain(args, deck, cfg, tide, dev, ws, ref):
+    """The mixed-precision form on the same domain (FP32 inner CG iterations in
+    FP64 refinement): device time of K steps after W warm-up steps, then the run
+    continued untimed to args.mixed_steps steps and its state compared with the
+    FP64 domain `ref` (the plain measurement's, at step W+K) continued to the
+    same step."""
+    import torch
 
     from frehdc_b200 import native
-    ref = native.Domain(cfg, dev)
-    ref.set_fine_bottoms(deck.zf, deck.r)
-    ref.set_tide(tide)
-    ref.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
-    if ref.run(1, steps) != 0:
-        raise RuntimeError("FP64 comparison run failed")
+    N = cfg["nx"] * cfg["ny"]
+    W, K, S = args.warmup, args.steps, args.mixed_steps
+    eps_inner = args.eps_inner if args.eps_inner is not None else 1e-5
+    g = native.Domain(cfg, dev)
+    g.set_fine_bottoms(deck.zf, deck.r)
+    g.set_tide(tide)
+    g.set_precision(native.PRECISION_MIXED, eps_inner)
+    g.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
+    if g.run(1, W) != 0:
+        raise RuntimeError("mixed warm-up failed")
+    g.sync()
+    g.set_profiling(True)
+    if g.run(1 + W, K) != 0:
+        raise RuntimeError("mixed timed steps failed")
+    g.sync()
+    kt = g.kernel_times()
+    g.set_profiling(False)
+    ms = _step_ms(kt)
+    if ws > 1:
+        t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    if S > W + K:
+        if g.run(1 + W + K, S - W - K) != 0 or ref.run(1 + W + K, S - W - K) != 0:
+            raise RuntimeError("mixed or FP64 continuation failed")
     names = ["surf", "uuXP", "vvYP", "S"]
-    a, b = dom.download(names), ref.download(names)
-    va, vb = dom.stats()["volume"], ref.stats()["volume"]
-    ref.close()
-
-    def rel(f):
-        return float(np.max(np.abs(a[f][:N] - b[f][:N])) / max(np.max(np.abs(b[f][:N])), 1e-300))
-    return {"steps": steps, "eta_max_abs_m": float(np.max(np.abs(a["surf"][:N] - b["surf"][:N]))),
-            "u_max_rel": rel("uuXP"), "v_max_rel": rel("vvYP"),
-            "S_max_abs": float(np.max(np.abs(a["S"][:N] - b["S"][:N]))),
-            "volume_rel": abs(va - vb) / abs(vb), "against": "the FP64 run of the same deck"}
+    a, r = g.download(names), ref.download(names)
+    import numpy as np
+    err = _state_errors(a, r, N)
+    err["S_max_abs"] = float(np.max(np.abs(a["S"][:N] - r["S"][:N])))
+    va, vr = g.stats()["volume"], ref.stats()["volume"]
+    err["volume_rel"] = abs(va - vr) / abs(vr)
+    err["after_steps"] = max(S, W + K)
+    err["against"] = "the FP64 run of the same deck and steps"
+    inner = kt["cg_iters"] / max(kt["steps"], 1)
+    g.close()
+    return {"value": ws * N * K / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / K,
+            "steps_timed": K, "warmup": W, "dtype": "f32+f64",
+            "config": {"workload": f"{cfg['nx']}x{cfg['ny']} mixed FP32/FP64 (the plain "
+                                   "workload's deck)", "eps_inner": eps_inner},
+            "per_kernel_ms_per_step": {k: kt[k] / kt["steps"] for k in
+                                       ("explicit_ms", "cg_ms", "update_geo_ms",
+                                        "update_vel_ms", "finish_ms")},
+            "cg_inner_iters_per_step": inner, "errors_vs_fp64": err}
 
 
 def run_e2e(args, deck, cfg, tide, dev, ws, N):
@@ -383,7 +444,7 @@ def cg_bytes_per_cell(iters: float, fp64: bool = True) -> float:
     return 48.0 + (72.0 if fp64 else 32.0) * iters
 
 
-def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk, errors=None):
+def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk, sub=None):
     N = n * n
     peak, peak_kind = measured_hbm_peak()
     cg_launch_ms = kt["cg_ms"] / kt["steps"]
@@ -440,8 +501,8 @@ def report(args, kt, st, iters, t_max, value, ws, n, spec, gen_s, e2e, clk, erro
         "cpu_baseline": cpu,
         "last_step": st,
     }
-    if errors is not None:
-        line["errors_vs_fp64"] = errors
+    for k, v in (sub or {}).items():
+        line[k] = v
     print(json.dumps(line), flush=True)
     return 0
 
@@ -495,58 +556,84 @@ def _dist_done(ws):
         dist.destroy_process_group()
 
 
-def run_batched_form(args):
-    """Cell-steps/s of a mix of domains stepped as one batch, against the same
-    mix stepped one domain at a time through the single-domain API.  Under
-    torchrun the mix is partitioned across ranks by cell count
-    (frehdc_b200.shard.balance); each rank batches its share on its own GPU
-    and the slowest rank's device time sets the whole-job rate."""
+def _step_ms(kt) -> float:
+    return sum(kt[k] for k in ("explicit_ms", "cg_ms", "update_geo_ms", "update_vel_ms",
+                               "finish_ms"))
+
+
+def _state_errors(a: dict, ref: dict, n: int) -> dict:
+    """Errors of a state against a reference state (both in the reference
+    layout): eta absolute (m), face velocities relative to the reference's max."""
+    import numpy as np
+
+    def rel(f):
+        sc = max(float(np.max(np.abs(ref[f][:n]))), 1e-300)
+        return float(np.max(np.abs(a[f][:n] - ref[f][:n]))) / sc
+    return {"eta_max_abs_m": float(np.max(np.abs(a["surf"][:n] - ref["surf"][:n]))),
+            "u_max_rel": rel("uuXP"), "v_max_rel": rel("vvYP")}
+
+
+def _worst(errs: list) -> dict | None:
+    errs = [e for e in errs if e]
+    return {k: max(e[k] for e in errs) for k in errs[0]} if errs else None
+
+
+def measure_batched(args, ws, rank, dev, n_mix, smin, smax, scalars, total_steps, precision,
+                    K, W):
+    """A mix of basins stepped as one batch (one launch per sub-step for all of
+    them, replayed from a CUDA graph), against the same mix stepped one domain
+    at a time through the single-domain API in FP64.
+
+    Under torchrun the mix is partitioned across ranks by cell count
+    (frehdc_b200.shard.balance); each rank batches its share on its own GPU and
+    the slowest rank's device time sets the whole-job rate.  The batch runs W
+    warm-up steps, K timed steps (device time, CUDA events on the batch's
+    stream) and the rest of total_steps untimed; in the mixed form every basin's
+    state after total_steps is compared with an FP64 run of the same steps (the
+    FP64 domains of the plain-form timing, continued in an FP64 batch)."""
     import torch
 
     from frehdc_b200 import deck as D
     from frehdc_b200 import native, shard
-    ws, rank, dev = _dist_init()
-    specs_all = mix_specs(args.mix, 77, args.mix_min, args.mix_max, args.steps + args.warmup + 5,
-                          (args.scalars, args.scalars))
+    specs_all = mix_specs(n_mix, 77, smin, smax, total_steps + 5, (scalars, scalars))
     mine = shard.balance([sp.nx * sp.ny for sp in specs_all], ws)[rank]
     specs = [specs_all[i] for i in mine]
     t0 = time.time()
-    decks = [D.make_deck(sp) for sp in specs]
+    decks = D.make_decks(specs)
     gen_s = time.time() - t0
     cells = [sp.nx * sp.ny for sp in specs]
-    K = args.steps
-    # plain form: each domain alone, device time of its K steps (kernel events)
+    prec = native.PRECISION_MIXED if precision == "mixed" else native.PRECISION_FP64
+    budget = args.budget_gb << 30
+    # plain form: each domain alone (FP64), device time of its K steps
+    ref = [native.domain_from_deck(dk, device=dev) for dk in decks]
     plain_ms = 0.0
-    for dk in decks:
-        g = native.domain_from_deck(dk, device=dev)
-        g.run(1, args.warmup)
+    for g in ref:
+        g.run(1, W)
         g.sync()
         g.set_profiling(True)
-        g.run(1 + args.warmup, K)
+        g.run(1 + W, K)
         g.sync()
-        kt = g.kernel_times()
-        plain_ms += sum(kt[k] for k in ("explicit_ms", "cg_ms", "update_geo_ms", "update_vel_ms",
-                                        "finish_ms"))
-        g.close()
-    # batched form (packing granularity and inner tolerance from the autotuner,
-    # tuned on rank 0's share and used by every rank)
-    prec = native.PRECISION_MIXED if args.precision == "mixed" else native.PRECISION_FP64
+        plain_ms += _step_ms(g.kernel_times())
+        g.set_profiling(False)
+    # packing granularity and inner tolerance from the autotuner, tuned on rank
+    # 0's share and used by every rank
     tuning = None
-    if args.cells_per_cta <= 0:
+    cpc, eps_inner = args.cells_per_cta, args.eps_inner
+    if cpc <= 0:
         from frehdc_b200 import autotune
         if rank == 0:
-            tuning = autotune.tune(decks, args.budget_gb << 30, prec, device=dev)
+            tuning = autotune.tune(decks, budget, prec, device=dev)
         tuning = shard.broadcast(tuning, ws)
-        args.cells_per_cta = tuning["best"]["cells_per_cta"]
-        args.eps_inner = tuning["best"]["eps_inner"]
-    if args.eps_inner is None:
-        args.eps_inner = 1e-5
-    doms = [native.domain_from_deck(dk, device=dev, precision=prec, eps_inner=args.eps_inner)
+        cpc = tuning["best"]["cells_per_cta"]
+        eps_inner = tuning["best"]["eps_inner"]
+    if eps_inner is None:
+        eps_inner = 1e-4
+    doms = [native.domain_from_deck(dk, device=dev, precision=prec, eps_inner=eps_inner)
             for dk in decks]
-    b = native.Batch(args.budget_gb << 30, args.cells_per_cta, dev)
+    b = native.Batch(budget, cpc, dev)
     for g in doms:
         b.admit(g, 1)
-    for _ in range(args.warmup):
+    for _ in range(W):
         b.step()
     b.sync()
     if ws > 1:
@@ -560,133 +647,173 @@ def run_batched_form(args):
         e1.record(st)
         e1.synchronize()
     batch_ms = e0.elapsed_time(e1)
+    for _ in range(total_steps - W - K):
+        b.step()
+    b.sync()
     info = b.info()
-    slots = list(b.members)
-    for sl in slots:
+    for sl in list(b.members):
         b.release(sl)
     b.close()
     errors = None
-    if args.precision == "mixed":  # every domain against its FP64 run of the same steps
+    if precision == "mixed":
         import numpy as np
-        worst = {"eta_max_abs_m": 0.0, "u_max_rel": 0.0, "v_max_rel": 0.0, "volume_rel": 0.0,
-                 "scalar_max_abs": 0.0}
-        for g, dk in zip(doms, decks):
-            r = native.domain_from_deck(dk, device=dev)
-            r.run(1, args.warmup + K)
+        fb = native.Batch(budget, cpc, dev)
+        for g in ref:
+            fb.admit(g, W + K + 1)
+        for _ in range(total_steps - W - K):
+            fb.step()
+        fb.sync()
+        for sl in list(fb.members):
+            fb.release(sl)
+        fb.close()
+        per = []
+        for g, r, dk in zip(doms, ref, decks):
             n_ = dk.spec.nx * dk.spec.ny
-            a, c = g.download(["surf", "uuXP", "vvYP"]), r.download(["surf", "uuXP", "vvYP"])
-            worst["eta_max_abs_m"] = max(worst["eta_max_abs_m"],
-                                         float(np.max(np.abs(a["surf"][:n_] - c["surf"][:n_]))))
-            for f, key in (("uuXP", "u_max_rel"), ("vvYP", "v_max_rel")):
-                sc = max(float(np.max(np.abs(c[f][:n_]))), 1e-300)
-                worst[key] = max(worst[key], float(np.max(np.abs(a[f][:n_] - c[f][:n_]))) / sc)
-            for s_ in range(1 + len(dk.tracers)):   # S and the tracers
-                worst["scalar_max_abs"] = max(worst["scalar_max_abs"], float(np.max(np.abs(
-                    g.download_scalar(s_)[:n_] - r.download_scalar(s_)[:n_]))))
-            va, vc = g.stats()["volume"], r.stats()["volume"]
-            worst["volume_rel"] = max(worst["volume_rel"], abs(va - vc) / abs(vc))
-            r.close()
-        errors = worst
-    for g in doms:
+            names = ["surf", "uuXP", "vvYP"]
+            e = _state_errors(g.download(names), r.download(names), n_)
+            e["scalar_max_abs"] = max(float(np.max(np.abs(
+                g.download_scalar(s_)[:n_] - r.download_scalar(s_)[:n_])))
+                for s_ in range(1 + len(dk.tracers)))
+            va, vr = g.stats()["volume"], r.stats()["volume"]
+            e["volume_rel"] = abs(va - vr) / abs(vr)
+            per.append(e)
+        errors = _worst(per)
+    for g in doms + ref:
         g.close()
     parts = shard.gather({"batch_ms": batch_ms, "plain_ms": plain_ms, "cells": int(sum(cells)),
                           "domains": len(decks), "errors": errors, "clocks": clk.summary(),
                           "info": info, "gen_s": gen_s}, ws)
-    _dist_done(ws)
-    if rank != 0:
-        return 0
     t_batch = max(p["batch_ms"] for p in parts)
     t_plain = max(p["plain_ms"] for p in parts)
     total_cells = sum(p["cells"] for p in parts)
     total = float(total_cells) * K
-    line = {"metric": METRIC, "form": "batched", "value": total / (t_batch / 1e3),
-            "unit": UNIT, "n_gpus": ws, "steps": K, "warmup": args.warmup,
-            "ms_per_step": t_batch / K, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
-            "data": "synthetic",
-            "config": {"precision": args.precision,
-                       "workload": f"{len(specs_all)} seeded basins, sides log-uniform "
-                                   f"{args.mix_min}-{args.mix_max} (square or 1:4), dx 10 m, "
-                                   "dt 1 s, depth 0.3-8 m, 0-40% dry, tide 0.1-0.5 m, "
-                                   f"n 0.02-0.04, 4x4 subgrid, {args.scalars} scalar(s)",
-                       "cells": int(total_cells), "cells_per_cta": args.cells_per_cta,
-                       "sharding": "by cell count over ranks" if ws > 1 else None,
-                       "deck_gen_s": round(max(p["gen_s"] for p in parts), 1)},
-            "plain_form_same_mix": {"value": total / (t_plain / 1e3), "unit": UNIT,
-                                    "note": "each domain stepped alone, device time of its "
-                                            "kernels summed over the mix"},
-            "batch": parts[0]["info"] if ws == 1 else [p["info"] for p in parts],
-            "gpu_launches": 5 * K, "clocks": parts[0]["clocks"]}
+    rec = {"value": total / (t_batch / 1e3), "unit": UNIT, "ms_per_step": t_batch / K,
+           "steps_timed": K, "warmup": W, "steps_total": total_steps,
+           "dtype": "f64" if precision == "fp64" else "f32+f64",
+           "config": {"precision": precision,
+                      "workload": f"{n_mix} seeded basins, sides log-uniform {smin}-{smax} "
+                                  "(square or 1:4), dx 10 m, dt 1 s, depth 0.3-8 m, 0-40% dry, "
+                                  "tide 0.1-0.5 m, n 0.02-0.04, 4x4 subgrid, "
+                                  f"{scalars} scalar(s)",
+                      "cells": int(total_cells), "cells_per_cta": cpc,
+                      "eps_inner": eps_inner if precision == "mixed" else None,
+                      "sharding": "by cell count over ranks" if ws > 1 else None,
+                      "deck_gen_s": round(max(p["gen_s"] for p in parts), 1)},
+           "plain_form_same_mix": {"value": total / (t_plain / 1e3), "unit": UNIT,
+                                   "note": "each domain stepped alone in FP64, device time of "
+                                           "its kernels summed over the mix"},
+           "batch": parts[0]["info"] if ws == 1 else [p["info"] for p in parts],
+           "gpu_launches_timed": 5 * K, "clocks": parts[0]["clocks"]}
+    rec["speedup_vs_plain_form"] = rec["value"] / rec["plain_form_same_mix"]["value"]
     if ws > 1:
-        line["per_rank"] = [{"domains": p["domains"], "cells": p["cells"], "batch_ms": p["batch_ms"]}
-                            for p in parts]
-    line["speedup_vs_plain_form"] = line["value"] / line["plain_form_same_mix"]["value"]
-    line["config"]["eps_inner"] = args.eps_inner if args.precision == "mixed" else None
+        rec["per_rank"] = [{"domains": p["domains"], "cells": p["cells"],
+                            "batch_ms": p["batch_ms"]} for p in parts]
     if tuning is not None:
-        line["autotune"] = tuning
-    if args.precision == "mixed":
-        errs = [p["errors"] for p in parts if p["errors"]]
-        line["errors_vs_fp64"] = {k: max(e[k] for e in errs) for k in errs[0]} if errs else None
-    print(json.dumps(line), flush=True)
-    return 0
+        rec["autotune"] = tuning
+    if precision == "mixed":
+        rec["errors_vs_fp64"] = _worst([p["errors"] for p in parts])
+        if rec["errors_vs_fp64"] is not None:
+            rec["errors_vs_fp64"]["after_steps"] = total_steps
+    return rec
 
 
-def run_served_form(args):
-    """A stream of requests with Poisson arrivals served by continuous batching.
-    Under torchrun each request goes to the rank with the least work assigned
-    so far, in arrival order (frehdc_b200.shard.assign_stream); every rank
-    serves its share on its own GPU at the original arrival times."""
+def measure_served(args, ws, rank, dev, n_stream, n_req, smin, smax, steps_lo, steps_hi,
+                   scalars_max, rate, precision, cells_per_cta, eps_inner, check_every):
+    """The first n_req requests of a seeded stream of n_stream (Poisson
+    arrivals at `rate`/s, sides log-uniform smin-smax, steps uniform in
+    steps_lo..steps_hi, 1..scalars_max scalars), served by continuous batching
+    (the native server).  Under torchrun each request goes to the rank with the
+    least work assigned so far, in arrival order (frehdc_b200.shard.assign_stream).
+    Every check_every-th request (mixed precision) is run again alone in FP64
+    afterwards and its final state compared with the served one."""
     import numpy as np
 
     from frehdc_b200 import deck as D
     from frehdc_b200 import native, serve, shard
-    ws, rank, dev = _dist_init()
     rng = np.random.default_rng(5)
-    specs = mix_specs(args.requests, 91, args.mix_min, args.mix_max, 10, (1, args.scalars_max))
-    steps = rng.integers(args.req_steps_min, args.req_steps_max + 1, size=len(specs))
-    arr = serve.poisson_arrivals(len(specs), args.rate, 17)
+    specs = mix_specs(n_stream, 91, smin, smax, 10, (1, scalars_max))[:n_req]
+    steps = rng.integers(steps_lo, steps_hi + 1, size=n_stream)[:n_req]
+    arr = serve.poisson_arrivals(n_stream, rate, 17)[:n_req]
     owner = shard.assign_stream(arr, [sp.nx * sp.ny * int(k) for sp, k in zip(specs, steps)], ws)
-    mine = [i for i in range(len(specs)) if owner[i] == rank]
+    mine = [i for i in range(n_req) if owner[i] == rank]
     t0 = time.time()
-    decks = {i: D.make_deck(specs[i].replace(steps=int(steps[i]) + 5)) for i in mine}
+    gen = D.make_decks([specs[i].replace(steps=int(steps[i]) + 5) for i in mine])
+    decks = dict(zip(mine, gen))
     gen_s = time.time() - t0
     reqs = [serve.Request(i, decks[i], int(steps[i]), float(arr[i])) for i in mine]
-    prec = native.PRECISION_MIXED if args.precision == "mixed" else native.PRECISION_FP64
-    if args.eps_inner is None:
-        # the inner tolerance the autotuner picks on the batched mix of the same
-        # sizes (64 basins, 64-512); on this stream 1e-5 served 1.8e8 against 3.0e8
-        args.eps_inner = 1e-4
+    prec = native.PRECISION_MIXED if precision == "mixed" else native.PRECISION_FP64
+    check = [i for i in mine if i % check_every == 0] if precision == "mixed" else []
+    served_state = {}
 
     def build(req):
-        return native.domain_from_deck(req.deck, device=dev, precision=prec,
-                                       eps_inner=args.eps_inner)
-    if args.cells_per_cta <= 0:
-        args.cells_per_cta = 32768.0
+        return native.domain_from_deck(req.deck, device=dev, precision=prec, eps_inner=eps_inner)
+
+    def done(req):
+        if req.rid in check:
+            served_state[req.rid] = req.domain.download(["surf", "uuXP", "vvYP"])
+
     if ws > 1:
         import torch
         torch.distributed.barrier()
     with ClockSampler(dev) as clk:
-        res = serve.serve(reqs, args.budget_gb << 30, args.cells_per_cta, device=dev, build=build)
-    parts = shard.gather({**res, "clocks": clk.summary(), "gen_s": gen_s}, ws)
-    _dist_done(ws)
-    if rank != 0:
-        return 0
+        res = serve.serve(reqs, args.budget_gb << 30, cells_per_cta, device=dev, build=build,
+                          on_done=done)
+    per = []
+    for i in check:
+        g = native.domain_from_deck(decks[i], device=dev)
+        g.run(1, int(steps[i]))
+        n_ = decks[i].nx * decks[i].ny
+        per.append(_state_errors(served_state[i], g.download(["surf", "uuXP", "vvYP"]), n_))
+        g.close()
+    parts = shard.gather({**res, "clocks": clk.summary(), "gen_s": gen_s,
+                          "errors": _worst(per), "checked": len(per)}, ws)
     merged = shard.merge_served(parts)
-    line = {"metric": METRIC, "form": "served", "value": merged["cell_steps_per_s"], "unit": UNIT,
-            "n_gpus": ws, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
-            "p50_latency_s": merged["p50_s"], "p99_latency_s": merged["p99_s"],
-            "config": {"workload": f"{len(specs)} requests, Poisson arrivals {args.rate}/s, sides "
-                                   f"log-uniform {args.mix_min}-{args.mix_max}, steps "
-                                   f"{args.req_steps_min}-{args.req_steps_max}, 1-{args.scalars_max} scalars, "
-                                   f"{args.precision}",
-                       "cells_per_cta": args.cells_per_cta,
-                       "eps_inner": args.eps_inner if args.precision == "mixed" else None,
-                       "sharding": "least assigned work, arrival order" if ws > 1 else None,
-                       "deck_gen_s": round(max(p["gen_s"] for p in parts), 1)},
-            "serving": merged, "clocks": parts[0]["clocks"],
-            "gpu_launches": 5 * sum(int(p.get("batch_steps", 0)) for p in parts)}
-    print(json.dumps(line), flush=True)
+    rec = {"value": merged["cell_steps_per_s"], "unit": UNIT,
+           "p50_latency_s": merged["p50_s"], "p99_latency_s": merged["p99_s"],
+           "dtype": "f64" if precision == "fp64" else "f32+f64",
+           "config": {"workload": f"the first {n_req} requests of a {n_stream}-request stream: "
+                                  f"Poisson arrivals {rate}/s, sides log-uniform {smin}-{smax} "
+                                  f"(square or 1:4), steps {steps_lo}-{steps_hi}, "
+                                  f"1-{scalars_max} scalars, {precision}",
+                      "requests": n_req, "cells_per_cta": cells_per_cta,
+                      "eps_inner": eps_inner if precision == "mixed" else None,
+                      "sharding": "least assigned work, arrival order" if ws > 1 else None,
+                      "deck_gen_s": round(max(p["gen_s"] for p in parts), 1)},
+           "serving": merged, "clocks": parts[0]["clocks"],
+           "gpu_launches": 5 * sum(int(p.get("batch_steps", 0)) for p in parts)}
+    if precision == "mixed":
+        rec["errors_vs_fp64"] = _worst([p["errors"] for p in parts])
+        rec["errors_checked_requests"] = int(sum(p["checked"] for p in parts))
+    return rec
+
+
+def run_batched_form(args):
+    """--form batched: the batched measurement alone, as its own JSON line."""
+    ws, rank, dev = _dist_init()
+    rec = measure_batched(args, ws, rank, dev, args.mix, args.mix_min, args.mix_max,
+                          args.scalars, args.steps + args.warmup, args.precision, args.steps,
+                          args.warmup)
+    _dist_done(ws)
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "form": "batched", "n_gpus": ws,
+                          "higher_is_better": True, "scaling": "weak", "data": "synthetic",
+                          **rec}), flush=True)
+    return 0
+
+
+def run_served_form(args):
+    """--form served: the served measurement alone, as its own JSON line."""
+    ws, rank, dev = _dist_init()
+    eps = args.eps_inner if args.eps_inner is not None else 1e-4
+    cpc = args.cells_per_cta if args.cells_per_cta > 0 else 65536.0
+    rec = measure_served(args, ws, rank, dev, args.requests, args.requests, args.mix_min,
+                         args.mix_max, args.req_steps_min, args.req_steps_max, args.scalars_max,
+                         args.rate, args.precision, cpc, eps, 10)
+    _dist_done(ws)
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "form": "served", "n_gpus": ws,
+                          "higher_is_better": True, "scaling": "weak", "data": "synthetic",
+                          **rec}), flush=True)
     return 0
 
 
@@ -722,6 +849,19 @@ def main():
     ap.add_argument("--scalars", type=int, default=2, help="batched form: scalars per basin")
     ap.add_argument("--scalars-max", type=int, default=3,
                     help="served form: scalars per request uniform in 1..this")
+    ap.add_argument("--extras", default="mixed,batched,served",
+                    help="plain form: the other forms measured into the same JSON line "
+                         "(comma list of mixed, batched, served; 'none' for none)")
+    ap.add_argument("--mixed-steps", type=int, default=1000,
+                    help="mixed sub-record: steps after which its state is compared with FP64")
+    ap.add_argument("--batched-steps", type=int, default=20,
+                    help="batched sub-record: timed batch steps")
+    ap.add_argument("--batched-total", type=int, default=500,
+                    help="batched sub-record: steps after which the errors are taken")
+    ap.add_argument("--served-requests", type=int, default=100,
+                    help="served sub-record: requests taken from the head of the 2000-request "
+                         "stream")
+    ap.add_argument("--served-cells-per-cta", type=float, default=65536.0)
     ap.add_argument("--requests", type=int, default=120)
     ap.add_argument("--rate", type=float, default=50.0)
     ap.add_argument("--req-steps-min", type=int, default=50)

@@ -72,6 +72,9 @@ class DeckSpec:
     # scalars carried (nscalar): S plus n_scalars - 1 tracers, plumes like S's
     # placed around it (see _tracer_fields)
     n_scalars: int = 1
+    # initial east-face velocity (uuic.dat, useConstU0 = 0): (i0, i1, j0, j1, value)
+    # sets u = value on cells i in [i0, i1), j in [j0, j1); None = u starts at 0
+    u0_block: tuple | None = None
     dsurf: float = 0.01
     eps: float = 1e-12
     max_iter: int = 100000
@@ -113,6 +116,7 @@ class Deck:
     wspd_v: np.ndarray | None = None     # windspd.dat values at tide_t (m/s)
     wdir_v: np.ndarray | None = None     # winddir.dat values at tide_t (degrees)
     tracers: list = field(default_factory=list)  # (N,) initial fields of tracers 1 ..
+    u0: np.ndarray | None = None         # (N,) initial uuXP (uuic.dat); None = zero
     extra: dict = field(default_factory=dict)
 
     @property
@@ -262,14 +266,33 @@ def make_deck(spec: DeckSpec, start: str = DEFAULT_START, with_tables: bool = Fa
     inflow_v = spec.inflow_q * (1.0 + 0.5 * np.sin(ph)) if spec.inflow_cells else None
     wspd_v = spec.wind_speed * (1.0 + 0.3 * np.sin(ph)) if spec.wind_speed > 0 else None
     wdir_v = spec.wind_dir + 20.0 * np.sin(0.7 * ph) if spec.wind_speed > 0 else None
+    u0 = None
+    if spec.u0_block is not None:
+        bi0, bi1, bj0, bj1, uval = spec.u0_block
+        u0 = np.zeros((ny, nx))
+        u0[bj0:bj1, bi0:bi1] = uval
+        u0 = u0.reshape(-1)
     deck = Deck(spec=spec, nx=nx, ny=ny, r=r, zf=zf, bottom=bottom, bottomXP=bxp, bottomYP=byp,
                 surf0=surf0.reshape(-1).copy(), S0=S0.reshape(-1).copy(), surfmin=surfmin,
                 surfmax=surfmax, dsurf=spec.dsurf, Ne=Ne, start=start, tide_t=tide_t,
                 tide_v=tide_v, Nt=Nt, NT_days=NT_days, offset=offset, inflow_v=inflow_v,
-                wspd_v=wspd_v, wdir_v=wdir_v, tracers=tracers)
+                wspd_v=wspd_v, wdir_v=wdir_v, tracers=tracers, u0=u0)
     if with_tables:
         deck.extra["tables"] = build_tables(deck, host)
     return deck
+
+
+def make_decks(specs, procs: int | None = None) -> list:
+    """make_deck of every spec, on a pool of spawned worker processes when
+    there are several (the generator is single-threaded numpy).  Spawned, not
+    forked: a worker never inherits a CUDA context of the caller."""
+    specs = list(specs)
+    n = procs or min(16, os.cpu_count() or 1, len(specs))
+    if n <= 1 or len(specs) < 4:
+        return [make_deck(sp) for sp in specs]
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(n) as pool:
+        return pool.map(make_deck, specs, chunksize=1)
 
 
 def build_tables(deck: Deck, host=None) -> np.ndarray:
@@ -364,7 +387,7 @@ def data_dat_values(deck: Deck, out_hours: float | None = None) -> list:
         *inflow_vals, M,                                        # 26..31 inflow cells
         1 if s.wind_speed > 0 else 0, s.north_angle, M, M,      # 32..35 wind
         1, s.scalar_adv, 1, s.inflow_s, 1, 0.0, M, 1, 0.0, M,   # 36..45 scalar, tide S = 0
-        0.0, 0.0, 0.0, 0.0, 0, 1, 1, 0,                         # 46..53 IC from files
+        0.0, 0.0, 0.0, 0.0, 0, 0 if deck.u0 is not None else 1, 1, 0,  # 46..53 IC files
         1, 0, s.dx / s.r, s.dx / s.r,                           # 54..57 subgrid
         deck.surfmax, deck.surfmin, deck.dsurf,                 # 58..60
         1, 0, 0.0, 3,                                           # 61..64 staggeredV, minA, beta, minV
@@ -449,6 +472,8 @@ def write_reference_deck(deck: Deck, path: str, tables: np.ndarray | None = None
         _write_table(os.path.join(sub, name + ".dat"), tables[k], binary_tables)
     inp = os.path.join(path, "input")
     _write_column(os.path.join(inp, "surfic.dat"), deck.surf0)
+    if deck.u0 is not None:
+        _write_column(os.path.join(inp, "uuic.dat"), deck.u0)
     _write_column(os.path.join(inp, "scalaric.dat"), deck.S0)
     with open(os.path.join(inp, "tideP.dat"), "w") as f:
         for t, v in zip(deck.tide_t, deck.tide_v):

@@ -655,7 +655,7 @@ def domain_from_deck(deck, device: int = 0, geometry: str = "fine", x0: int = X0
     d.set_decoupled(decoupled)
     if precision != PRECISION_FP64:
         d.set_precision(precision, eps_inner)
-    d.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
+    d.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, deck.u0, None, deck.S0)
     for s, field in enumerate(deck.tracers, start=1):
         d.init_scalar(s, field)
     return d

@@ -377,7 +377,15 @@ int frehd_domain_set_precision(frehd_domain *d, int mode, double eps_inner);
  * exits).  Every call shares it: calls that overlap on the GPU (other streams,
  * other threads without ordering) race; queue them on one stream.  The first
  * call on each device looks up that array's address with that device current;
- * make it before any stream capture.  With iters and rel_residual both NULL
+ * make it before any stream capture.  The array takes device memory when the
+ * code that holds it is loaded on the device; with CUDA's default lazy loading
+ * that happens at this first call (its address look-up), so a host whose pool
+ * reserves the GPU's memory up front makes one call on each device before the
+ * reservation (a 1 x 1 solve on its own buffers serves) or sets
+ * CUDA_MODULE_LOADING=EAGER.  The address found at the first call is kept for
+ * the process: cudaDeviceReset invalidates it, so a host that resets a device
+ * must not call this entry point on it again.  With iters and rel_residual
+ * both NULL
  * the call only queues work on `stream` (a cudaStream_t; NULL = legacy
  * default); otherwise it waits for the solve and reports them, returning
  * FREHD_ERR_TIMEOUT if a device-side wait gave up. */

@@ -226,5 +226,5 @@ def from_deck(deck, precond: int = PRECOND_SSOR, x0: int = X0_ZERO) -> Oracle:
     o = Oracle(cfg, tables, D.tide_series(deck), precond=precond, x0=x0)
     for kind, series in D.forcing_series(deck).items():
         o.set_series(kind, series)
-    o.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, None, None, deck.S0)
+    o.init(deck.bottom, deck.bottomXP, deck.bottomYP, deck.surf0, deck.u0, None, deck.S0)
     return o

@@ -133,3 +133,35 @@ def test_dropin_matches_reference_program(name, output, tmp_path):
         # values that agree to 1e-12 print the same 4 decimals except at a tie
         assert diff.max() <= 1.0001e-4, f
         assert np.count_nonzero(diff) <= 2, f
+
+
+@pytest.mark.gpu
+def test_dropin_exits_like_the_reference_on_cfl(tmp_path):
+    """CFL > 20 (an initial 100 m/s jet, uuic.dat): like the reference program,
+    whose monitorCFL writes the state and exits (nsfunctions.c:1225-1231), the
+    drop-in host stops at the same step with a failure status, the same message
+    and the same output files of that step."""
+    if native.device_count() < 1:
+        pytest.fail("no CUDA device visible: the GPU tests need a B200")
+    b = _binary()
+    spec = D.DeckSpec(nx=48, ny=40, steps=30, seed=3, u0_block=(20, 28, 16, 24, 100.0))
+    d = D.make_deck(spec, with_tables=True)
+    ref_deck, gpu_deck = str(tmp_path / "ref"), str(tmp_path / "gpu")
+    D.write_reference_deck(d, ref_deck, out_steps=OUT_STEPS)
+    shutil.copytree(ref_deck, gpu_deck)
+    r_ref = subprocess.run([refrun.JACOBI_BIN, "run", os.path.abspath(ref_deck), str(spec.steps),
+                            str(tmp_path / "ref.bin")], capture_output=True, text=True, timeout=300)
+    r_gpu = subprocess.run([b], cwd=gpu_deck, capture_output=True, text=True, timeout=300)
+    msg = "Max CFL exceeds 20, program forced to quit!"
+    assert r_ref.returncode == 1 and msg in r_ref.stdout
+    assert r_gpu.returncode == 1 and msg in r_gpu.stdout, r_gpu.stderr[-2000:]
+    ro = _read_outputs(os.path.join(ref_deck, "output"))
+    go = _read_outputs(os.path.join(gpu_deck, "output"))
+    # the step the reference stopped at: its DataOutput files beyond step 0
+    stopped = {f for f in ro if not f.endswith("_0.dat")}
+    assert stopped and stopped <= set(go)
+    assert {f for f in go if not f.endswith("_0.dat")} == stopped
+    for f in stopped:
+        diff = np.abs(go[f] - ro[f])
+        assert diff.max() <= 1.0001e-4, f
+        assert np.count_nonzero(diff) <= 2, f

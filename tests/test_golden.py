@@ -10,7 +10,7 @@ the C oracle reproduces both reference runs of the 128 x 128 case.
 
 GPU, default solver set-up (FREHD_DECOUPLED_AS_ASSEMBLED): against the Jacobi
 runs every field agrees to 1e-9 relative to its max magnitude and the total
-water volume to 1e-12.  Against the SSOR runs the surface, scalar, depth and
+water volume to 1e-12, also after the 512 x 512 case's 1000 steps.  Against the SSOR runs the surface, scalar, depth and
 cell volumes agree to 1e-9 as well; the face velocities differ by what the two
 preconditioners leave in the solution: both solves stop at ||r|| < 1e-12 ||b||,
 b carries eta*Z with the datum offset, so eta may differ by ~1e-11 m, and
@@ -26,11 +26,14 @@ import pytest
 from tests.golden import make_golden as G
 
 _BASE = {"surf": 1e-9, "S": 1e-9, "depth": 1e-9, "cellV": 1e-9}
+# The volume bound of a run against a different solver (another preconditioner,
+# or the eliminated form) covers the ledgers of two converged solves drifting
+# apart: 3.3e-11 and 3.8e-11 relative after the 512 x 512 case's 1000 steps.
 TOL = {  # (decoupled-row mode, reference preconditioner) -> field bounds, volume bound
     ("assembled", "jacobi"): ({**_BASE, "uuXP": 1e-9, "vvYP": 1e-9}, 1e-12),
-    ("assembled", "ssor"): ({**_BASE, "uuXP": 1e-7, "vvYP": 1e-7}, 1e-11),
-    ("eliminated", "jacobi"): ({**_BASE, "uuXP": 1e-8, "vvYP": 1e-8}, 1e-11),
-    ("eliminated", "ssor"): ({**_BASE, "uuXP": 1e-7, "vvYP": 1e-7}, 1e-11),
+    ("assembled", "ssor"): ({**_BASE, "uuXP": 1e-7, "vvYP": 1e-7}, 1e-10),
+    ("eliminated", "jacobi"): ({**_BASE, "uuXP": 1e-8, "vvYP": 1e-8}, 1e-10),
+    ("eliminated", "ssor"): ({**_BASE, "uuXP": 1e-7, "vvYP": 1e-7}, 1e-10),
 }
 _decks: dict = {}
 

@@ -314,8 +314,11 @@ def _guard(fn):
     """A sub-measurement's record, or its error: a failure there must not cost
     the headline line.  (Every rank takes the same collective steps either way:
     the sub-measurements gather only at their end.)"""
+    t0 = time.time()
     try:
-        return fn()
+        rec = fn()
+        rec["wall_s"] = round(time.time() - t0, 1)
+        return rec
     except Exception as e:  # reported in the JSON line
         import traceback
         traceback.print_exc(file=sys.stderr)
@@ -615,10 +618,11 @@ def measure_batched(args, ws, rank, dev, n_mix, smin, smax, scalars, total_steps
         g.sync()
         plain_ms += _step_ms(g.kernel_times())
         g.set_profiling(False)
-    # packing granularity and inner tolerance from the autotuner, tuned on rank
-    # 0's share and used by every rank
+    # packing of the solve and inner tolerance from the autotuner, tuned on rank
+    # 0's share and used by every rank (a given cells_per_cta selects CTA groups)
     tuning = None
     cpc, eps_inner = args.cells_per_cta, args.eps_inner
+    packing = "cta_groups" if cpc > 0 else "tile_list"
     if cpc <= 0:
         from frehdc_b200 import autotune
         if rank == 0:
@@ -626,11 +630,14 @@ def measure_batched(args, ws, rank, dev, n_mix, smin, smax, scalars, total_steps
         tuning = shard.broadcast(tuning, ws)
         cpc = tuning["best"]["cells_per_cta"]
         eps_inner = tuning["best"]["eps_inner"]
+        packing = tuning["best"]["packing"]
     if eps_inner is None:
         eps_inner = 1e-4
+    pk = native.BATCH_TILE_LIST if packing == "tile_list" else native.BATCH_CTA_GROUPS
     doms = [native.domain_from_deck(dk, device=dev, precision=prec, eps_inner=eps_inner)
             for dk in decks]
-    b = native.Batch(budget, cpc, dev)
+    b = native.Batch(budget, cpc if cpc > 0 else 1.0, dev)
+    b.set_cg_packing(pk)
     for g in doms:
         b.admit(g, 1)
     for _ in range(W):
@@ -657,7 +664,8 @@ def measure_batched(args, ws, rank, dev, n_mix, smin, smax, scalars, total_steps
     errors = None
     if precision == "mixed":
         import numpy as np
-        fb = native.Batch(budget, cpc, dev)
+        fb = native.Batch(budget, cpc if cpc > 0 else 1.0, dev)
+        fb.set_cg_packing(pk)
         for g in ref:
             fb.admit(g, W + K + 1)
         for _ in range(total_steps - W - K):
@@ -666,18 +674,39 @@ def measure_batched(args, ws, rank, dev, n_mix, smin, smax, scalars, total_steps
         for sl in list(fb.members):
             fb.release(sl)
         fb.close()
-        per = []
-        for g, r, dk in zip(doms, ref, decks):
+        # the noise floor: the same FP64 steps with the solve's sums added in the
+        # other packing's order; wet/dry branches amplify any rounding difference
+        other = native.BATCH_CTA_GROUPS if pk == native.BATCH_TILE_LIST else native.BATCH_TILE_LIST
+        alt = [native.domain_from_deck(dk, device=dev) for dk in decks]
+        ob = native.Batch(budget, 393216.0, dev)
+        ob.set_cg_packing(other)
+        for g in alt:
+            ob.admit(g, 1)
+        for _ in range(total_steps):
+            ob.step()
+        ob.sync()
+        for sl in list(ob.members):
+            ob.release(sl)
+        ob.close()
+        per, floor = [], []
+        names = ["surf", "uuXP", "vvYP"]
+        for g, r, h, dk in zip(doms, ref, alt, decks):
             n_ = dk.spec.nx * dk.spec.ny
-            names = ["surf", "uuXP", "vvYP"]
-            e = _state_errors(g.download(names), r.download(names), n_)
+            rs = r.download(names)
+            e = _state_errors(g.download(names), rs, n_)
             e["scalar_max_abs"] = max(float(np.max(np.abs(
                 g.download_scalar(s_)[:n_] - r.download_scalar(s_)[:n_])))
                 for s_ in range(1 + len(dk.tracers)))
             va, vr = g.stats()["volume"], r.stats()["volume"]
             e["volume_rel"] = abs(va - vr) / abs(vr)
             per.append(e)
-        errors = _worst(per)
+            f = _state_errors(h.download(names), rs, n_)
+            f["volume_rel"] = abs(h.stats()["volume"] - vr) / abs(vr)
+            floor.append(f)
+            h.close()
+        errors = {"mixed": _worst(per), "fp64_other_order": _worst(floor),
+                  "domains_eta_over_1e-6": sum(1 for e in per if e["eta_max_abs_m"] > 1e-6),
+                  "domains_fp64_eta_over_1e-6": sum(1 for e in floor if e["eta_max_abs_m"] > 1e-6)}
     for g in doms + ref:
         g.close()
     parts = shard.gather({"batch_ms": batch_ms, "plain_ms": plain_ms, "cells": int(sum(cells)),
@@ -695,7 +724,8 @@ def measure_batched(args, ws, rank, dev, n_mix, smin, smax, scalars, total_steps
                                   "(square or 1:4), dx 10 m, dt 1 s, depth 0.3-8 m, 0-40% dry, "
                                   "tide 0.1-0.5 m, n 0.02-0.04, 4x4 subgrid, "
                                   f"{scalars} scalar(s)",
-                      "cells": int(total_cells), "cells_per_cta": cpc,
+                      "cells": int(total_cells), "packing": packing,
+                      "cells_per_cta": cpc if packing == "cta_groups" else None,
                       "eps_inner": eps_inner if precision == "mixed" else None,
                       "sharding": "by cell count over ranks" if ws > 1 else None,
                       "deck_gen_s": round(max(p["gen_s"] for p in parts), 1)},
@@ -711,9 +741,15 @@ def measure_batched(args, ws, rank, dev, n_mix, smin, smax, scalars, total_steps
     if tuning is not None:
         rec["autotune"] = tuning
     if precision == "mixed":
-        rec["errors_vs_fp64"] = _worst([p["errors"] for p in parts])
-        if rec["errors_vs_fp64"] is not None:
-            rec["errors_vs_fp64"]["after_steps"] = total_steps
+        errs = [p["errors"] for p in parts if p["errors"]]
+        if errs:
+            rec["errors_vs_fp64"] = {**_worst([e["mixed"] for e in errs]), "after_steps": total_steps,
+                                     "domains_over_1e-6_m": sum(e["domains_eta_over_1e-6"] for e in errs)}
+            rec["fp64_vs_fp64_other_sum_order"] = {
+                **_worst([e["fp64_other_order"] for e in errs]),
+                "domains_over_1e-6_m": sum(e["domains_fp64_eta_over_1e-6"] for e in errs),
+                "note": "the same FP64 steps with the solve's partial sums added in the other "
+                        "packing's order: the spread any rounding difference grows to"}
     return rec
 
 

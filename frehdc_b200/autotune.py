@@ -1,12 +1,14 @@
-"""Autotuner of the batched form: picks the CG packing granularity
-(cells_per_cta: how many cells of a domain one CTA of its CG carries, hence how
-many CTAs each domain's solve gets and how the single-CTA domains are packed)
-and, for the mixed-precision form, the inner FP32 tolerance, by timing a few
-batch steps of the actual mix with each candidate.
+"""Autotuner of the batched form: picks the packing of the batched CG -- the
+tile list over all CTAs, or CTA groups with a granularity cells_per_cta (how
+many cells of a domain one CTA of its CG carries, hence how many CTAs each
+domain's solve gets and how the single-CTA domains are packed) -- and, for the
+mixed-precision form, the inner FP32 tolerance, by timing a few batch steps of
+the actual mix with each candidate.
 
-A domain's CG CTA count depends on its own size and cells_per_cta only, so the
-tuned value must be fixed before serving starts for results to stay
-independent of the mix; tune once on a representative mix, then serve.
+In either packing a domain's arithmetic depends on the domain alone (its own
+tile order; or its own size and cells_per_cta), so the tuned choice must be
+fixed before serving starts for results to stay independent of the mix; tune
+once on a representative mix, then serve.
 """
 from __future__ import annotations
 
@@ -38,7 +40,7 @@ def ctas_needed(sizes, cells_per_cta: float, capacity: int = 148) -> int:
 
 def time_batch(doms, cells_per_cta: float, steps: int, warmup: int, budget: int,
                precision: int = native.PRECISION_FP64, eps_inner: float = 1e-5,
-               device: int = 0) -> float:
+               device: int = 0, packing: int = native.BATCH_CTA_GROUPS) -> float:
     """Device milliseconds of `steps` batch steps of the domains (set to the
     given precision; their state advances), or None when the mix does not fit
     the batch (memory budget or CG CTA capacity)."""
@@ -47,6 +49,7 @@ def time_batch(doms, cells_per_cta: float, steps: int, warmup: int, budget: int,
         for g in doms:
             g.set_precision(precision, eps_inner)
     b = native.Batch(budget, cells_per_cta, device)
+    b.set_cg_packing(packing)
     try:
         for g in doms:
             if b.try_admit(g, 1) is None:
@@ -71,22 +74,27 @@ def time_batch(doms, cells_per_cta: float, steps: int, warmup: int, budget: int,
 def tune(decks, budget: int, precision: int = native.PRECISION_FP64, steps: int = 4,
          warmup: int = 2, cells_candidates=CELLS_PER_CTA, eps_candidates=EPS_INNER,
          device: int = 0) -> dict:
-    """The fastest (cells_per_cta, eps_inner) on this mix, and every timing.
-    Granularities whose CG would need more co-resident CTAs than the device
-    holds are skipped before any domain is built; the domains are built once
-    and stepped by every candidate in turn."""
+    """The fastest (packing, cells_per_cta, eps_inner) on this mix, and every
+    timing.  The tile-list packing takes any mix; CTA-group granularities whose
+    CG would need more co-resident CTAs than the device holds are skipped before
+    any domain is built.  The domains are built once and stepped by every
+    candidate in turn."""
     eps_list = eps_candidates if precision == native.PRECISION_MIXED else (1e-5,)
     capacity = native.Batch.capacity(device)
     sizes = [(dk.nx, dk.ny) for dk in decks]
     fits = [c for c in cells_candidates if ctas_needed(sizes, c, capacity) <= capacity]
+    cands = [("tile_list", 0.0)] + [("cta_groups", c) for c in fits]
+    packings = {"tile_list": native.BATCH_TILE_LIST, "cta_groups": native.BATCH_CTA_GROUPS}
     results = []
-    doms = [native.domain_from_deck(dk, device=device) for dk in decks] if fits else []
+    doms = [native.domain_from_deck(dk, device=device) for dk in decks]
     try:
-        for cpc, ein in itertools.product(fits, eps_list):
-            ms = time_batch(doms, cpc, steps, warmup, budget, precision, ein, device)
+        for (pk, cpc), ein in itertools.product(cands, eps_list):
+            ms = time_batch(doms, cpc if cpc > 0 else 1.0, steps, warmup, budget, precision, ein,
+                            device, packings[pk])
             if ms is None:  # the mix does not fit with this granularity
                 continue
-            results.append({"cells_per_cta": cpc, "eps_inner": ein, "ms_per_step": ms / steps})
+            results.append({"packing": pk, "cells_per_cta": cpc, "eps_inner": ein,
+                            "ms_per_step": ms / steps})
     finally:
         for g in doms:
             g.close()

@@ -6,17 +6,21 @@
 // with five launches in total, whatever the number of domains:
 //   k_explicit_batch, k_update_geo_batch, k_update_vel_batch   one block per
 //       (domain, 32 x 8 tile) entry of a tile table over all domains
-//   k_cg1_batch   one cooperative launch; each domain is solved by a group of
-//       CTAs whose size depends on the domain's own cell count only, so a
-//       domain's result does not depend on which other domains share the batch
+//   the solve, one cooperative launch over all co-resident CTAs, in one of two
+//       packings (frehd_batch_set_cg_packing):
+//     k_cg1_tiles (FREHD_BATCH_TILE_LIST, the default): the CG tiles of every
+//       domain form one list spread over all CTAs; each domain's sums are added
+//       in its own tile order, so its result does not depend on the mix
+//     k_cg1_batch (FREHD_BATCH_CTA_GROUPS): each domain solved by a group of
+//       CTAs whose size depends on the domain's own cell count only (multi-CTA
+//       groups on CTAs of their own; single-CTA domains packed onto the
+//       remaining CTAs, longest first onto the least loaded, one after another)
 //   k_finish_batch   one block per domain; flips the domain's ping-pong half
 // The five launches are captured once per batch composition into a CUDA graph
 // and replayed every step.
 //
-// Admission is by device-memory footprint (a budget given at creation) and by
-// the CTA capacity of the cooperative solve: domains solved by several CTAs get
-// CTAs of their own; domains solved by one CTA are packed onto the remaining
-// CTAs, longest first onto the least loaded (LPT), and solved one after another.
+// Admission is by device-memory footprint (a budget given at creation) and, in
+// the CTA-group packing, by the CTA capacity of the cooperative solve.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -78,7 +82,8 @@ struct frehd_batch {
   cudaStream_t stream = nullptr;
   long long budget = 0, used = 0;
   double cells_per_cta = 0;
-  int capacity = 0;  // co-resident CTAs of k_cg1_batch
+  int capacity = 0;        // co-resident CTAs of k_cg1_batch
+  int capacity_tiles = 0;  // co-resident CTAs of k_cg1_tiles
   std::vector<Slot> slots;
   bool dirty = true;
   // tables of the current composition
@@ -88,6 +93,14 @@ struct frehd_batch {
   DevArray<FinishJob> fins;
   DevArray<int> job_start;
   DevArray<CgJob> jobs;
+  // tile-list packing
+  int packing = FREHD_BATCH_TILE_LIST;
+  DevArray<BDom> bdoms;
+  DevArray<BTile> btiles;
+  DevArray<BState> bstates;
+  DevArray<double> bpartials, bpart;
+  DevArray<Scratch> bsync;
+  int nbdoms = 0, nbtiles = 0;
   long ntiles = 0;
   int nfin = 0, nctas = 0;
   // per-slot device status after each step, written by k_finish_batch into
@@ -113,8 +126,9 @@ int group_size(const frehd_batch *b, const frehd_domain *d) {
 }
 
 // CTAs the batch needs with the given domains: the multi-CTA groups plus one
-// CTA for the single-CTA domains (if any).
+// CTA for the single-CTA domains (if any); the tile-list packing takes any mix.
 int ctas_needed(const frehd_batch *b, const frehd_domain *extra) {
+  if (b->packing == FREHD_BATCH_TILE_LIST) return 1;
   int dedicated = 0, singles = 0;
   auto add = [&](const frehd_domain *d) {
     const int g = group_size(b, d);
@@ -156,11 +170,17 @@ void drop_graph(frehd_batch *b) {
 int launch_step(frehd_batch *b) {
   const dim3 bb(32, 8);
   k_explicit_batch<<<(unsigned)b->ntiles, bb, 0, b->stream>>>(b->views2.p, b->tiles.p);
-  int rc = cg1_launch_batch(b->views2.p, b->maps.p, b->job_start.p, b->jobs.p, b->nctas, b->stream);
+  const bool tl = b->packing == FREHD_BATCH_TILE_LIST;
+  int rc = tl ? cg1_launch_tiles(b->views2.p, b->maps.p, b->bdoms.p, b->bstates.p, b->btiles.p,
+                                 b->nbdoms, b->nbtiles, b->bpartials.p, b->bsync.p, b->bpart.p,
+                                 b->nctas, b->stream)
+              : cg1_launch_batch(b->views2.p, b->maps.p, b->job_start.p, b->jobs.p, b->nctas,
+                                 b->stream);
   if (rc) return rc;
-  k_update_geo_batch<<<(unsigned)b->ntiles, bb, 0, b->stream>>>(b->views2.p, b->tiles.p);
+  k_update_geo_batch<<<(unsigned)b->ntiles, bb, kGeoDynSmem, b->stream>>>(b->views2.p, b->tiles.p);
   k_update_vel_batch<<<(unsigned)b->ntiles, bb, 0, b->stream>>>(b->views2.p, b->tiles.p);
-  k_finish_batch<<<(unsigned)b->nfin, 256, 0, b->stream>>>(b->views2.p, b->fins.p);
+  k_finish_batch<<<(unsigned)b->nfin, 256, 0, b->stream>>>(b->views2.p, b->fins.p,
+                                                             tl ? b->bsync.p : nullptr);
   BATCH_TRY(cudaGetLastError());
   return FREHD_OK;
 }
@@ -204,15 +224,27 @@ int rebuild(frehd_batch *b) {
     return FREHD_OK;
   }
 
-  // CTA packing: multi-CTA groups on CTAs of their own, then single-CTA domains
-  // longest first onto the least loaded remaining CTA.
-  std::vector<std::vector<CgJob>> per_cta;
   auto flags_of = [&](int s) {
     const frehd_domain *d = b->slots[s].d;
     return (d->x0_mode == FREHD_X0_SURFACE ? 1 : 0) | (d->eliminate ? 2 : 0);
   };
+  // tile-list packing: every domain's CG tiles, domain after domain
+  std::vector<BDom> bd;
+  std::vector<BTile> bt;
+  if (b->packing == FREHD_BATCH_TILE_LIST) {
+    for (const Dom &m : doms) {
+      const frehd_domain *d = b->slots[m.slot].d;
+      const int ntx = (d->gr.nx + CTX - 1) / CTX, nty = (d->gr.ny + CTY - 1) / CTY;
+      bd.push_back(BDom{m.slot, (int)bt.size(), ntx * nty, ntx, flags_of(m.slot), 0});
+      for (int t = 0; t < ntx * nty; ++t) bt.push_back(BTile{(int)bd.size() - 1, t});
+    }
+  }
+  // CTA-group packing: multi-CTA groups on CTAs of their own, then single-CTA
+  // domains longest first onto the least loaded remaining CTA.
+  std::vector<std::vector<CgJob>> per_cta;
   std::vector<Dom> singles;
   for (const Dom &m : doms) {
+    if (b->packing == FREHD_BATCH_TILE_LIST) break;
     if (m.g > 1) {
       for (int r = 0; r < m.g; ++r) per_cta.push_back({CgJob{m.slot, r, m.g, flags_of(m.slot)}});
     } else {
@@ -220,7 +252,7 @@ int rebuild(frehd_batch *b) {
     }
   }
   const int free_ctas = b->capacity - (int)per_cta.size();
-  if (free_ctas < (singles.empty() ? 0 : 1))
+  if (b->packing != FREHD_BATCH_TILE_LIST && free_ctas < (singles.empty() ? 0 : 1))
     return fail(FREHD_ERR_STATE, "batch CTA capacity exceeded (%d CTAs for multi-CTA domains of %d)",
                 (int)per_cta.size(), b->capacity);
   if (!singles.empty()) {
@@ -251,6 +283,18 @@ int rebuild(frehd_batch *b) {
   rc = rc ? rc : b->fins.reserve(fins.size());
   rc = rc ? rc : b->job_start.reserve(start.size());
   rc = rc ? rc : b->jobs.reserve(jobs.size());
+  const bool tl = b->packing == FREHD_BATCH_TILE_LIST;
+  if (tl) {
+    const bool fresh_sync = b->bsync.cap == 0;
+    rc = rc ? rc : b->bdoms.reserve(bd.size());
+    rc = rc ? rc : b->btiles.reserve(bt.size());
+    rc = rc ? rc : b->bstates.reserve(bd.size());
+    rc = rc ? rc : b->bpartials.reserve(bt.size() * (size_t)kTilePartStride);
+    rc = rc ? rc : b->bpart.reserve(((size_t)b->capacity_tiles + 1) * kCg1PartialStride);
+    rc = rc ? rc : b->bsync.reserve(1);
+    if (!rc && fresh_sync)  // the barrier counters start at zero; k_finish_batch keeps them so
+      BATCH_TRY(cudaMemsetAsync(b->bsync.p, 0, sizeof(Scratch) * b->bsync.cap, b->stream));
+  }
   if (rc) return rc;
   BATCH_TRY(cudaMemcpyAsync(b->views2.p, views.data(), sizeof(View) * views.size(), cudaMemcpyHostToDevice, b->stream));
   BATCH_TRY(cudaMemcpyAsync(b->maps.p, maps.data(), sizeof(const Cg1Maps *) * maps.size(), cudaMemcpyHostToDevice, b->stream));
@@ -258,11 +302,17 @@ int rebuild(frehd_batch *b) {
   BATCH_TRY(cudaMemcpyAsync(b->fins.p, fins.data(), sizeof(FinishJob) * fins.size(), cudaMemcpyHostToDevice, b->stream));
   BATCH_TRY(cudaMemcpyAsync(b->job_start.p, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice, b->stream));
   BATCH_TRY(cudaMemcpyAsync(b->jobs.p, jobs.data(), sizeof(CgJob) * jobs.size(), cudaMemcpyHostToDevice, b->stream));
+  if (tl) {
+    BATCH_TRY(cudaMemcpyAsync(b->bdoms.p, bd.data(), sizeof(BDom) * bd.size(), cudaMemcpyHostToDevice, b->stream));
+    BATCH_TRY(cudaMemcpyAsync(b->btiles.p, bt.data(), sizeof(BTile) * bt.size(), cudaMemcpyHostToDevice, b->stream));
+  }
   // the host vectors go out of scope: the copies must have left them
   BATCH_TRY(cudaStreamSynchronize(b->stream));
   b->ntiles = (long)tiles.size();
   b->nfin = (int)fins.size();
-  b->nctas = (int)per_cta.size();
+  b->nctas = tl ? b->capacity_tiles : (int)per_cta.size();
+  b->nbdoms = (int)bd.size();
+  b->nbtiles = (int)bt.size();
   b->dirty = false;
   return FREHD_OK;
 }
@@ -331,7 +381,10 @@ extern "C" int frehd_batch_create(int device, long long hbm_budget_bytes, double
   b->device = device;
   b->budget = hbm_budget_bytes;
   b->cells_per_cta = cells_per_cta;
-  int rc = cg1_batch_capacity(device, &b->capacity);
+  int rc = geo_kernels_setup() == cudaSuccess ? FREHD_OK
+                                              : fail(FREHD_ERR_CUDA, "k_update_geo shared memory attribute");
+  if (!rc) rc = cg1_batch_capacity(device, &b->capacity);
+  if (!rc) rc = cg1_tiles_capacity(device, &b->capacity_tiles);
   if (!rc && cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
     rc = fail(FREHD_ERR_CUDA, "stream creation failed");
   if (rc) {
@@ -361,6 +414,12 @@ extern "C" int frehd_batch_destroy(frehd_batch *b) {
   b->fins.release();
   b->job_start.release();
   b->jobs.release();
+  b->bdoms.release();
+  b->btiles.release();
+  b->bstates.release();
+  b->bpartials.release();
+  b->bpart.release();
+  b->bsync.release();
   if (b->stream) cudaStreamDestroy(b->stream);
   delete b;
   return FREHD_OK;
@@ -462,7 +521,7 @@ extern "C" int frehd_batch_info(frehd_batch *b, frehd_batch_info_t *out) {
   for (const Slot &s : b->slots) n += s.d != nullptr;
   out->domains = n;
   out->cg_ctas = b->nctas;
-  out->cg_capacity = b->capacity;
+  out->cg_capacity = b->packing == FREHD_BATCH_TILE_LIST ? b->capacity_tiles : b->capacity;
   out->tiles = b->ntiles;
   out->graph = b->graph_live;
   out->bytes_used = b->used;
@@ -474,6 +533,24 @@ extern "C" int frehd_batch_info(frehd_batch *b, frehd_batch_info_t *out) {
 extern "C" int frehd_batch_stream(frehd_batch *b, void **stream) {
   if (!b || !stream) return fail(FREHD_ERR_INVALID, "null argument");
   *stream = b->stream;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_batch_set_cg_packing(frehd_batch *b, int packing) {
+  if (!b || (packing != FREHD_BATCH_TILE_LIST && packing != FREHD_BATCH_CTA_GROUPS))
+    return fail(FREHD_ERR_INVALID, "bad argument");
+  BATCH_TRY(cudaSetDevice(b->device));
+  BATCH_TRY(cudaStreamSynchronize(b->stream));  // queued steps use the current tables
+  if (packing == FREHD_BATCH_CTA_GROUPS && b->packing != packing) {
+    b->packing = packing;
+    if (ctas_needed(b, nullptr) > b->capacity) {
+      b->packing = FREHD_BATCH_TILE_LIST;
+      return fail(FREHD_ERR_NOMEM, "batch CTA capacity: the admitted domains need %d CTAs in groups",
+                  ctas_needed(b, nullptr));
+    }
+  }
+  b->packing = packing;
+  b->dirty = true;
   return FREHD_OK;
 }
 

@@ -99,6 +99,7 @@ View make_view_at(const frehd_domain *d, int cur) {
   w.inflow = d->inflow; w.ninflow = d->ninflow;
   w.wspd = d->wspd; w.nwspd = d->nwspd; w.wcos = d->wcos; w.wsin = d->wsin; w.nwdir = d->nwdir;
   w.dXP = d->dXP; w.dYP = d->dYP;
+  w.zf_map = d->zf_map_dev;
   w.sc = d->sc;
   return w;
 }
@@ -221,7 +222,7 @@ void mark(cudaEvent_t *ev, int slot, cudaStream_t st) {
 int launch_update(frehd_domain *d, const View &w, cudaEvent_t *ev = nullptr) {
   const dim3 gb = tile_grid(d), bb(32, 8);
   mark(ev, 2, d->stream);
-  k_update_geo<<<gb, bb, 0, d->stream>>>(w);
+  k_update_geo<<<gb, bb, kGeoDynSmem, d->stream>>>(w);
   mark(ev, 3, d->stream);
   if (d->p.scalarAdv == 2)
     k_update_vel_tvd<<<gb, bb, 0, d->stream>>>(w);
@@ -262,6 +263,11 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
   frehd_domain *d = new frehd_domain();
   d->cfg = *cfg;
   d->device = device;
+  if (geo_kernels_setup() != cudaSuccess) {
+    cudaGetLastError();
+    delete d;
+    return fail(FREHD_ERR_CUDA, "k_update_geo shared memory attribute");
+  }
   if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete d;
     return fail(FREHD_ERR_CUDA, "cudaStreamCreate failed");
@@ -366,6 +372,7 @@ extern "C" int frehd_domain_destroy(frehd_domain *d) {
   for (void *p : d->allocs) cudaFree(p);
   if (d->tables) cudaFree(d->tables);
   if (d->zf) cudaFree(d->zf);
+  if (d->zf_map_dev) cudaFree(d->zf_map_dev);
   if (d->tide) cudaFree(d->tide);
   for (double *a : {d->inflow, d->wspd, d->wcos, d->wsin})
     if (a) cudaFree(a);
@@ -425,6 +432,19 @@ extern "C" int frehd_domain_set_fine_bottoms_ex(frehd_domain *d, int r, const do
   d->p.fpitch = cols;
   d->p.r = r;
   d->p.check_block = check_block;
+  if (d->zf_map_dev) cudaFree(d->zf_map_dev);
+  d->zf_map_dev = nullptr;
+  if (r == 4 && !check_block) {  // the r = 4 path stages fine-bottom windows by TMA
+    CUtensorMap m;
+    int rc = encode_fine_box(d->zf, cols, rows, &m);
+    if (!rc && cudaMalloc(&d->zf_map_dev, sizeof(CUtensorMap)) != cudaSuccess) {
+      cudaGetLastError();
+      d->zf_map_dev = nullptr;
+      rc = fail(FREHD_ERR_NOMEM, "fine-bottom tensor map");
+    }
+    if (rc) return rc;
+    CUDA_TRY(cudaMemcpyAsync(d->zf_map_dev, &m, sizeof(m), cudaMemcpyHostToDevice, d->stream));
+  }
   d->geom_set = 1;
   return FREHD_OK;
 }
@@ -825,11 +845,15 @@ extern "C" int frehd_domain_init(frehd_domain *d, const double *bottom, const do
   st.depth = dep.data(); st.CDXP = cdx.data(); st.CDYP = cdy.data();
   st.bottomZ = bz.data(); st.bottomXP = bx.data(); st.bottomYP = by.data(); st.ind = ind.data();
   st.depthXP = hx.data(); st.depthYP = hy.data();  // held for the wind term only
+  // no previous step: the advection limiter's CFL numbers start at zero (the
+  // reference reads its never-written arrays), also on a domain set up again
+  std::vector<double> zeros(T, 0.0);
+  st.CFLx = zeros.data(); st.CFLy = zeros.data();
   int rc = frehd_domain_upload_state(d, &st);
   if (rc) return rc;
   {
     View w = make_view(d);
-    k_update_geo_init<<<tile_grid(d), dim3(32, 8), 0, d->stream>>>(w);
+    k_update_geo_init<<<tile_grid(d), dim3(32, 8), kGeoDynSmem, d->stream>>>(w);
     CUDA_TRY(cudaGetLastError());
     std::swap(d->ind[0], d->ind[1]);  // the evaluated indices become current
   }

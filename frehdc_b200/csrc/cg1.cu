@@ -57,6 +57,7 @@
 
 #include "cg1.h"
 #include "cg_common.cuh"
+#include "tma.cuh"
 #include "frehd_internal.h"
 
 namespace frehd {
@@ -114,51 +115,6 @@ template <>
 struct Pair<float> {
   using type = float2;
 };
-
-__device__ __forceinline__ unsigned smem_u32(const void *p) {
-  return (unsigned)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_test(unsigned long long *bar, unsigned parity) {
-  unsigned ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Wait for the phase `parity` of `bar` to complete, for at most `limit_ns`.
-__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity,
-                                          unsigned long long limit_ns) {
-  if (mbar_test(bar, parity)) return true;
-  const unsigned long long t0 = gtimer_ns();
-  while (!mbar_test(bar, parity)) {
-    if (gtimer_ns() - t0 > limit_ns) return false;
-  }
-  return true;
-}
-
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map,
-                                            unsigned long long *bar, int x, int y) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<unsigned long long>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
-      : "memory");
-}
 
 // Shared-memory arrays of one stage.
 template <typename T>
@@ -366,11 +322,6 @@ __device__ __forceinline__ double first_delta(const T *V, const T *HXg, const T 
   return d0;
 }
 
-__device__ __forceinline__ void acquire_maps(const CUtensorMap *maps, int n) {
-  // the maps were written to global memory by a host copy: make them visible to the TMA unit
-  for (int q = 0; q < n; ++q)
-    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(maps + q) : "memory");
-}
 
 }  // namespace
 
@@ -835,6 +786,758 @@ __global__ void __launch_bounds__(kCgThreads, kCg1MinBlocks)
   }
 }
 
+// ================================================================ batched solve, one tile list
+//
+// Every domain of a batch is solved by one cooperative launch of all co-resident
+// CTAs.  The domains' CG tiles form one list (domain after domain, each in its
+// own tile order) and CTA c works on entries c, c + C, c + 2C, ... (C CTAs), so
+// that every domain's work, large or small, is spread over the whole GPU.  The
+// solve runs in rounds: in a round every tile takes one step of its domain's
+// state machine (a set-up pass, one CG sweep, the final scaling; or the mixed
+// form's residual, inner sweep and correction passes), and writes the sums that
+// step needs to the tile's own slot of `part`; after a grid barrier, domain k's
+// slots are added up in tile order by CTA k mod C, which advances the domain's
+// state (the scalars of the next sweep, convergence, the stall and precision
+// fall-backs); a second barrier publishes the states.  A domain's arithmetic
+// thus depends on its own tiles only: its result is the same alone, in any mix
+// and for any number of CTAs.  The steps are those of cg1_fp64 and cg1_mixed
+// (same passes, same stopping rules, same fall-backs); only the order in which
+// the partial sums are added differs.
+// Arguments of k_cg1_tiles (the host's tables of the batch composition).
+struct TilesArgs {
+  const View *views2;
+  const Cg1Maps *const *maps;
+  const BDom *doms;
+  BState *states;
+  const BTile *tiles;
+  int ndom, ntiles;
+  double *part;
+  Scratch *bsync;
+  double *bpart;
+};
+
+namespace {
+
+enum : int {
+  kPhSetup1 = 0, kPhSetup2, kPhDelta0, kPhSweep, kPhFinal,
+  kPhMSetup, kPhMResid, kPhMDelta0, kPhMSweep, kPhMXupd, kPhDone
+};
+constexpr int kMaxAcqDomains = 4096;  // domains whose tensor maps a CTA tracks as acquired
+constexpr int kTlMaxDoms = 512;       // domains whose round parameters a CTA keeps in shared memory
+constexpr int kTlMaxLocal = 1024;     // a CTA's list entries kept in shared memory
+
+// What a tile of domain k needs in a round: its state's phase and sweep
+// scalars, and the domain's place (copied to shared memory at each round's start).
+struct TlDom {
+  double alpha, beta;
+  int phase, cur, vpar, elim, slot, ntx, ntiles, flags;
+};
+constexpr unsigned kStageStride = kSmemStages / 2;  // one stage of either element type
+
+// A domain's state as published by the last round (L2: written by another CTA).
+__device__ __forceinline__ BState load_state(const BState *p) {
+  static_assert(sizeof(BState) % 8 == 0, "BState is copied in 8-byte words");
+  BState st;
+  const unsigned long long *src = reinterpret_cast<const unsigned long long *>(p);
+  unsigned long long *dst = reinterpret_cast<unsigned long long *>(&st);
+#pragma unroll
+  for (int q = 0; q < (int)(sizeof(BState) / 8); ++q) dst[q] = __ldcg(src + q);
+  return st;
+}
+__device__ __forceinline__ int load_phase(const BState *p) { return __ldcg(&p->phase); }
+
+__device__ __forceinline__ bool is_sweep(int ph) { return ph == kPhSweep || ph == kPhMSweep; }
+
+// sums a phase's tiles produce
+__device__ __forceinline__ int phase_sums(int ph) {
+  switch (ph) {
+    case kPhSetup2: case kPhMResid: return 3;
+    case kPhDelta0: case kPhMDelta0: return 1;
+    case kPhSweep: case kPhMSweep: return 6;
+    default: return 0;
+  }
+}
+
+// A~ v at padded index k read from global memory: apply() on the arrays
+// themselves (zeros outside the interior), the same products and order.
+template <typename T>
+__device__ __forceinline__ T apply_g(const T *V, const T *HX, const T *HY, long k, long pitch) {
+  const T he = __ldcg(HX + k);
+  const T off = fabs(he) * __ldcg(V + k + 1) + fabs(__ldcg(HX + k - 1)) * __ldcg(V + k - 1) +
+                __ldcg(HY + k) * __ldcg(V + k + pitch) + __ldcg(HY + k - pitch) * __ldcg(V + k - pitch);
+  return signbit(he) ? __ldcg(V + k) : __ldcg(V + k) - off;
+}
+
+// ---- plain passes of one tile (cg1_fp64 / cg1_mixed, per tile)
+__device__ __forceinline__ void t_setup1(const View &w, int i0, int j0, int elim, int x0s) {
+  const Grid g = w.gr;
+  const long pitch = g.pitch;
+  const int tx = threadIdx.x & 31, j = j0 + (threadIdx.x >> 5);
+  const double *Ct = w.Ct, *Gx = w.Gx, *Gy = w.Gy;
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) {
+    const int i = i0 + c * 32 + tx;
+    if (i < g.nx && j < g.ny) {
+      const long k = g.at(i, j);
+      const double ct = Ct[k], ce = Ct[k + 1], cn = Ct[k + pitch];
+      const double d = sqrt(fabs(ct));
+      double hx = Gx[k] / (d * sqrt(fabs(ce))), hy = Gy[k] / (d * sqrt(fabs(cn)));
+      if (elim) {
+        if (!(ct > 0 && ce > 0)) hx = 0.0;
+        if (!(ct > 0 && cn > 0)) hy = 0.0;
+      }
+      w.Hx[k] = ct < 0 ? -fabs(hx) : fabs(hx);
+      w.Hy[k] = hy;
+      w.x[k] = x0s ? d * w.surf_cur[k] : 0.0;
+      w.p0[k] = 0.0;
+    }
+  }
+}
+
+__device__ __forceinline__ void t_setup2(const View &w, int i0, int j0, int elim, int x0s,
+                                         double (&acc)[6]) {
+  const Grid g = w.gr;
+  const long pitch = g.pitch;
+  const int tx = threadIdx.x & 31, j = j0 + (threadIdx.x >> 5);
+  const double *Ct = w.Ct, *Gx = w.Gx, *Gy = w.Gy;
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) {
+    const int i = i0 + c * 32 + tx;
+    if (i < g.nx && j < g.ny) {
+      const long k = g.at(i, j);
+      const double ct = Ct[k], bk = w.b[k];
+      auto x0 = [&](long kk) -> double { return x0s ? w.surf_cur[kk] : 0.0; };
+      auto xv = [&](long kk) -> double {
+        const double cc = Ct[kk];
+        return (elim && cc < 0) ? w.b[kk] / (-cc) : x0(kk);
+      };
+      double r;
+      if (ct > 0) {
+        const double ax = ct * x0(k) - (Gx[k] * xv(k + 1) + Gx[k - 1] * xv(k - 1) +
+                                        Gy[k] * xv(k + pitch) + Gy[k - pitch] * xv(k - pitch));
+        r = bk - ax;
+      } else {
+        r = bk - (-ct) * x0(k);
+      }
+      const double rs = r / sqrt(fabs(ct));
+      acc[0] += rs * rs;
+      acc[1] += r * r;
+      acc[2] += bk * bk;
+      w.r[k] = rs;
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void t_delta0(const Grid &g, const T *V, const T *HX, const T *HY, int i0,
+                                         int j0, double (&acc)[6]) {
+  const int tx = threadIdx.x & 31, j = j0 + (threadIdx.x >> 5);
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) {
+    const int i = i0 + c * 32 + tx;
+    if (i < g.nx && j < g.ny) {
+      const long k = g.at(i, j);
+      acc[0] += (double)apply_g<T>(V, HX, HY, k, g.pitch) * (double)__ldcg(V + k);
+    }
+  }
+}
+
+__device__ __forceinline__ void t_final(const View &w, int i0, int j0) {
+  const Grid g = w.gr;
+  const int tx = threadIdx.x & 31, j = j0 + (threadIdx.x >> 5);
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) {
+    const int i = i0 + c * 32 + tx;
+    if (i < g.nx && j < g.ny) {
+      const long k = g.at(i, j);
+      w.x[k] = w.x[k] / sqrt(fabs(w.Ct[k]));
+    }
+  }
+}
+
+__device__ __forceinline__ void t_msetup(const View &w, int i0, int j0, int elim, int x0s) {
+  const Grid g = w.gr;
+  const long pitch = g.pitch;
+  const int tx = threadIdx.x & 31, j = j0 + (threadIdx.x >> 5);
+  const double *Ct = w.Ct, *Gx = w.Gx, *Gy = w.Gy;
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) {
+    const int i = i0 + c * 32 + tx;
+    if (i < g.nx && j < g.ny) {
+      const long k = g.at(i, j);
+      const double ct = Ct[k], ce = Ct[k + 1], cn = Ct[k + pitch];
+      const double d = sqrt(fabs(ct));
+      double hx = Gx[k] / (d * sqrt(fabs(ce))), hy = Gy[k] / (d * sqrt(fabs(cn)));
+      if (elim) {
+        if (!(ct > 0 && ce > 0)) hx = 0.0;
+        if (!(ct > 0 && cn > 0)) hy = 0.0;
+      }
+      const float hxf = fabsf((float)hx);
+      w.fhx[k] = ct < 0 ? -hxf : hxf;
+      w.fhy[k] = (float)hy;
+      w.x[k] = x0s ? w.surf_cur[k] : 0.0;
+    }
+  }
+}
+
+__device__ __forceinline__ void t_mresid(const View &w, int i0, int j0, int elim, double (&acc)[6]) {
+  const Grid g = w.gr;
+  const long pitch = g.pitch;
+  const int tx = threadIdx.x & 31, j = j0 + (threadIdx.x >> 5);
+  const double *Ct = w.Ct, *Gx = w.Gx, *Gy = w.Gy;
+  double *const X = w.x;
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) {
+    const int i = i0 + c * 32 + tx;
+    if (i < g.nx && j < g.ny) {
+      const long k = g.at(i, j);
+      const double ct = Ct[k], bk = w.b[k];
+      auto xv = [&](long kk) -> double {
+        const double cc = Ct[kk];
+        return (elim && cc < 0) ? w.b[kk] / (-cc) : __ldcg(X + kk);
+      };
+      double r;
+      if (ct > 0) {
+        const double ax = ct * __ldcg(X + k) - (Gx[k] * xv(k + 1) + Gx[k - 1] * xv(k - 1) +
+                                                Gy[k] * xv(k + pitch) + Gy[k - pitch] * xv(k - pitch));
+        r = bk - ax;
+      } else {
+        r = bk - (-ct) * __ldcg(X + k);
+      }
+      const float rs = (float)(r / sqrt(fabs(ct)));
+      acc[0] += (double)rs * (double)rs;
+      acc[1] += r * r;
+      acc[2] += bk * bk;
+      w.fr0[k] = rs;
+      w.fp0[k] = 0.0f;
+      w.fd[k] = 0.0f;
+    }
+  }
+}
+
+__device__ __forceinline__ void t_xupd(const View &w, int i0, int j0) {
+  const Grid g = w.gr;
+  const int tx = threadIdx.x & 31, j = j0 + (threadIdx.x >> 5);
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) {
+    const int i = i0 + c * 32 + tx;
+    if (i < g.nx && j < g.ny) {
+      const long k = g.at(i, j);
+      w.x[k] = w.x[k] + (double)__ldcg(w.fd + k) / sqrt(fabs(w.Ct[k]));
+    }
+  }
+}
+
+// One CG sweep of one tile whose boxes are in stage `s` (sweep()'s passes A-C):
+// p = r~ + beta p_old, s = A~ p, r~' = r~ - alpha s, w = A~ r~', X += alpha p;
+// r~' and p stored to rn_out / pn_out; red gets the tile's six sums.
+template <typename T, bool kUnscaled, typename XT>
+__device__ __forceinline__ void sweep_tile(const Stage<T> &s, const Grid &g, int i0, int j0,
+                                           const XT (&xs)[CPT], const double (&ds)[CPT], XT *X,
+                                           T *rn_out, T *pn_out, T alpha, T beta, double (&red)[6]) {
+  using B = Box<T>;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int j = j0 + ty;
+  {
+    using P2 = typename Pair<T>::type;
+    P2 *pp = reinterpret_cast<P2 *>(s.P);
+    const P2 *rp = reinterpret_cast<const P2 *>(s.R);
+#pragma unroll
+    for (int e = threadIdx.x; e < B::kBox / 2; e += kCgThreads) {
+      const P2 rv = rp[e];
+      P2 pv = pp[e];
+      pv.x = rv.x + beta * pv.x;
+      pv.y = rv.y + beta * pv.y;
+      pp[e] = pv;
+    }
+  }
+  __syncthreads();
+  {
+    T rb[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int q = B::q(c * 32 + tx, ty);
+      const T sv = apply<T>(s.P, s.HX, s.HY, q);
+      rb[c] = s.R[q] - alpha * sv;
+      if (i0 + c * 32 + tx < g.nx && j < g.ny) {
+        red[2] += (double)rb[c] * (double)sv;
+        red[4] += (double)s.P[q] * (double)sv;
+      }
+    }
+    T rring[kRingPer];
+    int qr[kRingPer];
+#pragma unroll
+    for (int t = 0; t < kRingPer; ++t) {
+      const int e = threadIdx.x + t * kCgThreads;
+      qr[t] = e < kRing ? B::ring(e) : 0;
+      rring[t] = e < kRing ? s.R[qr[t]] - alpha * apply<T>(s.P, s.HX, s.HY, qr[t]) : T(0);
+    }
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) s.R[B::q(c * 32 + tx, ty)] = rb[c];
+#pragma unroll
+    for (int t = 0; t < kRingPer; ++t)
+      if (threadIdx.x + t * kCgThreads < kRing) s.R[qr[t]] = rring[t];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) {
+    const int i = i0 + c * 32 + tx;
+    if (i < g.nx && j < g.ny) {
+      const int q = B::q(c * 32 + tx, ty);
+      const T u = s.R[q], pc = s.P[q];
+      const T wv = apply<T>(s.R, s.HX, s.HY, q);
+      const double ud = u;
+      red[0] += ud * ud;
+      red[1] += (double)wv * ud;
+      red[3] += (double)pc * (double)wv;
+      red[5] += kUnscaled ? ds[c] * (ud * ud) : ud * ud;
+      const long k = g.at(i, j);
+      X[k] = xs[c] + alpha * pc;
+      rn_out[k] = u;
+      pn_out[k] = pc;
+    }
+  }
+}
+
+__device__ __forceinline__ const View &tile_view(const TilesArgs &a, const BDom &dm, int vpar) {
+  return a.views2[2 * dm.slot + vpar];
+}
+
+// Mark every domain of the launch failed (a wait that gave up strands them all).
+__device__ __forceinline__ void fail_all(const TilesArgs &a, int code) {
+  if (threadIdx.x != 0) return;
+  for (int k = 0; k < a.ndom; ++k) set_status(a.views2[2 * a.doms[k].slot].sc, code);
+}
+
+// The round parameters of domain k from its published state.
+__device__ __forceinline__ TlDom load_tldom(const TilesArgs &a, int k) {
+  const BState st = load_state(a.states + k);
+  const BDom dm = a.doms[k];
+  TlDom t;
+  t.alpha = st.alpha;
+  t.beta = st.beta;
+  t.phase = st.phase;
+  t.cur = st.cur;
+  t.vpar = st.vpar;
+  t.elim = st.elim;
+  t.slot = dm.slot;
+  t.ntx = dm.ntx;
+  t.ntiles = dm.ntiles;
+  t.flags = dm.flags;
+  return t;
+}
+
+// The CTA's shared copies: round parameters of the first kTlMaxDoms domains and
+// its first kTlMaxLocal list entries; the rest is read from global memory.
+struct TlCache {
+  const TlDom *dom;
+  const BTile *loc;
+  __device__ __forceinline__ TlDom get_dom(const TilesArgs &a, int k) const {
+    return k < kTlMaxDoms ? dom[k] : load_tldom(a, k);
+  }
+  __device__ __forceinline__ BTile get_tile(const TilesArgs &a, int idx, unsigned c, unsigned C) const {
+    return idx < kTlMaxLocal ? loc[idx] : a.tiles[(long)c + (long)idx * C];
+  }
+};
+
+// Issue the boxes of the sweep tile (list entry t of domain parameters dm) into
+// stage buffer `stage` (thread 0).
+__device__ __forceinline__ void issue_sweep(const TilesArgs &a, const BTile &t, const TlDom &dm,
+                                            unsigned char *stage, unsigned long long *bar,
+                                            unsigned *acq) {
+  const Cg1Maps *m = a.maps[dm.slot];
+  const bool fp32 = dm.phase == kPhMSweep;
+  // the maps were written by host copies: acquire them once per domain and precision
+  const int bit = 2 * t.dom + (fp32 ? 1 : 0);
+  if (t.dom >= kMaxAcqDomains || !((acq[bit >> 5] >> (bit & 31)) & 1u)) {
+    acquire_maps(fp32 ? &m->fr[0] : &m->r[0], 6);
+    if (t.dom < kMaxAcqDomains) acq[bit >> 5] |= 1u << (bit & 31);
+  }
+  TileIt ti;
+  ti.ntx = dm.ntx;
+  ti.ntiles = dm.ntiles;
+  ti.nty = dm.ntiles / dm.ntx;
+  if (fp32) {
+    const SweepMaps sm{&m->fr[dm.cur], &m->fp[dm.cur], &m->fhx, &m->fhy};
+    issue_tile<float>(sm, ti, t.tile, stage, bar);
+  } else {
+    const SweepMaps sm{&m->r[dm.cur], &m->p[dm.cur], &m->hx, &m->hy};
+    issue_tile<double>(sm, ti, t.tile, stage, bar);
+  }
+}
+
+// The CTA's next local list index at or after idx whose domain sweeps this round
+// (n: the CTA's entry count).
+__device__ __forceinline__ int next_sweep(const TilesArgs &a, const TlCache &tc, int idx, int n,
+                                          unsigned c, unsigned C) {
+  for (; idx < n; ++idx)
+    if (is_sweep(tc.get_dom(a, tc.get_tile(a, idx, c, C).dom).phase)) return idx;
+  return n;
+}
+
+// Advance domain k's state after its sums `tot` of this round (thread 0).
+__device__ void advance(const TilesArgs &a, int k, BState &st, const double (&tot)[6]) {
+  const BDom dm = a.doms[k];
+  const View &w = tile_view(a, dm, st.vpar);
+  const Params &p = w.p;
+  Scratch *sc = w.sc;
+  auto converged = [&](double rr_, double bn) {
+    const double rn = sqrt(rr_);
+    return rn < p.eps * bn || (bn == 0.0 && 1.0 + rn == 1.0);
+  };
+  auto finish = [&](int iters, int fallback, int noconv) {
+    sc->cg_iters = iters;
+    sc->cg_fallback = fallback;
+    sc->cg_noconv = noconv;
+    sc->cg_rr = st.rr;
+    sc->cg_bb = st.bnorm * st.bnorm;
+    st.phase = kPhDone;
+    atomicAdd(&a.bsync->n_done, 1);
+  };
+  // the next FP64 sweep, or the end of the solve (cg1_fp64's loop condition)
+  auto next_fp64 = [&]() {
+    if (!converged(st.rr, st.bnorm) && st.it < p.maxIter) {
+      st.beta = st.it == 0 ? 0.0 : st.gamma / st.gamma_old;
+      st.alpha = st.gamma / (st.delta + st.beta * (st.e1 + st.e2) + st.beta * st.beta * st.e3);
+      ++st.it;
+      st.phase = kPhSweep;
+    } else {
+      st.it_all += st.it;
+      st.noconv = !converged(st.rr, st.bnorm);
+      st.phase = kPhFinal;
+    }
+  };
+  // the next FP32 inner sweep, or the correction pass (cg1_mixed's inner loop)
+  auto next_inner = [&]() {
+    if (st.gamma > st.stop && st.it < p.maxIter) {
+      st.beta = st.it == 0 ? 0.0 : st.gamma / st.gamma_old;
+      st.alpha = st.gamma / (st.delta + st.beta * (st.e1 + st.e2) + st.beta * st.beta * st.e3);
+      ++st.it;
+      st.phase = kPhMSweep;
+    } else {
+      st.it_all += st.it;
+      st.phase = kPhMXupd;
+    }
+  };
+  // the mixed refinement hands the solve to the FP64 path (cg1_solve)
+  auto take_over = [&]() {
+    st.takeover = 1;
+    st.attempt = 0;
+    st.elim = (dm.flags >> 1) & 1;
+    st.it_all = 0;
+    st.fallback = 0;
+    st.phase = kPhSetup1;
+  };
+  switch (st.phase) {
+    case kPhSetup1:
+      st.phase = kPhSetup2;
+      break;
+    case kPhSetup2:
+      st.gamma = tot[0];
+      st.rr = tot[1];
+      st.bnorm = sqrt(tot[2]);
+      st.phase = kPhDelta0;
+      break;
+    case kPhDelta0:
+      st.delta = tot[0];
+      st.gamma_old = 1.0;
+      st.e1 = st.e2 = st.e3 = 0.0;
+      st.best = st.rr;
+      st.best_it = 0;
+      st.cur = 0;
+      st.it = 0;
+      next_fp64();
+      break;
+    case kPhSweep:
+      st.gamma_old = st.gamma;
+      st.gamma = tot[0];
+      st.delta = tot[1];
+      st.e1 = tot[2];
+      st.e2 = tot[3];
+      st.e3 = tot[4];
+      st.rr = tot[5];
+      st.cur ^= 1;
+      if (st.rr < 0.25 * st.best) {
+        st.best = st.rr;
+        st.best_it = st.it;
+      } else if (!st.elim && st.it - st.best_it >= kStallIters) {
+        // stalled on the assembled matrix: start again in the eliminated form
+        st.it_all += st.it;
+        st.attempt += 1;
+        st.elim = 1;
+        st.fallback = 1;
+        st.phase = kPhSetup1;
+        break;
+      }
+      next_fp64();
+      break;
+    case kPhFinal:
+      finish(st.it_all, st.takeover ? 2 : st.fallback, st.noconv);
+      break;
+    case kPhMSetup:
+      st.outer = 0;
+      st.phase = kPhMResid;
+      break;
+    case kPhMResid:
+      st.rr = tot[1];
+      if (st.outer == 0) st.bnorm = sqrt(tot[2]);
+      if (converged(st.rr, st.bnorm)) {
+        finish(st.it_all, 0, 0);
+      } else if (st.outer > 0 && st.rr > 1e-2 * st.rr_prev) {
+        take_over();  // no tenfold gain
+      } else {
+        st.rr_prev = st.rr;
+        st.gamma = tot[0];  // g0 of the inner solve
+        st.stop = p.eps_inner * p.eps_inner * tot[0];
+        st.phase = kPhMDelta0;
+      }
+      break;
+    case kPhMDelta0:
+      st.delta = tot[0];
+      st.gamma_old = 1.0;
+      st.e1 = st.e2 = st.e3 = 0.0;
+      st.cur = 0;
+      st.it = 0;
+      next_inner();
+      break;
+    case kPhMSweep:
+      st.gamma_old = st.gamma;
+      st.gamma = tot[0];
+      st.delta = tot[1];
+      st.e1 = tot[2];
+      st.e2 = tot[3];
+      st.e3 = tot[4];
+      st.cur ^= 1;
+      next_inner();
+      break;
+    case kPhMXupd:
+      st.outer += 1;
+      if (st.outer < kMaxOuter) st.phase = kPhMResid;
+      else take_over();
+      break;
+    default:
+      break;
+  }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kCgThreads, kCg1MinBlocks) k_cg1_tiles(TilesArgs a) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ double sh_red[2][6][NWARP];
+  __shared__ unsigned s_acq[2 * kMaxAcqDomains / 32];
+  __shared__ TlDom s_dom[kTlMaxDoms];
+  __shared__ BTile s_loc[kTlMaxLocal];
+  __shared__ int s_ok, s_next;
+  unsigned char *smem;
+  unsigned long long *bars;
+  const unsigned C = gridDim.x, c = blockIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (!cg1_smem(smem_raw, &smem, &bars)) {  // every CTA alike: nobody reaches a barrier
+    if (c == 0) fail_all(a, FREHD_ERR_CUDA);
+    return;
+  }
+  const TlCache tc{s_dom, s_loc};
+  // this CTA's list entries: c, c + C, c + 2C, ...
+  const int nloc = a.ntiles > (int)c ? (a.ntiles - (int)c + (int)C - 1) / (int)C : 0;
+  for (int q = threadIdx.x; q < 2 * kMaxAcqDomains / 32; q += blockDim.x) s_acq[q] = 0;
+  for (int q = threadIdx.x; q < nloc && q < kTlMaxLocal; q += blockDim.x)
+    s_loc[q] = a.tiles[(long)c + (long)q * C];
+  // ---- prologue: each CTA starts the solves of its domains
+  if (threadIdx.x == 0) {
+    for (int k = (int)c; k < a.ndom; k += (int)C) {
+      const BDom dm = a.doms[k];
+      Scratch *sc = a.views2[2 * dm.slot].sc;
+      BState st;
+      memset(&st, 0, sizeof(st));
+      st.vpar = *(volatile int *)&sc->cur & 1;
+      const View &w = a.views2[2 * dm.slot + st.vpar];
+      st.elim = (dm.flags >> 1) & 1;
+      if (*(volatile int *)&sc->status != FREHD_OK || (reinterpret_cast<unsigned long long>(a.maps[dm.slot]) & 63ull)) {
+        if (*(volatile int *)&sc->status == FREHD_OK) set_status(sc, FREHD_ERR_CUDA);
+        st.phase = kPhDone;
+        atomicAdd(&a.bsync->n_done, 1);
+      } else if (test_skip_barrier(sc, 0)) {  // the test hook of frehd_domain_set_wait_test
+        set_status(sc, FREHD_ERR_TIMEOUT);
+        st.phase = kPhDone;
+        atomicAdd(&a.bsync->n_done, 1);
+      } else {
+        st.phase = w.p.mixed ? kPhMSetup : kPhSetup1;
+      }
+      a.states[k] = st;
+    }
+  }
+  {
+    double none[1] = {0};
+    if (!grid_allreduce<1, kRedStride>(none, a.bsync, a.bpart, a.bpart + kRedStride * (long)C, C, c)) {
+      fail_all(a, FREHD_ERR_TIMEOUT);
+      return;
+    }
+  }
+  unsigned seq = 0;
+  int rbuf = 0;
+  for (;;) {
+    // ---- this round's parameters of every domain, then one step of every tile
+    for (int k = threadIdx.x; k < a.ndom && k < kTlMaxDoms; k += blockDim.x) s_dom[k] = load_tldom(a, k);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("fence.proxy.async.global;" ::: "memory");
+      s_next = next_sweep(a, tc, 0, nloc, c, C);
+      if (s_next < nloc) {
+        const BTile t = tc.get_tile(a, s_next, c, C);
+        issue_sweep(a, t, tc.get_dom(a, t.dom), smem + (seq & 1) * kStageStride, &bars[seq & 1], s_acq);
+      }
+    }
+    __syncthreads();
+    for (int idx = 0; idx < nloc; ++idx) {
+      const long g = (long)c + (long)idx * C;
+      const BTile t = tc.get_tile(a, idx, c, C);
+      const TlDom dm = tc.get_dom(a, t.dom);  // the same in every thread this round
+      const int ph = dm.phase;
+      if (ph == kPhDone) continue;
+      const View &w = a.views2[2 * dm.slot + dm.vpar];
+      const int i0 = (t.tile % dm.ntx) * CTX, j0 = (t.tile / dm.ntx) * CTY;
+      double acc[6] = {0, 0, 0, 0, 0, 0};
+      const int nv = phase_sums(ph);
+      if (is_sweep(ph)) {
+        const int st_idx = seq & 1;
+        unsigned char *stage = smem + st_idx * kStageStride;
+        const Grid gr = w.gr;
+        const int tx = threadIdx.x & 31, j = j0 + (threadIdx.x >> 5);
+        const bool fp32 = ph == kPhMSweep;
+        if (threadIdx.x == 0) {  // the next sweep tile's boxes, into the other stage
+          const int i2 = next_sweep(a, tc, idx + 1, nloc, c, C);
+          s_next = i2;
+          if (i2 < nloc) {
+            const BTile t2 = tc.get_tile(a, i2, c, C);
+            issue_sweep(a, t2, tc.get_dom(a, t2.dom), smem + (st_idx ^ 1) * kStageStride,
+                        &bars[st_idx ^ 1], s_acq);
+          }
+        }
+        // X and |Ct| of the owned cells: in flight while the boxes arrive
+        double xs[CPT], ds[CPT];
+        float fxs[CPT];
+#pragma unroll
+        for (int cc = 0; cc < CPT; ++cc) {
+          const int i = i0 + cc * 32 + tx;
+          const bool in = i < gr.nx && j < gr.ny;
+          const long k = gr.at(in ? i : 0, in ? j : 0);
+          if (fp32) {
+            fxs[cc] = w.fd[k];
+            xs[cc] = 0.0;
+            ds[cc] = 0.0;
+          } else {
+            xs[cc] = w.x[k];
+            ds[cc] = fabs(w.Ct[k]);
+            fxs[cc] = 0.0f;
+          }
+        }
+        if (threadIdx.x == 0) s_ok = mbar_wait(&bars[st_idx], (seq >> 1) & 1, kBarrierTimeoutNs);
+        __syncthreads();
+        if (!s_ok) {
+          if (threadIdx.x == 0) {
+            fail_all(a, FREHD_ERR_TIMEOUT);
+            if (s_next < nloc) mbar_wait(&bars[st_idx ^ 1], ((seq + 1) >> 1) & 1, kBarrierTimeoutNs);
+          }
+          return;
+        }
+        mbar_wait(&bars[st_idx], (seq >> 1) & 1, kBarrierTimeoutNs);  // acquire in every thread
+        if (fp32) {
+          float *rn_out = dm.cur ? w.fr0 : w.fr1, *pn_out = dm.cur ? w.fp0 : w.fp1;
+          sweep_tile<float, false, float>(Stage<float>(stage), gr, i0, j0, fxs, ds, w.fd, rn_out,
+                                          pn_out, (float)dm.alpha, (float)dm.beta, acc);
+        } else {
+          double *rn_out = dm.cur ? w.r : w.q, *pn_out = dm.cur ? w.p0 : w.p1;
+          sweep_tile<double, true, double>(Stage<double>(stage), gr, i0, j0, xs, ds, w.x, rn_out,
+                                           pn_out, dm.alpha, dm.beta, acc);
+        }
+        ++seq;
+      } else {
+        const int x0s = dm.flags & 1;
+        switch (ph) {
+          case kPhSetup1: t_setup1(w, i0, j0, dm.elim, x0s); break;
+          case kPhSetup2: t_setup2(w, i0, j0, dm.elim, x0s, acc); break;
+          case kPhDelta0: t_delta0<double>(w.gr, w.r, w.Hx, w.Hy, i0, j0, acc); break;
+          case kPhFinal: t_final(w, i0, j0); break;
+          case kPhMSetup: t_msetup(w, i0, j0, dm.elim, x0s); break;
+          case kPhMResid: t_mresid(w, i0, j0, dm.elim, acc); break;
+          case kPhMDelta0: t_delta0<float>(w.gr, w.fr0, w.fhx, w.fhy, i0, j0, acc); break;
+          case kPhMXupd: t_xupd(w, i0, j0); break;
+          default: break;
+        }
+      }
+      if (nv) {  // the tile's sums, added in a fixed order, into its slot
+#pragma unroll
+        for (int m = 0; m < 6; ++m)
+          if (m < nv) {
+            const double v = warp_sum(acc[m]);
+            if (lane == 0) sh_red[rbuf][m][wid] = v;
+          }
+        __syncthreads();
+        if (threadIdx.x < nv) {
+          double sum = 0;
+          for (int q = 0; q < NWARP; ++q) sum += sh_red[rbuf][threadIdx.x][q];
+          a.part[g * kTilePartStride + threadIdx.x] = sum;
+        }
+        rbuf ^= 1;
+      } else if (is_sweep(ph)) {
+        __syncthreads();  // the stage is free for the tile after next
+      }
+    }
+    // this thread's global writes before the next round's TMA reads (other CTAs)
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    {
+      double none[1] = {0};
+      if (!grid_allreduce<1, kRedStride>(none, a.bsync, a.bpart, a.bpart + kRedStride * (long)C, C, c)) {
+        fail_all(a, FREHD_ERR_TIMEOUT);
+        return;
+      }
+    }
+    // ---- reduce: domain k by CTA k mod C, its tiles' sums in tile order
+    for (int k = (int)c; k < a.ndom; k += (int)C) {
+      BState st = load_state(a.states + k);
+      __syncthreads();  // every thread read the state before thread 0 may replace it
+      if (st.phase == kPhDone) continue;
+      const BDom dm = a.doms[k];
+      const int nv = phase_sums(st.phase);
+      double tot[6] = {0, 0, 0, 0, 0, 0};
+      if (nv) {
+        double v[6] = {0, 0, 0, 0, 0, 0};
+        for (int q = threadIdx.x; q < dm.ntiles; q += blockDim.x)
+#pragma unroll
+          for (int m = 0; m < 6; ++m)
+            if (m < nv) v[m] += __ldcg(a.part + (long)(dm.tile0 + q) * kTilePartStride + m);
+#pragma unroll
+        for (int m = 0; m < 6; ++m)
+          if (m < nv) {
+            const double sum = warp_sum(v[m]);
+            if (lane == 0) sh_red[0][m][wid] = sum;
+          }
+        __syncthreads();
+        if (threadIdx.x == 0)
+#pragma unroll
+          for (int m = 0; m < 6; ++m)
+            if (m < nv)
+              for (int q = 0; q < NWARP; ++q) tot[m] += sh_red[0][m][q];
+      }
+      if (threadIdx.x == 0) {
+        advance(a, k, st, tot);
+        a.states[k] = st;
+      }
+      __syncthreads();
+    }
+    rbuf = 0;
+    {
+      double none[1] = {0};
+      if (!grid_allreduce<1, kRedStride>(none, a.bsync, a.bpart, a.bpart + kRedStride * (long)C, C, c)) {
+        fail_all(a, FREHD_ERR_TIMEOUT);
+        return;
+      }
+    }
+    if (*(volatile int *)&a.bsync->n_done >= a.ndom) break;
+  }
+}
+
 // ---------------------------------------------------------------- host side
 
 namespace {
@@ -883,6 +1586,21 @@ int cg1_make_maps(const Grid &g, double *r0, double *r1, double *p0, double *p1,
   rc = rc ? rc : encode(g, hx, &m->hx);
   rc = rc ? rc : encode(g, hy, &m->hy);
   return rc;
+}
+
+int encode_fine_box(const double *zf, long cols, long rows, CUtensorMap *out) {
+  auto fn = encode_fn();
+  if (!fn) return fail(FREHD_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  std::memset(out, 0, sizeof(*out));
+  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)cols * sizeof(double)};
+  const cuuint32_t box[2] = {(cuuint32_t)kFineBoxW, (cuuint32_t)kFineBoxH};
+  const cuuint32_t estr[2] = {1, 1};
+  CUresult e = fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(zf), dims, strides,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (e != CUDA_SUCCESS) return fail(FREHD_ERR_CUDA, "cuTensorMapEncodeTiled (fine bottoms) failed (%d)", (int)e);
+  return FREHD_OK;
 }
 
 int cg1_make_maps_f32(const Grid &g, float *r0, float *r1, float *p0, float *p1, float *hx,
@@ -945,6 +1663,29 @@ int cg1_launch(const View &w, const Cg1Maps *m_dev, int blocks, int x0_surface, 
   cudaError_t e = cudaLaunchCooperativeKernel((void *)k_cg1, dim3(blocks), dim3(kCgThreads), args,
                                               cg1_smem_bytes(), stream);
   if (e != cudaSuccess) return fail(FREHD_ERR_CUDA, "k_cg1 launch: %s", cudaGetErrorString(e));
+  return FREHD_OK;
+}
+
+int cg1_tiles_capacity(int device, int *ctas) {
+  static const size_t smem = cg1_smem_bytes();
+  cudaError_t e = cudaFuncSetAttribute(k_cg1_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return fail(FREHD_ERR_CUDA, "k_cg1_tiles shared memory: %s", cudaGetErrorString(e));
+  int nsm = 0, per = 0;
+  e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg1_tiles, kCgThreads, smem);
+  if (e != cudaSuccess) return fail(FREHD_ERR_CUDA, "k_cg1_tiles occupancy: %s", cudaGetErrorString(e));
+  *ctas = nsm * (per > 0 ? per : 0);
+  return *ctas > 0 ? FREHD_OK : fail(FREHD_ERR_CUDA, "k_cg1_tiles does not fit on an SM");
+}
+
+int cg1_launch_tiles(const View *views2, const Cg1Maps *const *maps, const BDom *doms,
+                     BState *states, const BTile *tiles, int ndom, int ntiles, double *part,
+                     Scratch *bsync, double *bpart, int nctas, cudaStream_t stream) {
+  TilesArgs a{views2, maps, doms, states, tiles, ndom, ntiles, part, bsync, bpart};
+  void *args[] = {&a};
+  cudaError_t e = cudaLaunchCooperativeKernel((void *)k_cg1_tiles, dim3(nctas), dim3(kCgThreads), args,
+                                              cg1_smem_bytes(), stream);
+  if (e != cudaSuccess) return fail(FREHD_ERR_CUDA, "k_cg1_tiles launch: %s", cudaGetErrorString(e));
   return FREHD_OK;
 }
 

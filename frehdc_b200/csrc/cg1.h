@@ -25,6 +25,9 @@ int cg1_make_maps(const Grid &g, double *r0, double *r1, double *p0, double *p1,
 int cg1_make_maps_f32(const Grid &g, float *r0, float *r1, float *p0, float *p1, float *hx,
                       float *hy, Cg1Maps *m);
 size_t cg1_smem_bytes();
+// Tensor map of a domain's fine bottoms (cols x rows doubles, row-major) with the
+// kFineBoxW x kFineBoxH window box k_update_geo stages.
+int encode_fine_box(const double *zf, long cols, long rows, CUtensorMap *out);
 // Co-resident blocks for a cooperative launch, at most one per tile.
 int cg1_blocks(int device, const Grid &g, int *blocks);
 int cg1_launch(const View &w, const Cg1Maps *m_dev, int blocks, int x0_surface, int eliminate,
@@ -44,6 +47,37 @@ int cg1_launch_batch(const View *views2, const Cg1Maps *const *maps, const int *
                      const CgJob *jobs, int nctas, cudaStream_t stream);
 // CTAs of the batched solve that fit on the device at once.
 int cg1_batch_capacity(int device, int *ctas);
+
+// ---- batched solve over one list of every domain's tiles (k_cg1_tiles)
+// One admitted domain of the solve (built by the host).
+struct BDom {
+  int slot;          // views2[2*slot + parity], maps[slot]
+  int tile0, ntiles; // its CG tiles in the global list, in its own tile order
+  int ntx;           // its tiles along x
+  int flags;         // bit 0: x0 = surface; bit 1: decoupled rows eliminated
+  int pad;
+};
+// One entry of the global tile list.
+struct BTile {
+  int dom;   // index into the BDom array
+  int tile;  // the domain's own tile number
+};
+// The solve's state of one domain (device memory; written by its reducing CTA
+// between the rounds of a launch, initialised at the launch's start).
+struct BState {
+  double alpha, beta, gamma, gamma_old, delta, e1, e2, e3, rr, bnorm, best, rr_prev, stop;
+  int phase, it, it_all, attempt, elim, cur, outer, fallback, noconv, best_it, vpar, takeover;
+};
+// Partial sums kept per tile of the global list.
+constexpr int kTilePartStride = 8;
+// Launch: nctas CTAs over ntiles list entries of ndom domains.  part: ntiles *
+// kTilePartStride doubles; bsync: the launch's barrier scratch (bar_count and
+// n_done zero at the launch, reset by k_finish_batch); bpart: (nctas + 1) *
+// kCg1PartialStride doubles.
+int cg1_launch_tiles(const View *views2, const Cg1Maps *const *maps, const BDom *doms,
+                     BState *states, const BTile *tiles, int ndom, int ntiles, double *part,
+                     Scratch *bsync, double *bpart, int nctas, cudaStream_t stream);
+int cg1_tiles_capacity(int device, int *ctas);
 
 }  // namespace frehd
 

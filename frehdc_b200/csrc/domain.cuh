@@ -95,6 +95,8 @@ struct Scratch {
                              // next solve's first grid barrier without arriving (0: none)
   long long cg_noconv_steps; // running count of completed steps whose solve stopped at maxIter
   unsigned long long wait_limit_ns;  // bound of the grid-barrier waits (0: kBarrierTimeoutNs)
+  int n_done;                // batched solve over a tile list: domains whose solve ended
+  int pad2;
 };
 
 // Device pointers of the state and work arrays for one step.  `cur`/`nxt`
@@ -129,6 +131,7 @@ struct View {
   const double *wcos, *wsin;   // cos/sin of the wind direction by step (nwdir + 1 entries;
   int nwdir;                   // the last one for steps past the series)
   double *dXP, *dYP;           // face depths of the last updateAllFaceDepth (wind only)
+  const void *zf_map;          // CUtensorMap of the fine bottoms (r = 4 boxes of k_update_geo), or null
   Scratch *sc;
 };
 

@@ -44,6 +44,7 @@ struct frehd_domain {
   int ninflow = 0, nwspd = 0, nwdir = 0;
   double *dXP = nullptr, *dYP = nullptr;  // face depths read by the wind term
   double *tables = nullptr, *zf = nullptr;
+  CUtensorMap *zf_map_dev = nullptr;  // window map of the fine bottoms (r = 4, no block check)
   frehd::Scratch *sc = nullptr;
   frehd::StepOut *out = nullptr;
   frehd::StepOut *out_host = nullptr;  // pinned

@@ -20,6 +20,7 @@
 #include "domain.cuh"
 #include "kernels.cuh"
 #include "subgrid_levels.h"
+#include "tma.cuh"
 
 namespace frehd {
 
@@ -290,11 +291,15 @@ __device__ __forceinline__ double level_surf(const Params &p, int k) {
 }
 
 // Table values of cell (i, j) at level k: all ten, or (part) only the west- or
-// south-face pair.
+// south-face pair.  zs: the cell's first fine pixel in the block's staged
+// window of fine bottoms (row pitch kFineBoxW), or null to read them from zf.
 __device__ __forceinline__ void level_values(const Params &p, int i, int j, int k, frehd_cell_levels *o,
-                                             int part) {
+                                             int part, const double *zs) {
   if (p.geom_fine) {
-    if (p.r == 4 && !p.check_block)
+    if (zs)
+      frehd_cell_levels_r4_at(zs, kFineBoxW, p.nx, p.ny, i, j, frehd_level(p.surfmin, p.dsurf, k),
+                              p.dxf * p.dyf, p.dxf, part, o);
+    else if (p.r == 4 && !p.check_block)
       frehd_cell_levels_r4(p.zf, p.fpitch, p.nx, p.ny, i, j, frehd_level(p.surfmin, p.dsurf, k),
                            p.dxf * p.dyf, p.dxf, part, o);
     else  // every value (a part's caller reads only its own)
@@ -318,7 +323,7 @@ struct SubCell {
 // FREHD_LV_SOUTH only Om and Vym (what the west/south neighbour's face needs).
 template <int PART>
 __device__ SubCell compute_sub_area(const View &w, int i, int j, double s, int *ind_io,
-                                    double depth_old) {
+                                    double depth_old, const double *zs) {
   const Params &p = w.p;
   const Grid &g = w.gr;
   const double ds = p.dsurf;
@@ -337,8 +342,8 @@ __device__ SubCell compute_sub_area(const View &w, int i, int j, double s, int *
   else j2 = s > level_surf(p, j1) ? j1 + 1 : j1 - 1;
   const double a1 = level_surf(p, j1), a2 = level_surf(p, j2);
   frehd_cell_levels L1, L2;
-  level_values(p, i, j, j1, &L1, PART);
-  if (j2 != j1) level_values(p, i, j, j2, &L2, PART); else L2 = L1;
+  level_values(p, i, j, j1, &L1, PART, zs);
+  if (j2 != j1) level_values(p, i, j, j2, &L2, PART, zs); else L2 = L1;
   SubCell c;
 #define FREHD_FACE(out, wd, f)                                                         \
   {                                                                                    \
@@ -432,8 +437,40 @@ static __device__ __forceinline__ void update_geo_tile(const View &w, int bx, in
   __shared__ double sh_s[EY][EX], sh_Np[EY][EX], sh_Nm[EY][EX], sh_Op[EY][EX], sh_Om[EY][EX];
   __shared__ double sh_Vxp[EY][EX], sh_Vxm[EY][EX], sh_Vyp[EY][EX], sh_Vym[EY][EX];
   __shared__ double sh_V[EY][EX], sh_Z[EY][EX];
+  __shared__ unsigned long long geo_bar;
+  extern __shared__ unsigned char geo_dyn[];
   const int i0 = bx * TBX, j0 = by * TBY;
   const int tid = threadIdx.y * TBX + threadIdx.x;
+  // The fine bottoms of the block's cells and of the pixels its faces and halo
+  // cells read (fine columns 4*i0-4 .. 4*i0+131, rows 4*j0-4 .. 4*j0+35; zero
+  // outside the domain) arrive as one TMA box while the new surface is formed;
+  // the level evaluations then read shared memory.
+  double *box = reinterpret_cast<double *>(geo_dyn + ((128u - (smem_u32(geo_dyn) & 127u)) & 127u));
+  const bool staged = w.zf_map != nullptr && p.geom_fine && p.r == 4 && !p.check_block;
+  const int fx0 = 4 * i0 - 4, fy0 = 4 * j0 - 4;
+  if (staged) {
+    if (tid == 0) {
+      mbar_init(&geo_bar, 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      const CUtensorMap *map = static_cast<const CUtensorMap *>(w.zf_map);
+      acquire_maps(map, 1);
+      mbar_expect_tx(&geo_bar, (unsigned)(kFineBoxW * kFineBoxH * sizeof(double)));
+      tma_load_2d(box, map, &geo_bar, fx0, fy0);
+    }
+    __syncthreads();
+  }
+  bool box_ready = false;
+  auto cell_box = [&](int i, int j) -> const double * {
+    if (!staged) return nullptr;
+    if (!box_ready) {
+      if (!mbar_wait(&geo_bar, 0, kBarrierTimeoutNs)) {
+        set_status(w.sc, FREHD_ERR_TIMEOUT);
+        return nullptr;  // the global copy holds the same doubles
+      }
+      box_ready = true;
+    }
+    return box + (long)(4 * j - fy0) * kFineBoxW + (4 * i - fx0);
+  };
   // Each thread evaluates its own cell; threads 0..TBX-1 then evaluate the north
   // halo row (only Om, Vym, s are read from it) and threads TBX..TBX+TBY-1 the
   // east halo column (only Nm, Vxm, s).
@@ -480,19 +517,22 @@ static __device__ __forceinline__ void update_geo_tile(const View &w, int bx, in
     int ind = w.ind_cur[k];
     sh_s[ey][ex] = s;
     if (own) {
-      const SubCell c = compute_sub_area<FREHD_LV_ALL>(w, i, j, s, &ind, depth_old);
+      const SubCell c = compute_sub_area<FREHD_LV_ALL>(w, i, j, s, &ind, depth_old, cell_box(i, j));
       w.ind_nxt[k] = ind;
       sh_Np[ey][ex] = c.Np; sh_Nm[ey][ex] = c.Nm; sh_Op[ey][ex] = c.Op; sh_Om[ey][ex] = c.Om;
       sh_Vxp[ey][ex] = c.Vxp; sh_Vxm[ey][ex] = c.Vxm; sh_Vyp[ey][ex] = c.Vyp; sh_Vym[ey][ex] = c.Vym;
       sh_V[ey][ex] = c.V; sh_Z[ey][ex] = c.Z;
     } else if (ex == TBX) {
-      const SubCell c = compute_sub_area<FREHD_LV_WEST>(w, i, j, s, &ind, depth_old);
+      const SubCell c = compute_sub_area<FREHD_LV_WEST>(w, i, j, s, &ind, depth_old, cell_box(i, j));
       sh_Nm[ey][ex] = c.Nm; sh_Vxm[ey][ex] = c.Vxm;
     } else {
-      const SubCell c = compute_sub_area<FREHD_LV_SOUTH>(w, i, j, s, &ind, depth_old);
+      const SubCell c = compute_sub_area<FREHD_LV_SOUTH>(w, i, j, s, &ind, depth_old, cell_box(i, j));
       sh_Om[ey][ex] = c.Om; sh_Vym[ey][ex] = c.Vym;
     }
   }
+  // the box's copy has landed (or its second bounded wait gave up) before any
+  // thread of the block may leave
+  if (staged && tid == 0) mbar_wait(&geo_bar, 0, kBarrierTimeoutNs);
   __syncthreads();
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i = i0 + tx, j = j0 + ty;
@@ -836,12 +876,25 @@ static __device__ __forceinline__ void update_vel_tile(const View &w, int bx, in
   const int j = by * TBY + threadIdx.y;
   double cflx = 0, cfly = 0, vol = 0;
   int nwarn = 0;
-  if (i < g.nx && j < g.ny) {
+  // Each face velocity once: a cell's west face is its west neighbour's east
+  // face (the lane before it) and its south face the north face of the cell
+  // below (the row before it in the block); the block's first column and row
+  // evaluate theirs.  The same function of the same inputs, so the same doubles.
+  __shared__ double s_vN[TBY][TBX];
+  const bool in = i < g.nx && j < g.ny;
+  const double uE_ = in ? face_u(w, i, j) : 0.0;
+  const double vN_ = in ? face_v(w, i, j) : 0.0;
+  const double uW_lane = __shfl_up_sync(0xffffffffu, uE_, 1);
+  s_vN[threadIdx.y][threadIdx.x] = vN_;
+  __syncthreads();
+  if (in) {
     const long k = g.at(i, j);
-    const double uE = face_u(w, i, j);
-    const double uW = i > 0 ? face_u(w, i - 1, j) : uE;  // enforceVelocityBC ghost copy
-    const double vN = face_v(w, i, j);
-    const double vS = j > 0 ? face_v(w, i, j - 1) : vN;
+    const double uE = uE_;
+    const double uW = i > 0 ? (threadIdx.x > 0 ? uW_lane : face_u(w, i - 1, j))
+                            : uE;  // enforceVelocityBC ghost copy
+    const double vN = vN_;
+    const double vS = j > 0 ? (threadIdx.y > 0 ? s_vN[threadIdx.y - 1][threadIdx.x] : face_v(w, i, j - 1))
+                            : vN;
     // computeFaceFlowRateSub (subgrid.c:1190-1212)
     const double NxW = rd(w.Nx, g, i - 1, j), OyS = rd(w.Oy, g, i, j - 1);
     const double FE = uE * w.Nx[k], FW = uW * NxW, FN = vN * w.Oy[k], FS = vS * OyS;
@@ -1099,16 +1152,33 @@ __global__ void __launch_bounds__(TBX *TBY) k_update_vel_batch(const View *views
 }
 
 // One block per domain: k_finish's work, then the domain's ping-pong half flips.
-__global__ void k_finish_batch(const View *views2, const FinishJob *jobs) {
+// bsync (may be null): the barrier scratch of the batch's tile-list solve, which
+// ran before this kernel; its counters start the next step's solve from zero,
+// also after a solve that gave up waiting.
+__global__ void k_finish_batch(const View *views2, const FinishJob *jobs, Scratch *bsync) {
   __shared__ View sv;
   __shared__ int s_cur;
   const FinishJob f = jobs[blockIdx.x];
+  if (bsync && blockIdx.x == 0 && threadIdx.x == 0) {
+    bsync->bar_count = 0;
+    bsync->n_done = 0;
+    bsync->status = FREHD_OK;
+  }
   stage_view(views2, f.d, &sv, &s_cur, threadIdx.x, blockDim.x);
   const bool ran = finish_block(sv, f.nblocks_vel, f.out);
   if (ran && threadIdx.x == 0) sv.sc->cur = s_cur ^ 1;
   // the batch's owner sees a failed domain (CFL > 20, a wait that gave up) after
   // this step without reading the domain's statistics
   if (threadIdx.x == 0) *(volatile int *)f.status = *(volatile int *)&sv.sc->status;
+}
+
+cudaError_t geo_kernels_setup() {
+  cudaError_t e = cudaFuncSetAttribute(k_update_geo, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGeoDynSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_update_geo_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGeoDynSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_update_geo_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGeoDynSmem);
+  return e;
 }
 
 // ---------------------------------------------------------------- layout

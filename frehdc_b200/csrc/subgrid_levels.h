@@ -278,13 +278,14 @@ enum { FREHD_LV_ALL = 0, FREHD_LV_WEST = 1, FREHD_LV_SOUTH = 2 };
  * areas reuse the block's own edge depths instead of recomputing them.  Same
  * operations in the same order, so the same doubles.  `part` selects all ten
  * values, or only the west-face pair (Nm, Vxm) or the south-face pair (Om, Vym)
- * that the west or south neighbour's face combination needs.
+ * that the west or south neighbour's face combination needs.  b points at the
+ * cell's first fine pixel in an array of row pitch fpitch that also holds the
+ * neighbouring pixels the faces read (the whole domain, or a staged window).
  */
-FREHD_HD void frehd_cell_levels_r4(const double *zf, long fpitch, int nx, int ny, int i, int j,
-                                   double h, double dA, double dxf, int part,
-                                   frehd_cell_levels *o) {
+FREHD_HD void frehd_cell_levels_r4_at(const double *b, long fpitch, int nx, int ny, int i, int j,
+                                      double h, double dA, double dxf, int part,
+                                      frehd_cell_levels *o) {
   (void)nx;
-  const double *b = zf + (long)j * 4 * fpitch + (long)i * 4;
   double d[4][4];
   if (part == FREHD_LV_ALL) {
     for (int fj = 0; fj < 4; ++fj)
@@ -367,6 +368,14 @@ FREHD_HD void frehd_cell_levels_r4(const double *zf, long fpitch, int nx, int ny
     }
     o->Om = s * dxf;
   }
+}
+
+/* The same with the fine bottoms zf[fj * fpitch + fi] of the whole domain. */
+FREHD_HD void frehd_cell_levels_r4(const double *zf, long fpitch, int nx, int ny, int i, int j,
+                                   double h, double dA, double dxf, int part,
+                                   frehd_cell_levels *o) {
+  frehd_cell_levels_r4_at(zf + (long)j * 4 * fpitch + (long)i * 4, fpitch, nx, ny, i, j, h, dA, dxf,
+                          part, o);
 }
 
 /* Coarse bottom and face-bottom elevations of cell (i, j) (host pre-processing;

@@ -147,6 +147,7 @@ CG_SINGLE_SWEEP, CG_TWO_PHASE = 0, 1
 DECOUPLED_AS_ASSEMBLED, DECOUPLED_ELIMINATED = 0, 1
 PRECISION_FP64, PRECISION_MIXED = 0, 1
 SERIES_TIDE, SERIES_INFLOW, SERIES_WIND_SPEED, SERIES_WIND_DIR = 0, 1, 2, 3
+BATCH_TILE_LIST, BATCH_CTA_GROUPS = 0, 1
 STATUS = {0: "ok", 1: "invalid", 2: "unsupported", 3: "cuda", 4: "nomem", 5: "cg_noconverge",
           6: "cfl", 7: "timeout", 8: "state"}
 
@@ -447,6 +448,7 @@ def _declare_batch(L: C.CDLL) -> None:
     L.frehd_batch_info.argtypes = [_vp, C.POINTER(BatchInfo)]
     L.frehd_batch_stream.argtypes = [_vp, C.POINTER(_vp)]
     L.frehd_batch_set_graph.argtypes = [_vp, C.c_int]
+    L.frehd_batch_set_cg_packing.argtypes = [_vp, C.c_int]
     L.frehd_server_create.argtypes = [C.c_int, C.c_longlong, C.c_double, C.POINTER(_vp)]
     L.frehd_server_submit.argtypes = [_vp, _vp, C.c_int, C.c_int, C.POINTER(C.c_longlong)]
     L.frehd_server_poll.argtypes = [_vp, C.POINTER(ServerDone), C.c_int, C.c_int, _ip]
@@ -540,6 +542,10 @@ class Batch:
 
     def set_graph(self, on: bool):
         check(lib().frehd_batch_set_graph(self.h, int(on)), "frehd_batch_set_graph")
+
+    def set_cg_packing(self, packing: int):
+        """BATCH_TILE_LIST (default) or BATCH_CTA_GROUPS (frehd_batch_set_cg_packing)."""
+        check(lib().frehd_batch_set_cg_packing(self.h, int(packing)), "frehd_batch_set_cg_packing")
 
     def close(self):
         if getattr(self, "h", None):

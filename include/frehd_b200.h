@@ -402,8 +402,16 @@ int frehd_cg_solve_noalloc(int nx, int ny, const double *Ct, const double *Gx, c
  * frehd_batch_step advances every admitted domain by one step with five kernel
  * launches in total (replayed from a CUDA graph where the driver accepts the
  * capture).  A domain's results do not depend on which other domains share the
- * batch: its CG runs on round(cells / cells_per_cta) CTAs (at least
- * one) whatever the mix.
+ * batch.  The solve of all domains is one cooperative launch in one of two
+ * packings (frehd_batch_set_cg_packing):
+ *   FREHD_BATCH_TILE_LIST (default): every domain's CG tiles form one list spread
+ *     over all CTAs; a domain's sums are added in its own tile order, so its
+ *     result is the same in any mix; cells_per_cta is not used, and admission is
+ *     by memory alone;
+ *   FREHD_BATCH_CTA_GROUPS: a domain's CG runs on round(cells / cells_per_cta)
+ *     CTAs (at least one) whatever the mix; admission also needs free CTAs.
+ * The two packings add the solve's partial sums in different orders: their
+ * results agree to the solver's rounding, not bit for bit.
  */
 typedef struct frehd_batch frehd_batch;
 typedef struct frehd_batch_info_t {
@@ -436,6 +444,10 @@ int frehd_batch_info(frehd_batch *b, frehd_batch_info_t *out);
 int frehd_batch_stream(frehd_batch *b, void **stream);
 /* Replay steps from a captured CUDA graph (default 1) or launch them directly. */
 int frehd_batch_set_graph(frehd_batch *b, int on);
+/* Packing of the batched solve (see above); FREHD_ERR_NOMEM when the admitted
+ * domains do not fit the CTA groups (the packing then stays the tile list). */
+enum { FREHD_BATCH_TILE_LIST = 0, FREHD_BATCH_CTA_GROUPS = 1 };
+int frehd_batch_set_cg_packing(frehd_batch *b, int packing);
 
 /* ------------------------------------------------------------ serving */
 /*

@@ -2,10 +2,14 @@
 sub-step over all of them.
 
 A domain's arithmetic in a batch is the single-domain step's: the stencil
-kernels run the same tile code, and its CG runs on round(cells/cells_per_cta)
-CTAs.  So with cells_per_cta = 1 (as many CTAs as the single-domain solve uses)
-a batch reproduces single-domain runs bit for bit, and for any fixed
-cells_per_cta a domain's result is the same alone and in a mix.
+kernels run the same tile code.  Its solve depends on the packing:
+* CTA groups: its CG runs on round(cells/cells_per_cta) CTAs; with
+  cells_per_cta = 1 (as many CTAs as the single-domain solve uses) a batch
+  reproduces single-domain runs bit for bit;
+* the tile list (default): the same sweeps over the domain's tiles, with the
+  partial sums added in the domain's own tile order; its results agree with
+  the single-domain runs to the solver's rounding.
+In either packing a domain's result is the same alone and in a mix, bit for bit.
 """
 import numpy as np
 import pytest
@@ -24,13 +28,16 @@ def _need_gpu():
         pytest.fail("no CUDA device visible: the GPU tests need a B200")
 
 
-def _run_batch(names, steps, scratch, cells_per_cta, graph=True):
+def _run_batch(names, steps, scratch, cells_per_cta, graph=True, packing=None,
+               precision=native.PRECISION_FP64):
     b = native.Batch(BUDGET, cells_per_cta)
     b.set_graph(graph)
+    if packing is not None:
+        b.set_cg_packing(packing)
     doms = {}
     for n in names:
         d, _ = deck_for(n, str(scratch))
-        g = native.domain_from_deck(d, geometry="fine")
+        g = native.domain_from_deck(d, geometry="fine", precision=precision, eps_inner=1e-5)
         doms[n] = (g, b.admit(g, 1))
     for _ in range(steps):
         b.step()
@@ -45,7 +52,7 @@ def _run_batch(names, steps, scratch, cells_per_cta, graph=True):
 
 def test_batch_matches_single_domain_bitwise(scratch):
     names = list(SPECS)
-    got, info = _run_batch(names, 12, scratch, cells_per_cta=1)
+    got, info = _run_batch(names, 12, scratch, cells_per_cta=1, packing=native.BATCH_CTA_GROUPS)
     assert info["domains"] == len(names)
     for n in names:
         d, _ = deck_for(n, str(scratch))
@@ -58,13 +65,49 @@ def test_batch_matches_single_domain_bitwise(scratch):
         assert got[n][1]["volume"] == st["volume"]
 
 
-@pytest.mark.parametrize("graph", [True, False])
-def test_same_alone_and_in_mix(graph, scratch):
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_tile_list_matches_single_domain(precision, scratch):
+    """The tile-list solve against each domain stepped alone: the same solver,
+    partial sums added in another order."""
     names = list(SPECS)
-    mix, info = _run_batch(names, 10, scratch, cells_per_cta=1e9, graph=graph)
+    prec = native.PRECISION_MIXED if precision == "mixed" else native.PRECISION_FP64
+    got, info = _run_batch(names, 12, scratch, cells_per_cta=1, packing=native.BATCH_TILE_LIST,
+                           precision=prec)
+    assert info["cg_ctas"] == info["cg_capacity"] > 0
+    for n in names:
+        d, _ = deck_for(n, str(scratch))
+        g = native.domain_from_deck(d, geometry="fine", precision=prec, eps_inner=1e-5)
+        assert g.run(1, 12) == 0
+        ref = g.download(FIELDS)
+        # the parity tests' whole-run bounds: 1e-9, face velocities 3e-9
+        assert mismatches(got[n][0], ref, ["ind"]) == [], n
+        assert mismatches(got[n][0], ref, ["uuXP", "vvYP"], exact=False, rtol=3e-9) == [], n
+        assert mismatches(got[n][0], ref, [f for f in FIELDS if f not in ("ind", "uuXP", "vvYP")],
+                          exact=False, rtol=1e-9) == [], n
+        st = g.stats()
+        assert got[n][1]["step"] == st["step"] == 12
+        assert abs(got[n][1]["volume"] - st["volume"]) <= 1e-12 * abs(st["volume"])
+        if precision == "fp64":
+            assert abs(got[n][1]["cg_iters"] - st["cg_iters"]) <= 2
+
+
+@pytest.mark.parametrize("packing", ["tile_list", "cta_groups"])
+@pytest.mark.parametrize("graph", [True, False])
+def test_same_alone_and_in_mix(graph, packing, scratch):
+    names = list(SPECS)
+    pk = native.BATCH_TILE_LIST if packing == "tile_list" else native.BATCH_CTA_GROUPS
+    mix, info = _run_batch(names, 10, scratch, cells_per_cta=1e9, graph=graph, packing=pk)
     assert info["graph"] == (1 if graph else 0)
     for n in names:
-        alone, _ = _run_batch([n], 10, scratch, cells_per_cta=1e9, graph=graph)
+        alone, _ = _run_batch([n], 10, scratch, cells_per_cta=1e9, graph=graph, packing=pk)
+        assert mismatches(mix[n][0], alone[n][0], FIELDS) == [], n
+
+
+def test_mixed_precision_same_alone_and_in_mix(scratch):
+    names = list(SPECS)
+    mix, _ = _run_batch(names, 10, scratch, cells_per_cta=1, precision=native.PRECISION_MIXED)
+    for n in ("wet48x40", "dry40x36", "tvd44x36"):
+        alone, _ = _run_batch([n], 10, scratch, cells_per_cta=1, precision=native.PRECISION_MIXED)
         assert mismatches(mix[n][0], alone[n][0], FIELDS) == [], n
 
 

@@ -13,24 +13,25 @@ once on a representative mix, then serve.
 from __future__ import annotations
 
 import itertools
+import math
 
 from . import native
 
-CELLS_PER_CTA = (8192.0, 16384.0, 32768.0, 65536.0, 131072.0, 196608.0, 262144.0, 393216.0,
-                 524288.0)
+CELLS_PER_CTA = (8192.0, 16384.0, 32768.0, 65536.0, 131072.0, 196608.0, 229376.0, 262144.0,
+                 294912.0, 327680.0, 393216.0, 524288.0)
 EPS_INNER = (1e-4, 1e-5, 1e-6)
 CTX, CTY = 128, 16   # CG tile of k_cg1
 
 
 def ctas_needed(sizes, cells_per_cta: float, capacity: int = 148) -> int:
     """CTAs of the batched CG for domains of these (nx, ny): each domain's
-    group is round(cells / cells_per_cta) CTAs (at least 1, at most its tile
+    group is ceil(cells / cells_per_cta) CTAs (at least 1, at most its tile
     count), multi-CTA groups get CTAs of their own and the single-CTA domains
     share the rest (batch.cu, group_size / ctas_needed)."""
     dedicated, singles = 0, 0
     for nx, ny in sizes:
         ntiles = ((nx + CTX - 1) // CTX) * ((ny + CTY - 1) // CTY)
-        g = max(1, min(int(round(nx * ny / cells_per_cta)), ntiles, capacity))
+        g = max(1, min(int(math.ceil(nx * ny / cells_per_cta)), ntiles, capacity))
         if g > 1:
             dedicated += g
         else:

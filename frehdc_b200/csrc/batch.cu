@@ -8,13 +8,13 @@
 //       (domain, 32 x 8 tile) entry of a tile table over all domains
 //   the solve, one cooperative launch over all co-resident CTAs, in one of two
 //       packings (frehd_batch_set_cg_packing):
-//     k_cg1_tiles (FREHD_BATCH_TILE_LIST, the default): the CG tiles of every
-//       domain form one list spread over all CTAs; each domain's sums are added
-//       in its own tile order, so its result does not depend on the mix
-//     k_cg1_batch (FREHD_BATCH_CTA_GROUPS): each domain solved by a group of
+//     k_cg1_batch (FREHD_BATCH_CTA_GROUPS, the default): each domain solved by a group of
 //       CTAs whose size depends on the domain's own cell count only (multi-CTA
-//       groups on CTAs of their own; single-CTA domains packed onto the
-//       remaining CTAs, longest first onto the least loaded, one after another)
+//       groups on CTAs of their own; single-CTA domains, longest first, taken
+//       one after another by whichever CTA is free)
+//     k_cg1_tiles (FREHD_BATCH_TILE_LIST): the CG tiles of every domain form one
+//       list spread over all CTAs; each domain's sums are added in its own tile
+//       order, so its result depends neither on the mix nor on cells_per_cta
 //   k_finish_batch   one block per domain; flips the domain's ping-pong half
 // The five launches are captured once per batch composition into a CUDA graph
 // and replayed every step.
@@ -45,6 +45,10 @@ using namespace frehd;
   } while (0)
 
 namespace {
+
+// Stencil tiles (32 x 8) one block of the batched stencil kernels runs, one
+// after another along a tile row: the domain's view is staged once for them.
+constexpr int kTilesPerBlock = 4;
 
 struct Slot {
   frehd_domain *d = nullptr;
@@ -93,15 +97,18 @@ struct frehd_batch {
   DevArray<FinishJob> fins;
   DevArray<int> job_start;
   DevArray<CgJob> jobs;
+  DevArray<CgJob> singles;  // single-CTA solves, longest first
+  int nsingles = 0;
+  int any_mixed = 0;        // an admitted domain solves in mixed precision
   // tile-list packing
-  int packing = FREHD_BATCH_TILE_LIST;
+  int packing = FREHD_BATCH_CTA_GROUPS;
   DevArray<BDom> bdoms;
   DevArray<BTile> btiles;
   DevArray<BState> bstates;
   DevArray<double> bpartials, bpart;
   DevArray<Scratch> bsync;
   int nbdoms = 0, nbtiles = 0;
-  long ntiles = 0;
+  long ntiles = 0, ntiles_upwind = 0;  // stencil tiles; those of upwind domains come first
   int nfin = 0, nctas = 0;
   // per-slot device status after each step, written by k_finish_batch into
   // host-mapped pinned memory (read by the server between steps)
@@ -120,7 +127,8 @@ namespace {
 int group_size(const frehd_batch *b, const frehd_domain *d) {
   const long ntiles = (long)((d->gr.nx + CTX - 1) / CTX) * ((d->gr.ny + CTY - 1) / CTY);
   const double cells = (double)d->gr.nx * d->gr.ny;
-  long g = (long)std::lround(cells / b->cells_per_cta);
+  // ceil: no CTA of a group carries more than cells_per_cta cells
+  long g = (long)std::ceil(cells / b->cells_per_cta);
   g = std::max(1L, std::min(g, std::min(ntiles, (long)b->capacity)));
   return (int)g;
 }
@@ -174,13 +182,17 @@ int launch_step(frehd_batch *b) {
   int rc = tl ? cg1_launch_tiles(b->views2.p, b->maps.p, b->bdoms.p, b->bstates.p, b->btiles.p,
                                  b->nbdoms, b->nbtiles, b->bpartials.p, b->bsync.p, b->bpart.p,
                                  b->nctas, b->stream)
-              : cg1_launch_batch(b->views2.p, b->maps.p, b->job_start.p, b->jobs.p, b->nctas,
+              : cg1_launch_batch(b->views2.p, b->maps.p, b->job_start.p, b->jobs.p, b->singles.p,
+                                 b->nsingles, &b->bsync.p->n_done, b->nctas, b->any_mixed,
                                  b->stream);
   if (rc) return rc;
   k_update_geo_batch<<<(unsigned)b->ntiles, bb, kGeoDynSmem, b->stream>>>(b->views2.p, b->tiles.p);
-  k_update_vel_batch<<<(unsigned)b->ntiles, bb, 0, b->stream>>>(b->views2.p, b->tiles.p);
-  k_finish_batch<<<(unsigned)b->nfin, 256, 0, b->stream>>>(b->views2.p, b->fins.p,
-                                                             tl ? b->bsync.p : nullptr);
+  if (b->ntiles_upwind > 0)
+    k_update_vel_batch<<<(unsigned)b->ntiles_upwind, bb, 0, b->stream>>>(b->views2.p, b->tiles.p);
+  if (b->ntiles > b->ntiles_upwind)
+    k_update_vel_tvd_batch<<<(unsigned)(b->ntiles - b->ntiles_upwind), bb, 0, b->stream>>>(
+        b->views2.p, b->tiles.p + b->ntiles_upwind);
+  k_finish_batch<<<(unsigned)b->nfin, 256, 0, b->stream>>>(b->views2.p, b->fins.p, b->bsync.p);
   BATCH_TRY(cudaGetLastError());
   return FREHD_OK;
 }
@@ -202,6 +214,19 @@ int rebuild(frehd_batch *b) {
     double cells;
   };
   std::vector<Dom> doms;
+  // stencil tiles of the upwind domains first, then the TVD ones (two kernels)
+  for (int pass = 0; pass < 2; ++pass)
+    for (int s = 0; s < nslot; ++s) {
+      frehd_domain *d = b->slots[s].d;
+      if (!d || (d->p.scalarAdv == 2) != (pass == 1)) continue;
+      const int gx = (d->gr.nx + 31) / 32, gy = (d->gr.ny + 7) / 8;
+      for (int by = 0; by < gy; ++by)
+        for (int bx = 0; bx < gx; bx += kTilesPerBlock)
+          tiles.push_back(BatchTile{s, bx, by, gx, std::min(kTilesPerBlock, gx - bx), 0});
+    }
+  long nup = 0;
+  for (const BatchTile &t : tiles)
+    if (b->slots[t.d].d->p.scalarAdv != 2) ++nup;
   for (int s = 0; s < nslot; ++s) {
     frehd_domain *d = b->slots[s].d;
     if (!d) continue;
@@ -209,14 +234,13 @@ int rebuild(frehd_batch *b) {
     views[2 * s + 1] = domain_view(d, 1);
     maps[s] = d->cg1_maps_dev;
     const int gx = (d->gr.nx + 31) / 32, gy = (d->gr.ny + 7) / 8;
-    for (int by = 0; by < gy; ++by)
-      for (int bx = 0; bx < gx; ++bx) tiles.push_back(BatchTile{s, bx, by, gx});
     fins.push_back(FinishJob{s, gx * gy, d->out, b->status_dev + s});
     doms.push_back(Dom{s, group_size(b, d), (double)d->gr.nx * d->gr.ny});
   }
   // the launch sizes describe the device tables: they stay zero (no launch) and
   // the batch stays dirty until every table of this composition is uploaded
   b->ntiles = 0;
+  b->ntiles_upwind = 0;
   b->nfin = 0;
   b->nctas = 0;
   if (doms.empty()) {
@@ -239,8 +263,8 @@ int rebuild(frehd_batch *b) {
       for (int t = 0; t < ntx * nty; ++t) bt.push_back(BTile{(int)bd.size() - 1, t});
     }
   }
-  // CTA-group packing: multi-CTA groups on CTAs of their own, then single-CTA
-  // domains longest first onto the least loaded remaining CTA.
+  // CTA-group packing: multi-CTA groups on CTAs of their own; single-CTA
+  // domains in one list that every CTA takes from once its own jobs are done.
   std::vector<std::vector<CgJob>> per_cta;
   std::vector<Dom> singles;
   for (const Dom &m : doms) {
@@ -255,19 +279,14 @@ int rebuild(frehd_batch *b) {
   if (b->packing != FREHD_BATCH_TILE_LIST && free_ctas < (singles.empty() ? 0 : 1))
     return fail(FREHD_ERR_STATE, "batch CTA capacity exceeded (%d CTAs for multi-CTA domains of %d)",
                 (int)per_cta.size(), b->capacity);
-  if (!singles.empty()) {
-    std::stable_sort(singles.begin(), singles.end(),
-                     [](const Dom &a, const Dom &c) { return a.cells > c.cells; });
-    const int nbins = std::min(free_ctas, (int)singles.size());
-    std::vector<double> load(nbins, 0.0);
-    std::vector<std::vector<CgJob>> bins(nbins);
-    for (const Dom &m : singles) {
-      const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-      load[k] += m.cells;
-      bins[k].push_back(CgJob{m.slot, 0, 1, flags_of(m.slot)});
-    }
-    for (auto &bin : bins) per_cta.push_back(bin);
-  }
+  // single-CTA domains, longest first, taken by whichever CTA is free (k_cg1_batch)
+  std::stable_sort(singles.begin(), singles.end(),
+                   [](const Dom &a, const Dom &c) { return a.cells > c.cells; });
+  std::vector<CgJob> single_jobs;
+  for (const Dom &m : singles) single_jobs.push_back(CgJob{m.slot, 0, 1, flags_of(m.slot)});
+  const int ngroups = (int)per_cta.size();
+  const int nctas_groups = single_jobs.empty() ? ngroups : b->capacity;
+  per_cta.resize(std::max(ngroups, nctas_groups));
   std::vector<int> start(per_cta.size() + 1, 0);
   std::vector<CgJob> jobs;
   for (size_t c = 0; c < per_cta.size(); ++c) {
@@ -283,17 +302,20 @@ int rebuild(frehd_batch *b) {
   rc = rc ? rc : b->fins.reserve(fins.size());
   rc = rc ? rc : b->job_start.reserve(start.size());
   rc = rc ? rc : b->jobs.reserve(jobs.size());
+  rc = rc ? rc : b->singles.reserve(single_jobs.size());
+  {  // the launch counter (both packings), zeroed once and reset by k_finish_batch
+    const bool fresh_sync = b->bsync.cap == 0;
+    rc = rc ? rc : b->bsync.reserve(1);
+    if (!rc && fresh_sync)
+      BATCH_TRY(cudaMemsetAsync(b->bsync.p, 0, sizeof(Scratch) * b->bsync.cap, b->stream));
+  }
   const bool tl = b->packing == FREHD_BATCH_TILE_LIST;
   if (tl) {
-    const bool fresh_sync = b->bsync.cap == 0;
     rc = rc ? rc : b->bdoms.reserve(bd.size());
     rc = rc ? rc : b->btiles.reserve(bt.size());
     rc = rc ? rc : b->bstates.reserve(bd.size());
     rc = rc ? rc : b->bpartials.reserve(bt.size() * (size_t)kTilePartStride);
     rc = rc ? rc : b->bpart.reserve(((size_t)b->capacity_tiles + 1) * kCg1PartialStride);
-    rc = rc ? rc : b->bsync.reserve(1);
-    if (!rc && fresh_sync)  // the barrier counters start at zero; k_finish_batch keeps them so
-      BATCH_TRY(cudaMemsetAsync(b->bsync.p, 0, sizeof(Scratch) * b->bsync.cap, b->stream));
   }
   if (rc) return rc;
   BATCH_TRY(cudaMemcpyAsync(b->views2.p, views.data(), sizeof(View) * views.size(), cudaMemcpyHostToDevice, b->stream));
@@ -302,6 +324,9 @@ int rebuild(frehd_batch *b) {
   BATCH_TRY(cudaMemcpyAsync(b->fins.p, fins.data(), sizeof(FinishJob) * fins.size(), cudaMemcpyHostToDevice, b->stream));
   BATCH_TRY(cudaMemcpyAsync(b->job_start.p, start.data(), sizeof(int) * start.size(), cudaMemcpyHostToDevice, b->stream));
   BATCH_TRY(cudaMemcpyAsync(b->jobs.p, jobs.data(), sizeof(CgJob) * jobs.size(), cudaMemcpyHostToDevice, b->stream));
+  if (!single_jobs.empty())
+    BATCH_TRY(cudaMemcpyAsync(b->singles.p, single_jobs.data(), sizeof(CgJob) * single_jobs.size(),
+                              cudaMemcpyHostToDevice, b->stream));
   if (tl) {
     BATCH_TRY(cudaMemcpyAsync(b->bdoms.p, bd.data(), sizeof(BDom) * bd.size(), cudaMemcpyHostToDevice, b->stream));
     BATCH_TRY(cudaMemcpyAsync(b->btiles.p, bt.data(), sizeof(BTile) * bt.size(), cudaMemcpyHostToDevice, b->stream));
@@ -309,8 +334,12 @@ int rebuild(frehd_batch *b) {
   // the host vectors go out of scope: the copies must have left them
   BATCH_TRY(cudaStreamSynchronize(b->stream));
   b->ntiles = (long)tiles.size();
+  b->ntiles_upwind = nup;
   b->nfin = (int)fins.size();
   b->nctas = tl ? b->capacity_tiles : (int)per_cta.size();
+  b->nsingles = (int)single_jobs.size();
+  b->any_mixed = 0;
+  for (const Dom &m : doms) b->any_mixed |= b->slots[m.slot].d->p.mixed ? 1 : 0;
   b->nbdoms = (int)bd.size();
   b->nbtiles = (int)bt.size();
   b->dirty = false;
@@ -414,6 +443,7 @@ extern "C" int frehd_batch_destroy(frehd_batch *b) {
   b->fins.release();
   b->job_start.release();
   b->jobs.release();
+  b->singles.release();
   b->bdoms.release();
   b->btiles.release();
   b->bstates.release();

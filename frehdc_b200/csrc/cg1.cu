@@ -65,11 +65,14 @@ namespace frehd {
 namespace {
 
 constexpr int kTW = CTX, kTH = CTY;              // owned cells of a tile (128 x 16)
-constexpr int kRing = 2 * (kTW + 2) + 2 * kTH;   // cells of the one-cell halo ring: 292
 constexpr int kRedStride = 8;                    // partial sums per block in grid_allreduce
 constexpr int kMaxOuter = 8;                     // refinements of one mixed-precision solve
 static_assert(kTH == kCgThreads / 32, "one warp per tile row");
-constexpr int kRingPer = (kRing + kCgThreads - 1) / kCgThreads;  // halo-ring cells per thread
+// The FP32 inner sweeps of the mixed solve work on tiles twice as tall (128 x 32,
+// each warp two rows): the FP32 boxes move half the bytes of the FP64 ones, and
+// the taller tile spreads each tile's barriers and TMA round trip over twice the
+// cells.
+constexpr int kTallTH = 2 * kTH;
 // resident CTAs per SM the launch bounds ask for: 128 registers per thread either way
 constexpr int kCg1MinBlocks = kCgThreads >= 512 ? 1 : 512 / kCgThreads;
 
@@ -77,12 +80,16 @@ constexpr int kCg1MinBlocks = kCgThreads >= 512 ? 1 : 512 / kCgThreads;
 // two-cell halo at least, kLeft chosen so that the box's first column is
 // 16-byte aligned in the padded layout (column offset kXOff = 4, tiles start at
 // multiples of 128 cells).
-template <typename T>
+template <typename T, int TH = kTH>
 struct Box {
+  static constexpr int kRows = TH;                 // owned rows of a tile
+  static constexpr int kRowsPerWarp = TH / (kCgThreads / 32);
   static constexpr int kLeft = sizeof(T) == 8 ? 2 : 4;
   static constexpr int kBW = kTW + 2 * kLeft;      // 132 (FP64) / 136 (FP32)
-  static constexpr int kBH = kTH + 4;              // 20
+  static constexpr int kBH = TH + 4;               // 20 (36 for the tall FP32 tiles)
   static constexpr int kBox = kBW * kBH;
+  static constexpr int kRing = 2 * (kTW + 2) + 2 * TH;  // cells of the one-cell halo ring
+  static constexpr int kRingPer = (kRing + kCgThreads - 1) / kCgThreads;  // ring cells per thread
   static constexpr unsigned kArrBytes = kBox * (unsigned)sizeof(T);
   static constexpr unsigned kStageBytes = 4 * kArrBytes;  // r~, p, Hx, Hy
   static_assert(kArrBytes % 128 == 0, "TMA destinations must stay 128-byte aligned");
@@ -95,15 +102,21 @@ struct Box {
   __device__ static __forceinline__ int ring(int t) {
     if (t < kTW + 2) return q(t - 1, -1);          // row above the tile
     t -= kTW + 2;
-    if (t < kTW + 2) return q(t - 1, kTH);         // row below
+    if (t < kTW + 2) return q(t - 1, TH);          // row below
     t -= kTW + 2;
-    if (t < kTH) return q(-1, t);                  // column left
-    t -= kTH;
+    if (t < TH) return q(-1, t);                   // column left
+    t -= TH;
     return q(kTW, t);                              // column right
+  }
+  // origin (first owned cell) of tile `tile` of a grid of these tiles
+  __device__ static __forceinline__ void origin(const TileIt &ti, int tile, int *i0, int *j0) {
+    *i0 = (tile % ti.ntx) * kTW;
+    *j0 = (tile / ti.ntx) * TH;
   }
 };
 constexpr unsigned kSmemStages = 2 * Box<double>::kStageBytes;  // FP64 stages are the larger
 static_assert(2 * Box<float>::kStageBytes <= kSmemStages, "FP32 stages fit the FP64 ones");
+static_assert(2 * Box<float, kTallTH>::kStageBytes <= kSmemStages, "tall FP32 stages fit too");
 
 template <typename T>
 struct Pair;
@@ -117,14 +130,14 @@ struct Pair<float> {
 };
 
 // Shared-memory arrays of one stage.
-template <typename T>
+template <typename T, int TH = kTH>
 struct Stage {
   T *R, *P, *HX, *HY;
   __device__ Stage(unsigned char *base) {
     R = reinterpret_cast<T *>(base);
-    P = R + Box<T>::kBox;
-    HX = P + Box<T>::kBox;
-    HY = HX + Box<T>::kBox;
+    P = R + Box<T, TH>::kBox;
+    HX = P + Box<T, TH>::kBox;
+    HY = HX + Box<T, TH>::kBox;
   }
 };
 
@@ -134,17 +147,18 @@ struct SweepMaps {
 };
 
 // Issue the four box loads of tile `tile` into a stage (one thread).
-template <typename T>
+template <typename T, int TH = kTH>
 __device__ __forceinline__ void issue_tile(const SweepMaps &m, const TileIt &ti, int tile,
                                            unsigned char *stage_base, unsigned long long *bar) {
+  using B = Box<T, TH>;
   int i0, j0;
-  tile_origin(ti, tile, &i0, &j0);
+  B::origin(ti, tile, &i0, &j0);
   // box origin: cell (i0 - kLeft, j0 - 2) = padded column i0 - kLeft + kXOff (16-byte aligned), row j0 - 1
-  const int x = i0 - Box<T>::kLeft + kXOff, y = j0 - 2 + 1;
-  Stage<T> s(stage_base);
+  const int x = i0 - B::kLeft + kXOff, y = j0 - 2 + 1;
+  Stage<T, TH> s(stage_base);
   // generic-proxy writes to this stage (the in-place passes) come before the TMA writes
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  mbar_expect_tx(bar, Box<T>::kStageBytes);
+  mbar_expect_tx(bar, B::kStageBytes);
   tma_load_2d(s.R, m.r, bar, x, y);
   tma_load_2d(s.P, m.p, bar, x, y);
   tma_load_2d(s.HX, m.hx, bar, x, y);
@@ -166,38 +180,41 @@ __device__ __forceinline__ T apply(const T *V, const T *HX, const T *HY, int q) 
 // rn_out / pn_out.  red += (r~',r~'), (w,r~'), (r~',s), (p,w), (p,s) and
 // sum D r~'^2 (kUnscaled; D = |Ct|) or (r~',r~') again.  seq: tiles this CTA
 // consumed so far (stage and mbarrier phase).
-template <typename T, bool kUnscaled, typename XT>
+template <typename T, bool kUnscaled, typename XT, int TH = kTH>
 __device__ __forceinline__ bool sweep(const SweepMaps &m, T *rn_out, T *pn_out, XT *X, const double *Ct,
                                       const Grid &g, const TileIt &ti, unsigned rank, unsigned nb,
                                       T alpha, T beta, double (&red)[6], unsigned char *smem,
                                       unsigned long long *bars, unsigned &seq, Scratch *sc) {
-  using B = Box<T>;
+  using B = Box<T, TH>;
+  constexpr int RW = B::kRowsPerWarp, NW = kCgThreads / 32;
   __shared__ int s_ok;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   // generic writes of the previous sweep (all blocks) come before this sweep's TMA reads
   if (threadIdx.x == 0) {
     asm volatile("fence.proxy.async.global;" ::: "memory");
-    issue_tile<T>(m, ti, rank, smem + (seq & 1) * B::kStageBytes, &bars[seq & 1]);
+    if ((int)rank < ti.ntiles)
+      issue_tile<T, TH>(m, ti, rank, smem + (seq & 1) * B::kStageBytes, &bars[seq & 1]);
   }
   for (int tile = rank; tile < ti.ntiles; tile += nb, ++seq) {
     const int st = seq & 1;
     const int next = tile + (int)nb;
     if (threadIdx.x == 0 && next < ti.ntiles)
-      issue_tile<T>(m, ti, next, smem + (st ^ 1) * B::kStageBytes, &bars[st ^ 1]);
+      issue_tile<T, TH>(m, ti, next, smem + (st ^ 1) * B::kStageBytes, &bars[st ^ 1]);
     int i0, j0;
-    tile_origin(ti, tile, &i0, &j0);
+    B::origin(ti, tile, &i0, &j0);
     // X and |Ct| of the owned cells: in flight while the boxes arrive
-    const int j = j0 + ty;
-    XT xs[CPT];
-    double ds[CPT];
+    XT xs[RW][CPT];
+    double ds[RW][CPT];
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-      const int i = i0 + c * 32 + tx;
-      const bool in = i < g.nx && j < g.ny;
-      const long k = g.at(in ? i : 0, in ? j : 0);
-      xs[c] = X[k];
-      ds[c] = kUnscaled ? fabs(Ct[k]) : 0.0;
-    }
+    for (int rr = 0; rr < RW; ++rr)
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        const int i = i0 + c * 32 + tx, j = j0 + ty + rr * NW;
+        const bool in = i < g.nx && j < g.ny;
+        const long k = g.at(in ? i : 0, in ? j : 0);
+        xs[rr][c] = X[k];
+        ds[rr][c] = kUnscaled ? fabs(Ct[k]) : 0.0;
+      }
     if (threadIdx.x == 0) s_ok = mbar_wait(&bars[st], (seq >> 1) & 1, kBarrierTimeoutNs);
     __syncthreads();
     if (!s_ok) {
@@ -209,7 +226,7 @@ __device__ __forceinline__ bool sweep(const SweepMaps &m, T *rn_out, T *pn_out, 
       return false;
     }
     mbar_wait(&bars[st], (seq >> 1) & 1, kBarrierTimeoutNs);  // completed: acquire in every thread
-    Stage<T> s(smem + st * B::kStageBytes);
+    Stage<T, TH> s(smem + st * B::kStageBytes);
 
     // pass A: p_i = r~_i + beta p_{i-1} on the whole box
     {
@@ -227,55 +244,62 @@ __device__ __forceinline__ bool sweep(const SweepMaps &m, T *rn_out, T *pn_out, 
     }
     __syncthreads();
 
-    // pass B: r~_{i+1} = r~_i - alpha A~ p_i on the tile (4 cells per thread) and its ring;
-    // it reads only P, HX, HY besides each thread's own R cells, so R is updated in place
+    // pass B: r~_{i+1} = r~_i - alpha A~ p_i on the tile (4 cells per thread and row) and its
+    // ring; it reads only P, HX, HY besides each thread's own R cells, so R is updated in place
     {
-      T rb[CPT];
+      T rb[RW][CPT];
 #pragma unroll
-      for (int c = 0; c < CPT; ++c) {
-        const int q = B::q(c * 32 + tx, ty);
-        const T sv = apply<T>(s.P, s.HX, s.HY, q);
-        rb[c] = s.R[q] - alpha * sv;
-        if (i0 + c * 32 + tx < g.nx && j < g.ny) {
-          red[2] += (double)rb[c] * (double)sv;
-          red[4] += (double)s.P[q] * (double)sv;
+      for (int rr = 0; rr < RW; ++rr)
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          const int ly = ty + rr * NW;
+          const int q = B::q(c * 32 + tx, ly);
+          const T sv = apply<T>(s.P, s.HX, s.HY, q);
+          rb[rr][c] = s.R[q] - alpha * sv;
+          if (i0 + c * 32 + tx < g.nx && j0 + ly < g.ny) {
+            red[2] += (double)rb[rr][c] * (double)sv;
+            red[4] += (double)s.P[q] * (double)sv;
+          }
         }
-      }
-      T rring[kRingPer];
-      int qr[kRingPer];
+      T rring[B::kRingPer];
+      int qr[B::kRingPer];
 #pragma unroll
-      for (int t = 0; t < kRingPer; ++t) {
+      for (int t = 0; t < B::kRingPer; ++t) {
         const int e = threadIdx.x + t * kCgThreads;
-        qr[t] = e < kRing ? B::ring(e) : 0;
-        rring[t] = e < kRing ? s.R[qr[t]] - alpha * apply<T>(s.P, s.HX, s.HY, qr[t]) : T(0);
+        qr[t] = e < B::kRing ? B::ring(e) : 0;
+        rring[t] = e < B::kRing ? s.R[qr[t]] - alpha * apply<T>(s.P, s.HX, s.HY, qr[t]) : T(0);
       }
 #pragma unroll
-      for (int c = 0; c < CPT; ++c) s.R[B::q(c * 32 + tx, ty)] = rb[c];
+      for (int rr = 0; rr < RW; ++rr)
 #pragma unroll
-      for (int t = 0; t < kRingPer; ++t)
-        if (threadIdx.x + t * kCgThreads < kRing) s.R[qr[t]] = rring[t];
+        for (int c = 0; c < CPT; ++c) s.R[B::q(c * 32 + tx, ty + rr * NW)] = rb[rr][c];
+#pragma unroll
+      for (int t = 0; t < B::kRingPer; ++t)
+        if (threadIdx.x + t * kCgThreads < B::kRing) s.R[qr[t]] = rring[t];
     }
     __syncthreads();
 
     // pass C: w = A~ r~_{i+1}; sums; X_{i+1} = X_i + alpha p_i; store r~, p, X
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-      const int i = i0 + c * 32 + tx;
-      if (i < g.nx && j < g.ny) {
-        const int q = B::q(c * 32 + tx, ty);
-        const T u = s.R[q], pc = s.P[q];
-        const T wv = apply<T>(s.R, s.HX, s.HY, q);
-        const double ud = u;
-        red[0] += ud * ud;
-        red[1] += (double)wv * ud;
-        red[3] += (double)pc * (double)wv;
-        red[5] += kUnscaled ? ds[c] * (ud * ud) : ud * ud;
-        const long k = g.at(i, j);
-        X[k] = xs[c] + alpha * pc;
-        rn_out[k] = u;
-        pn_out[k] = pc;
+    for (int rr = 0; rr < RW; ++rr)
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        const int i = i0 + c * 32 + tx, ly = ty + rr * NW, j = j0 + ly;
+        if (i < g.nx && j < g.ny) {
+          const int q = B::q(c * 32 + tx, ly);
+          const T u = s.R[q], pc = s.P[q];
+          const T wv = apply<T>(s.R, s.HX, s.HY, q);
+          const double ud = u;
+          red[0] += ud * ud;
+          red[1] += (double)wv * ud;
+          red[3] += (double)pc * (double)wv;
+          red[5] += kUnscaled ? ds[rr][c] * (ud * ud) : ud * ud;
+          const long k = g.at(i, j);
+          X[k] = xs[rr][c] + alpha * pc;
+          rn_out[k] = u;
+          pn_out[k] = pc;
+        }
       }
-    }
     __syncthreads();  // stage st is free for the tile after next
   }
   // this thread's global writes before the next sweep's TMA reads (other blocks)
@@ -284,20 +308,21 @@ __device__ __forceinline__ bool sweep(const SweepMaps &m, T *rn_out, T *pn_out, 
 }
 
 // delta0 = (A~ v, v) of a stored scaled vector v (plain halo loads into stage 0).
-template <typename T>
+template <typename T, int TH = kTH>
 __device__ __forceinline__ double first_delta(const T *V, const T *HXg, const T *HYg, const Grid &g,
                                               const TileIt &ti, unsigned rank, unsigned nb,
                                               unsigned char *smem) {
-  using B = Box<T>;
+  using B = Box<T, TH>;
+  constexpr int RW = B::kRowsPerWarp, NW = kCgThreads / 32;
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   double d0 = 0.0;
-  Stage<T> s(smem);
+  Stage<T, TH> s(smem);
   for (int tile = rank; tile < ti.ntiles; tile += nb) {
     int i0, j0;
-    tile_origin(ti, tile, &i0, &j0);
+    B::origin(ti, tile, &i0, &j0);
     __syncthreads();
     // V, Hx, Hy of the tile and its one-cell ring (zeros outside the interior)
-    for (int e = threadIdx.x; e < (kTW + 2) * (kTH + 2); e += kCgThreads) {
+    for (int e = threadIdx.x; e < (kTW + 2) * (TH + 2); e += kCgThreads) {
       const int ly = e / (kTW + 2) - 1, lx = e % (kTW + 2) - 1;
       const int i = i0 + lx, jj = j0 + ly;
       const bool in = (unsigned)i < (unsigned)g.nx && (unsigned)jj < (unsigned)g.ny;
@@ -308,15 +333,16 @@ __device__ __forceinline__ double first_delta(const T *V, const T *HXg, const T 
       s.HY[q] = in ? __ldcg(HYg + k) : T(0);
     }
     __syncthreads();
-    const int j = j0 + ty;
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-      const int i = i0 + c * 32 + tx;
-      if (i < g.nx && j < g.ny) {
-        const int q = B::q(c * 32 + tx, ty);
-        d0 += (double)apply<T>(s.R, s.HX, s.HY, q) * (double)s.R[q];
+    for (int rr = 0; rr < RW; ++rr)
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        const int i = i0 + c * 32 + tx, ly = ty + rr * NW, j = j0 + ly;
+        if (i < g.nx && j < g.ny) {
+          const int q = B::q(c * 32 + tx, ly);
+          d0 += (double)apply<T>(s.R, s.HX, s.HY, q) * (double)s.R[q];
+        }
       }
-    }
   }
   __syncthreads();
   return d0;
@@ -541,7 +567,12 @@ static __device__ __forceinline__ int cg1_mixed(const View &w, const Cg1Maps *__
   const double *Ct = w.Ct, *Gx = w.Gx, *Gy = w.Gy;
   double *const X = w.x;
   float *const FD = w.fd;
-  if (threadIdx.x == 0) acquire_maps(&m->fr[0], 6);
+  if (threadIdx.x == 0) acquire_maps(&m->tfr[0], 6);
+  // the inner sweeps' tiles: 128 x 32
+  TileIt ti2;
+  ti2.ntx = ti.ntx;
+  ti2.nty = (ny + kTallTH - 1) / kTallTH;
+  ti2.ntiles = ti2.ntx * ti2.nty;
 
   // ---- setup: x = x0 (FP64, unscaled), FP32 scaled couplings with the row flag
   for (int tile = rank; tile < ti.ntiles; tile += nb) {
@@ -626,7 +657,7 @@ static __device__ __forceinline__ int cg1_mixed(const View &w, const Cg1Maps *__
     const double g0 = acc[0];
     double gamma = g0, delta;
     {
-      double d0[1] = {first_delta<float>(w.fr0, w.fhx, w.fhy, g, ti, rank, nb, smem)};
+      double d0[1] = {first_delta<float, kTallTH>(w.fr0, w.fhx, w.fhy, g, ti2, rank, nb, smem)};
       if (!grid_allreduce<1, kRedStride>(d0, sc, partials, totals, nb, rank)) return 0;
       delta = d0[0];
     }
@@ -639,9 +670,9 @@ static __device__ __forceinline__ int cg1_mixed(const View &w, const Cg1Maps *__
       ++it;
       float *rn_out = cur ? w.fr0 : w.fr1, *pn_out = cur ? w.fp0 : w.fp1;
       double red[6] = {0, 0, 0, 0, 0, 0};
-      const SweepMaps sm{&m->fr[cur], &m->fp[cur], &m->fhx, &m->fhy};
-      if (!sweep<float, false, float>(sm, rn_out, pn_out, FD, Ct, g, ti, rank, nb, (float)alpha,
-                                      (float)beta, red, smem, bars, seq, sc))
+      const SweepMaps sm{&m->tfr[cur], &m->tfp[cur], &m->tfhx, &m->tfhy};
+      if (!sweep<float, false, float, kTallTH>(sm, rn_out, pn_out, FD, Ct, g, ti2, rank, nb,
+                                               (float)alpha, (float)beta, red, smem, bars, seq, sc))
         return 0;
       if (!grid_allreduce<6, kRedStride>(red, sc, partials, totals, nb, rank)) return 0;
       gamma_old = gamma;
@@ -684,6 +715,9 @@ static __device__ __forceinline__ int cg1_mixed(const View &w, const Cg1Maps *__
 }
 
 // The domain's solve in its configured precision.
+// kMix: the kernel carries the mixed-precision path too (its FP32 tall-tile
+// sweeps cost registers that the FP64-only kernels do not pay).
+template <bool kMix>
 static __device__ __forceinline__ bool cg1_solve(const View &w, const Cg1Maps *__restrict__ m,
                                                  int x0_surface, int eliminate, unsigned rank,
                                                  unsigned nb, unsigned char *smem,
@@ -692,7 +726,7 @@ static __device__ __forceinline__ bool cg1_solve(const View &w, const Cg1Maps *_
     if (nb == 1 && threadIdx.x == 0) set_status(w.sc, FREHD_ERR_TIMEOUT);
     return false;
   }
-  if (w.p.mixed) {
+  if (kMix && w.p.mixed) {
     const int r = cg1_mixed(w, m, x0_surface, eliminate, rank, nb, smem, bars, seq);
     if (r != 2) return r == 1;
     const bool ok = cg1_fp64(w, m, x0_surface, eliminate, rank, nb, smem, bars, seq);
@@ -720,6 +754,7 @@ static __device__ __forceinline__ bool cg1_smem(unsigned char *smem_raw, unsigne
   return true;
 }
 
+template <bool kMix>
 __global__ void __launch_bounds__(kCgThreads, kCg1MinBlocks)
     k_cg1(View w, const Cg1Maps *__restrict__ m, int x0_surface, int eliminate) {
   if (*(volatile int *)&w.sc->status != FREHD_OK) return;
@@ -741,26 +776,42 @@ __global__ void __launch_bounds__(kCgThreads, kCg1MinBlocks)
   }
   __syncthreads();
   unsigned seq = 0;
-  cg1_solve(s_view, m, x0_surface, eliminate, blockIdx.x, gridDim.x, smem, bars, seq);
+  cg1_solve<kMix>(s_view, m, x0_surface, eliminate, blockIdx.x, gridDim.x, smem, bars, seq);
 }
 
-// Batched solve: CTA c runs jobs[job_start[c] .. job_start[c+1]) in order, each
-// one CTA's share of one domain's solve (rank `rank` of a group of `nb` CTAs,
-// all co-resident in this cooperative launch; a CTA of a multi-CTA group runs
-// no other job).  Each domain's view is taken at its current parity.
+// Batched solve: CTA c first runs jobs[job_start[c] .. job_start[c+1]) in
+// order (its share of a multi-CTA domain's solve: rank `rank` of a group of
+// `nb` CTAs, all co-resident in this cooperative launch), then takes
+// single-CTA solves from the shared list `singles` (largest first; *taken
+// counts the entries handed out, zero at the launch) until none is left, so
+// that the CTAs which finish early carry the rest.  A single-CTA domain's solve
+// is the same whichever CTA runs it.  Each domain's view is taken at its
+// current parity.
+template <bool kMix>
 __global__ void __launch_bounds__(kCgThreads, kCg1MinBlocks)
     k_cg1_batch(const View *__restrict__ views2, const Cg1Maps *const *__restrict__ maps,
-                const int *__restrict__ job_start, const CgJob *__restrict__ jobs) {
+                const int *__restrict__ job_start, const CgJob *__restrict__ jobs,
+                const CgJob *__restrict__ singles, int nsingles, int *taken) {
   extern __shared__ unsigned char smem_raw[];
   __shared__ View s_view;
-  __shared__ int s_cur;
+  __shared__ int s_cur, s_next;
   unsigned char *smem;
   unsigned long long *bars;
   const int q0 = job_start[blockIdx.x], q1 = job_start[blockIdx.x + 1];
   const bool aligned = cg1_smem(smem_raw, &smem, &bars);
   unsigned seq = 0;
-  for (int q = q0; q < q1; ++q) {
-    const CgJob jb = jobs[q];
+  const int nstatic = q1 - q0;
+  for (int n = 0;; ++n) {
+    CgJob jb;
+    if (n < nstatic) {
+      jb = jobs[q0 + n];
+    } else {
+      __syncthreads();  // every thread read the previous s_next
+      if (threadIdx.x == 0) s_next = atomicAdd(taken, 1);
+      __syncthreads();
+      if (s_next >= nsingles) break;
+      jb = singles[s_next];
+    }
     __syncthreads();  // the previous job is done with s_view
     if (threadIdx.x == 0) s_cur = *(volatile int *)&views2[2 * jb.d].sc->cur;
     __syncthreads();
@@ -776,10 +827,11 @@ __global__ void __launch_bounds__(kCgThreads, kCg1MinBlocks)
       if (threadIdx.x == 0) set_status(s_view.sc, FREHD_ERR_CUDA);
       continue;
     }
-    if (!cg1_solve(s_view, maps[jb.d], jb.flags & 1, (jb.flags >> 1) & 1, jb.rank, jb.nb, smem, bars,
-                   seq)) {
-      // this CTA's later jobs are not run: mark their domains failed
-      for (int r = q + 1; r < q1; ++r)
+    if (!cg1_solve<kMix>(s_view, maps[jb.d], jb.flags & 1, (jb.flags >> 1) & 1, jb.rank, jb.nb, smem,
+                         bars, seq)) {
+      // this CTA's later static jobs are not run: mark their domains failed (the
+      // shared list's remaining entries go to the other CTAs)
+      for (int r = q0 + n + 1; r < q1; ++r)
         if (threadIdx.x == 0) set_status(views2[2 * jobs[r].d].sc, FREHD_ERR_TIMEOUT);
       return;
     }
@@ -1064,19 +1116,19 @@ __device__ __forceinline__ void sweep_tile(const Stage<T> &s, const Grid &g, int
         red[4] += (double)s.P[q] * (double)sv;
       }
     }
-    T rring[kRingPer];
-    int qr[kRingPer];
+    T rring[B::kRingPer];
+    int qr[B::kRingPer];
 #pragma unroll
-    for (int t = 0; t < kRingPer; ++t) {
+    for (int t = 0; t < B::kRingPer; ++t) {
       const int e = threadIdx.x + t * kCgThreads;
-      qr[t] = e < kRing ? B::ring(e) : 0;
-      rring[t] = e < kRing ? s.R[qr[t]] - alpha * apply<T>(s.P, s.HX, s.HY, qr[t]) : T(0);
+      qr[t] = e < B::kRing ? B::ring(e) : 0;
+      rring[t] = e < B::kRing ? s.R[qr[t]] - alpha * apply<T>(s.P, s.HX, s.HY, qr[t]) : T(0);
     }
 #pragma unroll
     for (int c = 0; c < CPT; ++c) s.R[B::q(c * 32 + tx, ty)] = rb[c];
 #pragma unroll
-    for (int t = 0; t < kRingPer; ++t)
-      if (threadIdx.x + t * kCgThreads < kRing) s.R[qr[t]] = rring[t];
+    for (int t = 0; t < B::kRingPer; ++t)
+      if (threadIdx.x + t * kCgThreads < B::kRing) s.R[qr[t]] = rring[t];
   }
   __syncthreads();
 #pragma unroll
@@ -1556,13 +1608,13 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-template <typename T>
+template <typename T, int TH = kTH>
 int encode(const Grid &g, T *base, CUtensorMap *out) {
   auto fn = encode_fn();
   if (!fn) return fail(FREHD_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
   const cuuint64_t dims[2] = {(cuuint64_t)g.pitch, (cuuint64_t)(g.ny + 2)};
   const cuuint64_t strides[1] = {(cuuint64_t)g.pitch * sizeof(T)};
-  const cuuint32_t box[2] = {(cuuint32_t)Box<T>::kBW, (cuuint32_t)Box<T>::kBH};
+  const cuuint32_t box[2] = {(cuuint32_t)Box<T, TH>::kBW, (cuuint32_t)Box<T, TH>::kBH};
   const cuuint32_t estr[2] = {1, 1};
   const CUtensorMapDataType dt =
       sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
@@ -1612,6 +1664,13 @@ int cg1_make_maps_f32(const Grid &g, float *r0, float *r1, float *p0, float *p1,
   rc = rc ? rc : encode(g, p1, &m->fp[1]);
   rc = rc ? rc : encode(g, hx, &m->fhx);
   rc = rc ? rc : encode(g, hy, &m->fhy);
+  // the same arrays as the mixed solve's tall inner-sweep boxes
+  rc = rc ? rc : encode<float, kTallTH>(g, r0, &m->tfr[0]);
+  rc = rc ? rc : encode<float, kTallTH>(g, r1, &m->tfr[1]);
+  rc = rc ? rc : encode<float, kTallTH>(g, p0, &m->tfp[0]);
+  rc = rc ? rc : encode<float, kTallTH>(g, p1, &m->tfp[1]);
+  rc = rc ? rc : encode<float, kTallTH>(g, hx, &m->tfhx);
+  rc = rc ? rc : encode<float, kTallTH>(g, hy, &m->tfhy);
   return rc;
 }
 
@@ -1620,11 +1679,13 @@ size_t cg1_smem_bytes() { return (size_t)kSmemStages + 2 * sizeof(unsigned long 
 
 int cg1_blocks(int device, const Grid &g, int *blocks) {
   static const size_t smem = cg1_smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(k_cg1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(k_cg1<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_cg1<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return fail(FREHD_ERR_CUDA, "k_cg1 shared memory: %s", cudaGetErrorString(e));
   int nsm = 0, per = 0;
   e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg1, kCgThreads, smem);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg1<true>, kCgThreads, smem);
   if (e != cudaSuccess) return fail(FREHD_ERR_CUDA, "k_cg1 occupancy: %s", cudaGetErrorString(e));
   if (per < 1) return fail(FREHD_ERR_CUDA, "k_cg1 does not fit on an SM");
   const long ntiles = (long)((g.nx + CTX - 1) / CTX) * ((g.ny + CTY - 1) / CTY);
@@ -1635,20 +1696,24 @@ int cg1_blocks(int device, const Grid &g, int *blocks) {
 
 int cg1_batch_capacity(int device, int *ctas) {
   static const size_t smem = cg1_smem_bytes();
-  cudaError_t e = cudaFuncSetAttribute(k_cg1_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(k_cg1_batch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_cg1_batch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return fail(FREHD_ERR_CUDA, "k_cg1_batch shared memory: %s", cudaGetErrorString(e));
   int nsm = 0, per = 0;
   e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg1_batch, kCgThreads, smem);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cg1_batch<true>, kCgThreads, smem);
   if (e != cudaSuccess) return fail(FREHD_ERR_CUDA, "k_cg1_batch occupancy: %s", cudaGetErrorString(e));
   *ctas = nsm * (per > 0 ? per : 0);
   return *ctas > 0 ? FREHD_OK : fail(FREHD_ERR_CUDA, "k_cg1_batch does not fit on an SM");
 }
 
 int cg1_launch_batch(const View *views2, const Cg1Maps *const *maps, const int *job_start,
-                     const CgJob *jobs, int nctas, cudaStream_t stream) {
-  void *args[] = {&views2, &maps, &job_start, &jobs};
-  cudaError_t e = cudaLaunchCooperativeKernel((void *)k_cg1_batch, dim3(nctas), dim3(kCgThreads), args,
+                     const CgJob *jobs, const CgJob *singles, int nsingles, int *taken, int nctas,
+                     int any_mixed, cudaStream_t stream) {
+  void *args[] = {&views2, &maps, &job_start, &jobs, &singles, &nsingles, &taken};
+  void *fn = any_mixed ? (void *)k_cg1_batch<true> : (void *)k_cg1_batch<false>;
+  cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(nctas), dim3(kCgThreads), args,
                                               cg1_smem_bytes(), stream);
   if (e != cudaSuccess) return fail(FREHD_ERR_CUDA, "k_cg1_batch launch: %s", cudaGetErrorString(e));
   return FREHD_OK;
@@ -1660,7 +1725,8 @@ int cg1_launch(const View &w, const Cg1Maps *m_dev, int blocks, int x0_surface, 
   const Cg1Maps *mp = m_dev;
   int x0 = x0_surface, el = eliminate;
   void *args[] = {&wv, &mp, &x0, &el};
-  cudaError_t e = cudaLaunchCooperativeKernel((void *)k_cg1, dim3(blocks), dim3(kCgThreads), args,
+  void *fn = w.p.mixed ? (void *)k_cg1<true> : (void *)k_cg1<false>;
+  cudaError_t e = cudaLaunchCooperativeKernel(fn, dim3(blocks), dim3(kCgThreads), args,
                                               cg1_smem_bytes(), stream);
   if (e != cudaSuccess) return fail(FREHD_ERR_CUDA, "k_cg1 launch: %s", cudaGetErrorString(e));
   return FREHD_OK;

@@ -17,6 +17,7 @@ namespace frehd {
 struct Cg1Maps {
   CUtensorMap r[2], p[2], hx, hy;
   CUtensorMap fr[2], fp[2], fhx, fhy;
+  CUtensorMap tfr[2], tfp[2], tfhx, tfhy;  // the FP32 arrays as 128 x 32-tile boxes
 };
 
 int cg1_make_maps(const Grid &g, double *r0, double *r1, double *p0, double *p1, double *hx,
@@ -42,9 +43,12 @@ struct CgJob {
   int nb;     // CTAs of the group (all co-resident)
   int flags;  // bit 0: x0 = surface; bit 1: decoupled rows eliminated
 };
-// Launch the batched solve: nctas CTAs, CTA c runs jobs[job_start[c] .. job_start[c+1]).
+// Launch the batched solve: nctas CTAs, CTA c runs jobs[job_start[c] ..
+// job_start[c+1]), then single-CTA jobs from `singles` (nsingles of them;
+// *taken zero at the launch, reset by k_finish_batch).
 int cg1_launch_batch(const View *views2, const Cg1Maps *const *maps, const int *job_start,
-                     const CgJob *jobs, int nctas, cudaStream_t stream);
+                     const CgJob *jobs, const CgJob *singles, int nsingles, int *taken, int nctas,
+                     int any_mixed, cudaStream_t stream);
 // CTAs of the batched solve that fit on the device at once.
 int cg1_batch_capacity(int device, int *ctas);
 

@@ -42,7 +42,8 @@ __global__ void k_fill(double *a, long n, double v);
 // Batched launches over many domains (views2[2*d + half]: domain d's view with
 // ping-pong half `half` current).
 struct BatchTile {
-  int d, bx, by, gx;  // domain slot, tile coordinates, the domain's tile-grid width
+  int d, bx, by, gx;  // domain slot, first tile's coordinates, the domain's tile-grid width
+  int nt, pad;        // tiles nt along x from (bx, by), one after another in one block
 };
 struct FinishJob {
   int d, nblocks_vel;  // domain slot, its k_update_vel tile count
@@ -52,6 +53,7 @@ struct FinishJob {
 __global__ void k_explicit_batch(const View *views2, const BatchTile *tiles);
 __global__ void k_update_geo_batch(const View *views2, const BatchTile *tiles);
 __global__ void k_update_vel_batch(const View *views2, const BatchTile *tiles);
+__global__ void k_update_vel_tvd_batch(const View *views2, const BatchTile *tiles);
 __global__ void k_finish_batch(const View *views2, const FinishJob *jobs, Scratch *bsync);
 __global__ void k_interp_velocity(View w, double *uuYP, double *vvXP);
 __global__ void k_system_to_ref(View w, double *GnCt, double *GnXP, double *GnXM, double *GnYP,

@@ -293,10 +293,17 @@ __device__ __forceinline__ double level_surf(const Params &p, int k) {
 // Table values of cell (i, j) at level k: all ten, or (part) only the west- or
 // south-face pair.  zs: the cell's first fine pixel in the block's staged
 // window of fine bottoms (row pitch kFineBoxW), or null to read them from zf.
+// bz: the cell's bottom with the offset (the minimum of its fine bottoms): a
+// level below it leaves every fine depth zero, and then every value is +0,
+// exactly what the evaluation would add up (the margin covers the two
+// roundings of the offset).
 __device__ __forceinline__ void level_values(const Params &p, int i, int j, int k, frehd_cell_levels *o,
-                                             int part, const double *zs) {
+                                             int part, const double *zs, double bz) {
   if (p.geom_fine) {
-    if (zs)
+    if (frehd_level(p.surfmin, p.dsurf, k) + p.offset < bz - 1e-9) {
+      o->V = o->Z = o->Vxp = o->Vxm = o->Vyp = o->Vym = 0.0;
+      o->Np = o->Nm = o->Op = o->Om = 0.0;
+    } else if (zs)
       frehd_cell_levels_r4_at(zs, kFineBoxW, p.nx, p.ny, i, j, frehd_level(p.surfmin, p.dsurf, k),
                               p.dxf * p.dyf, p.dxf, part, o);
     else if (p.r == 4 && !p.check_block)
@@ -342,8 +349,9 @@ __device__ SubCell compute_sub_area(const View &w, int i, int j, double s, int *
   else j2 = s > level_surf(p, j1) ? j1 + 1 : j1 - 1;
   const double a1 = level_surf(p, j1), a2 = level_surf(p, j2);
   frehd_cell_levels L1, L2;
-  level_values(p, i, j, j1, &L1, PART, zs);
-  if (j2 != j1) level_values(p, i, j, j2, &L2, PART, zs); else L2 = L1;
+  const double bzc = rd(w.bottomZ, g, i, j);
+  level_values(p, i, j, j1, &L1, PART, zs, bzc);
+  if (j2 != j1) level_values(p, i, j, j2, &L2, PART, zs, bzc); else L2 = L1;
   SubCell c;
 #define FREHD_FACE(out, wd, f)                                                         \
   {                                                                                    \
@@ -1120,13 +1128,19 @@ static __device__ __forceinline__ void stage_view(const View *views2, int d, Vie
   __syncthreads();
 }
 
+// A block stages its domain's view once and runs the tile code on t.nt
+// consecutive tiles of one tile row (the barrier between them frees the
+// tile's shared memory for the next).
 __global__ void __launch_bounds__(TBX *TBY, 4) k_explicit_batch(const View *views2, const BatchTile *tiles) {
   __shared__ View sv;
   __shared__ int s_cur;
   const BatchTile t = tiles[blockIdx.x];
   stage_view(views2, t.d, &sv, &s_cur, threadIdx.y * TBX + threadIdx.x, TBX * TBY);
   if (*(volatile int *)&sv.sc->status != FREHD_OK) return;
-  explicit_tile(sv, t.bx, t.by);
+  for (int q = 0; q < t.nt; ++q) {
+    if (q) __syncthreads();
+    explicit_tile(sv, t.bx + q, t.by);
+  }
 }
 
 __global__ void __launch_bounds__(TBX *TBY, FREHD_GEO_MIN_BLOCKS)
@@ -1136,19 +1150,37 @@ __global__ void __launch_bounds__(TBX *TBY, FREHD_GEO_MIN_BLOCKS)
   const BatchTile t = tiles[blockIdx.x];
   stage_view(views2, t.d, &sv, &s_cur, threadIdx.y * TBX + threadIdx.x, TBX * TBY);
   if (*(volatile int *)&sv.sc->status != FREHD_OK) return;
-  update_geo_tile<false>(sv, t.bx, t.by);
+  for (int q = 0; q < t.nt; ++q) {
+    if (q) __syncthreads();  // also: the window's mbarrier is re-armed only after every wait on it
+    update_geo_tile<false>(sv, t.bx + q, t.by);
+  }
 }
 
-__global__ void __launch_bounds__(TBX *TBY) k_update_vel_batch(const View *views2, const BatchTile *tiles) {
+// Upwind and TVD domains in kernels of their own (the batch orders its tiles
+// upwind first), so that the TVD stencil's registers do not cost the upwind
+// kernel its four blocks per SM.
+__global__ void __launch_bounds__(TBX *TBY, 4) k_update_vel_batch(const View *views2, const BatchTile *tiles) {
   __shared__ View sv;
   __shared__ int s_cur;
   const BatchTile t = tiles[blockIdx.x];
   stage_view(views2, t.d, &sv, &s_cur, threadIdx.y * TBX + threadIdx.x, TBX * TBY);
   if (*(volatile int *)&sv.sc->status != FREHD_OK) return;
-  if (sv.p.scalarAdv == 2)
-    update_vel_tile<true>(sv, t.bx, t.by, t.gx);
-  else
-    update_vel_tile<false>(sv, t.bx, t.by, t.gx);
+  for (int q = 0; q < t.nt; ++q) {
+    if (q) __syncthreads();
+    update_vel_tile<false>(sv, t.bx + q, t.by, t.gx);
+  }
+}
+
+__global__ void __launch_bounds__(TBX *TBY) k_update_vel_tvd_batch(const View *views2, const BatchTile *tiles) {
+  __shared__ View sv;
+  __shared__ int s_cur;
+  const BatchTile t = tiles[blockIdx.x];
+  stage_view(views2, t.d, &sv, &s_cur, threadIdx.y * TBX + threadIdx.x, TBX * TBY);
+  if (*(volatile int *)&sv.sc->status != FREHD_OK) return;
+  for (int q = 0; q < t.nt; ++q) {
+    if (q) __syncthreads();
+    update_vel_tile<true>(sv, t.bx + q, t.by, t.gx);
+  }
 }
 
 // One block per domain: k_finish's work, then the domain's ping-pong half flips.

@@ -404,12 +404,14 @@ int frehd_cg_solve_noalloc(int nx, int ny, const double *Ct, const double *Gx, c
  * capture).  A domain's results do not depend on which other domains share the
  * batch.  The solve of all domains is one cooperative launch in one of two
  * packings (frehd_batch_set_cg_packing):
- *   FREHD_BATCH_TILE_LIST (default): every domain's CG tiles form one list spread
- *     over all CTAs; a domain's sums are added in its own tile order, so its
- *     result is the same in any mix; cells_per_cta is not used, and admission is
- *     by memory alone;
- *   FREHD_BATCH_CTA_GROUPS: a domain's CG runs on round(cells / cells_per_cta)
- *     CTAs (at least one) whatever the mix; admission also needs free CTAs.
+ *   FREHD_BATCH_CTA_GROUPS (default): a domain's CG runs on
+ *     ceil(cells / cells_per_cta) CTAs (at most its tile count) whatever the mix; the
+ *     single-CTA solves, largest first, go to whichever CTA is free; admission
+ *     also needs free CTAs;
+ *   FREHD_BATCH_TILE_LIST: every domain's CG tiles form one list spread over
+ *     all CTAs; a domain's sums are added in its own tile order, so its result is
+ *     the same in any mix; cells_per_cta is not used, and admission is by memory
+ *     alone.
  * The two packings add the solve's partial sums in different orders: their
  * results agree to the solver's rounding, not bit for bit.
  */
@@ -418,7 +420,8 @@ typedef struct frehd_batch_info_t {
   int domains;             /* admitted domains */
   int cg_ctas;             /* CTAs of the batched CG launch */
   int cg_capacity;         /* CTAs the device holds at once for it */
-  long tiles;              /* stencil tiles per step over all domains */
+  long tiles;              /* blocks of each stencil kernel per step over all domains (each
+                              runs up to four 32 x 8 tiles of one domain) */
   int graph;               /* 1: steps replay a captured CUDA graph */
   long long bytes_used, bytes_budget;
   long long steps;         /* batch steps taken */
@@ -426,7 +429,8 @@ typedef struct frehd_batch_info_t {
 
 /* Device memory a domain of this configuration holds, with r x r fine bottoms. */
 int frehd_domain_footprint(const frehd_config *cfg, int r, long long *bytes);
-/* cells_per_cta: cells of a domain per CTA of its CG (the packing granularity). */
+/* cells_per_cta: cells of a domain per CTA of its CG (the packing granularity):
+ * in the CTA-group packing a domain's CG runs on ceil(cells / cells_per_cta) CTAs. */
 int frehd_batch_create(int device, long long hbm_budget_bytes, double cells_per_cta,
                        frehd_batch **out);
 /* Domains still admitted are handed back to their owners (not destroyed). */

@@ -3,7 +3,7 @@ sub-step over all of them.
 
 A domain's arithmetic in a batch is the single-domain step's: the stencil
 kernels run the same tile code.  Its solve depends on the packing:
-* CTA groups: its CG runs on round(cells/cells_per_cta) CTAs; with
+* CTA groups: its CG runs on ceil(cells/cells_per_cta) CTAs; with
   cells_per_cta = 1 (as many CTAs as the single-domain solve uses) a batch
   reproduces single-domain runs bit for bit;
 * the tile list (default): the same sweeps over the domain's tiles, with the

@@ -38,6 +38,7 @@ ranks; the batched mix and the request stream are partitioned over the ranks.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -581,6 +582,24 @@ def _worst(errs: list) -> dict | None:
     return {k: max(e[k] for e in errs) for k in errs[0]} if errs else None
 
 
+def _fp64_batch_run(decks, dev, budget, packing, cpc, steps):
+    """Fresh FP64 domains of `decks` stepped `steps` times in one batch; the
+    domains (released from the batch, still open) are returned."""
+    from frehdc_b200 import native
+    doms = [native.domain_from_deck(dk, device=dev) for dk in decks]
+    b = native.Batch(budget, cpc, dev)
+    b.set_cg_packing(packing)
+    for g in doms:
+        b.admit(g, 1)
+    for _ in range(steps):
+        b.step()
+    b.sync()
+    for sl in list(b.members):
+        b.release(sl)
+    b.close()
+    return doms
+
+
 def measure_batched(args, ws, rank, dev, n_mix, smin, smax, scalars, total_steps, precision,
                     K, W):
     """A mix of basins stepped as one batch (one launch per sub-step for all of
@@ -674,39 +693,44 @@ def measure_batched(args, ws, rank, dev, n_mix, smin, smax, scalars, total_steps
         for sl in list(fb.members):
             fb.release(sl)
         fb.close()
-        # the noise floor: the same FP64 steps with the solve's sums added in the
-        # other packing's order; wet/dry branches amplify any rounding difference
+        # two noise floors of the FP64 run itself: the same steps with the
+        # solve's sums added in the other packing's order (rounding only), and
+        # with the CG tolerance tightened tenfold (another solution that meets
+        # the same residual bound); wet/dry branches amplify either difference
         other = native.BATCH_CTA_GROUPS if pk == native.BATCH_TILE_LIST else native.BATCH_TILE_LIST
-        alt = [native.domain_from_deck(dk, device=dev) for dk in decks]
-        ob = native.Batch(budget, 393216.0, dev)
-        ob.set_cg_packing(other)
-        for g in alt:
-            ob.admit(g, 1)
-        for _ in range(total_steps):
-            ob.step()
-        ob.sync()
-        for sl in list(ob.members):
-            ob.release(sl)
-        ob.close()
-        per, floor = [], []
         names = ["surf", "uuXP", "vvYP"]
-        for g, r, h, dk in zip(doms, ref, alt, decks):
+        ref_state = [(r.download(names), r.stats()["volume"]) for r in ref]
+
+        def spread(run):  # each floor run's domains compared, then closed
+            out = []
+            for h, (rs, vr), dk in zip(run, ref_state, decks):
+                f = _state_errors(h.download(names), rs, dk.spec.nx * dk.spec.ny)
+                f["volume_rel"] = abs(h.stats()["volume"] - vr) / abs(vr)
+                out.append(f)
+                h.close()
+            return out
+
+        per = []
+        for g, r, (rs, vr), dk in zip(doms, ref, ref_state, decks):
             n_ = dk.spec.nx * dk.spec.ny
-            rs = r.download(names)
             e = _state_errors(g.download(names), rs, n_)
             e["scalar_max_abs"] = max(float(np.max(np.abs(
                 g.download_scalar(s_)[:n_] - r.download_scalar(s_)[:n_])))
                 for s_ in range(1 + len(dk.tracers)))
-            va, vr = g.stats()["volume"], r.stats()["volume"]
-            e["volume_rel"] = abs(va - vr) / abs(vr)
+            e["volume_rel"] = abs(g.stats()["volume"] - vr) / abs(vr)
             per.append(e)
-            f = _state_errors(h.download(names), rs, n_)
-            f["volume_rel"] = abs(h.stats()["volume"] - vr) / abs(vr)
-            floor.append(f)
-            h.close()
+        floor = spread(_fp64_batch_run(decks, dev, budget, other, 393216.0, total_steps))
+        tight_decks = [dataclasses.replace(dk, spec=dataclasses.replace(dk.spec, eps=dk.spec.eps / 10))
+                       for dk in decks]
+        tfloor = spread(_fp64_batch_run(tight_decks, dev, budget, pk, cpc if cpc > 0 else 1.0,
+                                        total_steps))
+        over = lambda es: sum(1 for e in es if e["eta_max_abs_m"] > 1e-6)  # noqa: E731
         errors = {"mixed": _worst(per), "fp64_other_order": _worst(floor),
-                  "domains_eta_over_1e-6": sum(1 for e in per if e["eta_max_abs_m"] > 1e-6),
-                  "domains_fp64_eta_over_1e-6": sum(1 for e in floor if e["eta_max_abs_m"] > 1e-6)}
+                  "fp64_tighter_eps": _worst(tfloor),
+                  "domains_eta_over_1e-6": over(per), "domains_fp64_eta_over_1e-6": over(floor),
+                  "domains_tight_eta_over_1e-6": over(tfloor),
+                  "over_1e-6_both": sum(1 for a, c in zip(per, tfloor)
+                                        if a["eta_max_abs_m"] > 1e-6 and c["eta_max_abs_m"] > 1e-6)}
     for g in doms + ref:
         g.close()
     parts = shard.gather({"batch_ms": batch_ms, "plain_ms": plain_ms, "cells": int(sum(cells)),
@@ -750,6 +774,13 @@ def measure_batched(args, ws, rank, dev, n_mix, smin, smax, scalars, total_steps
                 "domains_over_1e-6_m": sum(e["domains_fp64_eta_over_1e-6"] for e in errs),
                 "note": "the same FP64 steps with the solve's partial sums added in the other "
                         "packing's order: the spread any rounding difference grows to"}
+            rec["fp64_vs_fp64_tighter_eps"] = {
+                **_worst([e["fp64_tighter_eps"] for e in errs]),
+                "domains_over_1e-6_m": sum(e["domains_tight_eta_over_1e-6"] for e in errs),
+                "domains_over_1e-6_m_in_both": sum(e["over_1e-6_both"] for e in errs),
+                "note": "the same FP64 steps with the CG tolerance 1e-13 instead of 1e-12: the "
+                        "spread between two solutions that both meet the FP64 residual bound; "
+                        "in_both counts domains over 1e-6 m here and in the mixed run"}
     return rec
 
 

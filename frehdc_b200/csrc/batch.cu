@@ -186,7 +186,7 @@ int launch_step(frehd_batch *b) {
                                  b->nsingles, &b->bsync.p->n_done, b->nctas, b->any_mixed,
                                  b->stream);
   if (rc) return rc;
-  k_update_geo_batch<<<(unsigned)b->ntiles, bb, kGeoDynSmem, b->stream>>>(b->views2.p, b->tiles.p);
+  k_update_geo_batch<<<(unsigned)b->ntiles, bb, 0, b->stream>>>(b->views2.p, b->tiles.p);
   if (b->ntiles_upwind > 0)
     k_update_vel_batch<<<(unsigned)b->ntiles_upwind, bb, 0, b->stream>>>(b->views2.p, b->tiles.p);
   if (b->ntiles > b->ntiles_upwind)
@@ -396,6 +396,7 @@ extern "C" int frehd_domain_footprint(const frehd_config *cfg, int r, long long 
   b += 4 * N + 2 * 8 * T;           // fix list, staging
   b += 8 * std::max(nvel, 8LL * 148 + 8) + 4096;  // partials, scratch, maps
   b += 8 * N * (long long)r * r;    // fine bottoms
+  b += (20 * 8 + 2 * 4) * tot;      // level-value cache of the fine geometry
   *bytes = b;
   return FREHD_OK;
 }
@@ -410,9 +411,7 @@ extern "C" int frehd_batch_create(int device, long long hbm_budget_bytes, double
   b->device = device;
   b->budget = hbm_budget_bytes;
   b->cells_per_cta = cells_per_cta;
-  int rc = geo_kernels_setup() == cudaSuccess ? FREHD_OK
-                                              : fail(FREHD_ERR_CUDA, "k_update_geo shared memory attribute");
-  if (!rc) rc = cg1_batch_capacity(device, &b->capacity);
+  int rc = cg1_batch_capacity(device, &b->capacity);
   if (!rc) rc = cg1_tiles_capacity(device, &b->capacity_tiles);
   if (!rc && cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
     rc = fail(FREHD_ERR_CUDA, "stream creation failed");

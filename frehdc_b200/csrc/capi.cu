@@ -91,7 +91,7 @@ View make_view_at(const frehd_domain *d, int cur) {
   w.EnXP = d->EnXP; w.EnYP = d->EnYP; w.Gx = d->Gx; w.Gy = d->Gy; w.Ct = d->Ct; w.b = d->b;
   w.Hx = d->Hx; w.Hy = d->Hy;
   w.fr0 = d->fr0; w.fr1 = d->fr1; w.fp0 = d->fp0; w.fp1 = d->fp1; w.fd = d->fd;
-  w.fhx = d->fhx; w.fhy = d->fhy;
+  w.fhx = d->fhx; w.fhy = d->fhy; w.fs = d->fs;
   w.x = d->x; w.r = d->r; w.p0 = d->p0; w.p1 = d->p1; w.q = d->q;
   w.cellV = d->cellV; w.Sm = d->Sm; w.Fuu = d->Fuu; w.Fvv = d->Fvv;
   w.rmv = d->rmv; w.fix_list = d->fix_list; w.partials = d->partials;
@@ -99,7 +99,8 @@ View make_view_at(const frehd_domain *d, int cur) {
   w.inflow = d->inflow; w.ninflow = d->ninflow;
   w.wspd = d->wspd; w.nwspd = d->nwspd; w.wcos = d->wcos; w.wsin = d->wsin; w.nwdir = d->nwdir;
   w.dXP = d->dXP; w.dYP = d->dYP;
-  w.zf_map = d->zf_map_dev;
+  w.lvc = d->lvc;
+  w.lvi = d->lvi;
   w.sc = d->sc;
   return w;
 }
@@ -222,7 +223,7 @@ void mark(cudaEvent_t *ev, int slot, cudaStream_t st) {
 int launch_update(frehd_domain *d, const View &w, cudaEvent_t *ev = nullptr) {
   const dim3 gb = tile_grid(d), bb(32, 8);
   mark(ev, 2, d->stream);
-  k_update_geo<<<gb, bb, kGeoDynSmem, d->stream>>>(w);
+  k_update_geo<<<gb, bb, 0, d->stream>>>(w);
   mark(ev, 3, d->stream);
   if (d->p.scalarAdv == 2)
     k_update_vel_tvd<<<gb, bb, 0, d->stream>>>(w);
@@ -263,11 +264,6 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
   frehd_domain *d = new frehd_domain();
   d->cfg = *cfg;
   d->device = device;
-  if (geo_kernels_setup() != cudaSuccess) {
-    cudaGetLastError();
-    delete d;
-    return fail(FREHD_ERR_CUDA, "k_update_geo shared memory attribute");
-  }
   if (cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete d;
     return fail(FREHD_ERR_CUDA, "cudaStreamCreate failed");
@@ -372,7 +368,8 @@ extern "C" int frehd_domain_destroy(frehd_domain *d) {
   for (void *p : d->allocs) cudaFree(p);
   if (d->tables) cudaFree(d->tables);
   if (d->zf) cudaFree(d->zf);
-  if (d->zf_map_dev) cudaFree(d->zf_map_dev);
+  if (d->lvc) cudaFree(d->lvc);
+  if (d->lvi) cudaFree(d->lvi);
   if (d->tide) cudaFree(d->tide);
   for (double *a : {d->inflow, d->wspd, d->wcos, d->wsin})
     if (a) cudaFree(a);
@@ -428,23 +425,26 @@ extern "C" int frehd_domain_set_fine_bottoms_ex(frehd_domain *d, int r, const do
                              sizeof(double) * cols, rows, cudaMemcpyHostToDevice, d->stream));
   d->p.geom_fine = 1;
   d->p.zf = d->zf;
-  d->bytes += (long long)(sizeof(double) * rows * cols);
+  d->bytes += (long long)(sizeof(double) * rows * cols) - d->zf_bytes;
+  d->zf_bytes = (long long)(sizeof(double) * rows * cols);
   d->p.fpitch = cols;
   d->p.r = r;
   d->p.check_block = check_block;
-  if (d->zf_map_dev) cudaFree(d->zf_map_dev);
-  d->zf_map_dev = nullptr;
-  if (r == 4 && !check_block) {  // the r = 4 path stages fine-bottom windows by TMA
-    CUtensorMap m;
-    int rc = encode_fine_box(d->zf, cols, rows, &m);
-    if (!rc && cudaMalloc(&d->zf_map_dev, sizeof(CUtensorMap)) != cudaSuccess) {
+  // the level-value cache: allocated once, emptied for every new set of bottoms
+  const long tot = d->gr.total;
+  if (!d->lvc) {
+    const size_t vb = sizeof(double) * 20 * (size_t)tot, ib = sizeof(int) * 2 * (size_t)tot;
+    if (cudaMalloc(&d->lvc, vb) != cudaSuccess || cudaMalloc(&d->lvi, ib) != cudaSuccess) {
       cudaGetLastError();
-      d->zf_map_dev = nullptr;
-      rc = fail(FREHD_ERR_NOMEM, "fine-bottom tensor map");
+      if (d->lvc) cudaFree(d->lvc);
+      d->lvc = nullptr;
+      d->lvi = nullptr;
+      return fail(FREHD_ERR_NOMEM, "level-value cache: %zu bytes", vb + ib);
     }
-    if (rc) return rc;
-    CUDA_TRY(cudaMemcpyAsync(d->zf_map_dev, &m, sizeof(m), cudaMemcpyHostToDevice, d->stream));
+    d->lvc_bytes = (long long)(vb + ib);
+    d->bytes += d->lvc_bytes;
   }
+  CUDA_TRY(cudaMemsetAsync(d->lvi, 0xff, sizeof(int) * 2 * (size_t)tot, d->stream));  // -1: empty
   d->geom_set = 1;
   return FREHD_OK;
 }
@@ -561,7 +561,7 @@ extern "C" int frehd_domain_set_precision(frehd_domain *d, int mode, double eps_
   if (mode == FREHD_PRECISION_MIXED && !d->fr0) {
     const long tot = d->gr.total;
     int r = 0;
-    float **arrs[] = {&d->fr0, &d->fr1, &d->fp0, &d->fp1, &d->fd, &d->fhx, &d->fhy};
+    float **arrs[] = {&d->fr0, &d->fr1, &d->fp0, &d->fp1, &d->fd, &d->fhx, &d->fhy, &d->fs};
     for (auto a : arrs)
       if (!r) r |= dalloc(d, a, tot);
     if (!r) r |= cg1_make_maps_f32(d->gr, d->fr0, d->fr1, d->fp0, d->fp1, d->fhx, d->fhy, &d->cg1_maps);
@@ -853,7 +853,7 @@ extern "C" int frehd_domain_init(frehd_domain *d, const double *bottom, const do
   if (rc) return rc;
   {
     View w = make_view(d);
-    k_update_geo_init<<<tile_grid(d), dim3(32, 8), kGeoDynSmem, d->stream>>>(w);
+    k_update_geo_init<<<tile_grid(d), dim3(32, 8), 0, d->stream>>>(w);
     CUDA_TRY(cudaGetLastError());
     std::swap(d->ind[0], d->ind[1]);  // the evaluated indices become current
   }

@@ -184,7 +184,9 @@ template <typename T, bool kUnscaled, typename XT, int TH = kTH>
 __device__ __forceinline__ bool sweep(const SweepMaps &m, T *rn_out, T *pn_out, XT *X, const double *Ct,
                                       const Grid &g, const TileIt &ti, unsigned rank, unsigned nb,
                                       T alpha, T beta, double (&red)[6], unsigned char *smem,
-                                      unsigned long long *bars, unsigned &seq, Scratch *sc) {
+                                      unsigned long long *bars, unsigned &seq, Scratch *sc,
+                                      bool x_zero = false) {
+  // x_zero: X starts from zero (its stored values are not read)
   using B = Box<T, TH>;
   constexpr int RW = B::kRowsPerWarp, NW = kCgThreads / 32;
   __shared__ int s_ok;
@@ -212,7 +214,7 @@ __device__ __forceinline__ bool sweep(const SweepMaps &m, T *rn_out, T *pn_out, 
         const int i = i0 + c * 32 + tx, j = j0 + ty + rr * NW;
         const bool in = i < g.nx && j < g.ny;
         const long k = g.at(in ? i : 0, in ? j : 0);
-        xs[rr][c] = X[k];
+        xs[rr][c] = x_zero ? XT(0) : X[k];
         ds[rr][c] = kUnscaled ? fabs(Ct[k]) : 0.0;
       }
     if (threadIdx.x == 0) s_ok = mbar_wait(&bars[st], (seq >> 1) & 1, kBarrierTimeoutNs);
@@ -594,6 +596,7 @@ static __device__ __forceinline__ int cg1_mixed(const View &w, const Cg1Maps *__
         const float hxf = fabsf((float)hx);
         w.fhx[k] = ct < 0 ? -hxf : hxf;
         w.fhy[k] = (float)hy;
+        w.fs[k] = (float)(1.0 / d);
         X[k] = x0_surface ? w.surf_cur[k] : 0.0;
       }
     }
@@ -608,8 +611,17 @@ static __device__ __forceinline__ int cg1_mixed(const View &w, const Cg1Maps *__
   };
   double rr = 0.0, rr_prev = 0.0, bnorm = 0.0;
   int it_all = 0, done = 0;
+  // The correction x += d~ * fs (fs = 1/sqrt|Ct| in FP32: the correction
+  // only needs FP32 accuracy, the next residual is exact in FP64 for whatever
+  // x results) of an inner solve is applied inside the next residual pass:
+  // every cell forms that sum for itself and its neighbours (the same
+  // expression, so the same doubles) and writes its own into the other buffer;
+  // x then alternates between w.x and w.q (the FP64 solve's work vector, free
+  // in this form).
+  double *xc = X, *xn = w.q;
+  bool add_fd = false;
   for (int outer = 0; outer < kMaxOuter; ++outer) {
-    // ---- residual in FP64: r = b - A x; r~ = r/sqrt|Ct| in FP32; d~ = 0, p_{-1} = 0
+    // ---- residual in FP64: r = b - A x; r~ = r/sqrt|Ct| in FP32; p_{-1} = 0
     double acc[3] = {0, 0, 0};
     for (int tile = rank; tile < ti.ntiles; tile += nb) {
       int i0, j0;
@@ -621,17 +633,23 @@ static __device__ __forceinline__ int cg1_mixed(const View &w, const Cg1Maps *__
         if (i < nx && j < ny) {
           const long k = g.at(i, j);
           const double ct = Ct[k], bk = w.b[k];
+          auto xval = [&](long kk) -> double {
+            const double x0 = __ldcg(xc + kk);
+            return add_fd ? fma((double)__ldcg(FD + kk), (double)w.fs[kk], x0) : x0;
+          };
           auto xv = [&](long kk) -> double {
             const double cc = Ct[kk];
-            return (elim && cc < 0) ? w.b[kk] / (-cc) : __ldcg(X + kk);
+            return (elim && cc < 0) ? w.b[kk] / (-cc) : xval(kk);
           };
+          const double xk = xval(k);
+          if (add_fd) xn[k] = xk;
           double r;
           if (ct > 0) {
-            const double ax = ct * __ldcg(X + k) - (Gx[k] * xv(k + 1) + Gx[k - 1] * xv(k - 1) +
-                                                    Gy[k] * xv(k + pitch) + Gy[k - pitch] * xv(k - pitch));
+            const double ax = ct * xk - (Gx[k] * xv(k + 1) + Gx[k - 1] * xv(k - 1) +
+                                         Gy[k] * xv(k + pitch) + Gy[k - pitch] * xv(k - pitch));
             r = bk - ax;
           } else {
-            r = bk - (-ct) * __ldcg(X + k);
+            r = bk - (-ct) * xk;
           }
           const float rs = (float)(r / sqrt(fabs(ct)));
           acc[0] += (double)rs * (double)rs;
@@ -639,11 +657,15 @@ static __device__ __forceinline__ int cg1_mixed(const View &w, const Cg1Maps *__
           acc[2] += bk * bk;
           w.fr0[k] = rs;
           w.fp0[k] = 0.0f;
-          FD[k] = 0.0f;
         }
       }
     }
     if (!grid_allreduce<3, kRedStride>(acc, sc, partials, totals, nb, rank)) return 0;
+    if (add_fd) {  // the corrected x is in the other buffer now
+      double *t = xc;
+      xc = xn;
+      xn = t;
+    }
     rr = acc[1];
     if (outer == 0) bnorm = sqrt(acc[2]);
     if (converged(rr, bnorm)) {
@@ -671,8 +693,10 @@ static __device__ __forceinline__ int cg1_mixed(const View &w, const Cg1Maps *__
       float *rn_out = cur ? w.fr0 : w.fr1, *pn_out = cur ? w.fp0 : w.fp1;
       double red[6] = {0, 0, 0, 0, 0, 0};
       const SweepMaps sm{&m->tfr[cur], &m->tfp[cur], &m->tfhx, &m->tfhy};
+      // d~ starts from zero at the inner solve's first sweep
       if (!sweep<float, false, float, kTallTH>(sm, rn_out, pn_out, FD, Ct, g, ti2, rank, nb,
-                                               (float)alpha, (float)beta, red, smem, bars, seq, sc))
+                                               (float)alpha, (float)beta, red, smem, bars, seq, sc,
+                                               it == 1))
         return 0;
       if (!grid_allreduce<6, kRedStride>(red, sc, partials, totals, nb, rank)) return 0;
       gamma_old = gamma;
@@ -684,9 +708,10 @@ static __device__ __forceinline__ int cg1_mixed(const View &w, const Cg1Maps *__
       cur ^= 1;
     }
     it_all += it;
-
-    // ---- x += d~/sqrt|Ct| in FP64 (each block its own cells; the barrier orders
-    //      them before the next residual reads neighbours)
+    add_fd = it > 0;  // the next residual pass applies this solve's correction
+  }
+  if (!done) return 2;
+  if (xc != X) {  // the solution in w.x, where the step reads it (own cells; no barrier after)
     for (int tile = rank; tile < ti.ntiles; tile += nb) {
       int i0, j0;
       tile_origin(ti, tile, &i0, &j0);
@@ -696,14 +721,11 @@ static __device__ __forceinline__ int cg1_mixed(const View &w, const Cg1Maps *__
         const int i = i0 + c * 32 + tx;
         if (i < nx && j < ny) {
           const long k = g.at(i, j);
-          X[k] = X[k] + (double)FD[k] / sqrt(fabs(Ct[k]));
+          X[k] = xc[k];
         }
       }
     }
-    double none[1] = {0};
-    if (!grid_allreduce<1, kRedStride>(none, sc, partials, totals, nb, rank)) return 0;
   }
-  if (!done) return 2;
   if (rank == 0 && threadIdx.x == 0) {
     sc->cg_iters = it_all;
     sc->cg_fallback = 0;
@@ -1638,21 +1660,6 @@ int cg1_make_maps(const Grid &g, double *r0, double *r1, double *p0, double *p1,
   rc = rc ? rc : encode(g, hx, &m->hx);
   rc = rc ? rc : encode(g, hy, &m->hy);
   return rc;
-}
-
-int encode_fine_box(const double *zf, long cols, long rows, CUtensorMap *out) {
-  auto fn = encode_fn();
-  if (!fn) return fail(FREHD_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
-  std::memset(out, 0, sizeof(*out));
-  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)cols * sizeof(double)};
-  const cuuint32_t box[2] = {(cuuint32_t)kFineBoxW, (cuuint32_t)kFineBoxH};
-  const cuuint32_t estr[2] = {1, 1};
-  CUresult e = fn(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double *>(zf), dims, strides,
-                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (e != CUDA_SUCCESS) return fail(FREHD_ERR_CUDA, "cuTensorMapEncodeTiled (fine bottoms) failed (%d)", (int)e);
-  return FREHD_OK;
 }
 
 int cg1_make_maps_f32(const Grid &g, float *r0, float *r1, float *p0, float *p1, float *hx,

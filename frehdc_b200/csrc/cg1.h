@@ -26,9 +26,6 @@ int cg1_make_maps(const Grid &g, double *r0, double *r1, double *p0, double *p1,
 int cg1_make_maps_f32(const Grid &g, float *r0, float *r1, float *p0, float *p1, float *hx,
                       float *hy, Cg1Maps *m);
 size_t cg1_smem_bytes();
-// Tensor map of a domain's fine bottoms (cols x rows doubles, row-major) with the
-// kFineBoxW x kFineBoxH window box k_update_geo stages.
-int encode_fine_box(const double *zf, long cols, long rows, CUtensorMap *out);
 // Co-resident blocks for a cooperative launch, at most one per tile.
 int cg1_blocks(int device, const Grid &g, int *blocks);
 int cg1_launch(const View &w, const Cg1Maps *m_dev, int blocks, int x0_surface, int eliminate,

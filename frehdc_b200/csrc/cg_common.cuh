@@ -42,6 +42,21 @@ static __device__ __forceinline__ bool grid_allreduce(double (&v)[NV], Scratch *
     if (lane == 0) sh[m][wid] = s;
   }
   __syncthreads();
+  if (nblocks == 1) {
+    // A lone block: every thread forms the total the general path would give
+    // (thread 0's fixed-order sum over the warps) from shared memory.  Thread 0
+    // makes the block's writes visible at device scope, as the general path's
+    // fence does, before it issues the next TMA loads.
+#pragma unroll
+    for (int m = 0; m < NV; ++m) {
+      double a = 0;
+      for (int q = 0; q < NWARP; ++q) a += sh[m][q];
+      v[m] = a;
+    }
+    if (threadIdx.x == 0) __threadfence();
+    __syncthreads();  // sh is rewritten by the next call
+    return true;
+  }
   unsigned my_gen = 0;
   if (threadIdx.x == 0) {
 #pragma unroll

@@ -117,6 +117,7 @@ struct View {
   // FP32 arrays of the mixed-precision CG (null unless enabled): scaled residual
   // and direction (two buffers each), correction, scaled couplings
   float *fr0, *fr1, *fp0, *fp1, *fd, *fhx, *fhy;
+  float *fs;  // mixed form: 1/sqrt|Ct| rounded to FP32 (the correction's unscaling)
   double *x, *r, *p0, *p1, *q;
   double *cellV, *Sm, *Fuu, *Fvv;
   unsigned char *rmv;
@@ -131,7 +132,12 @@ struct View {
   const double *wcos, *wsin;   // cos/sin of the wind direction by step (nwdir + 1 entries;
   int nwdir;                   // the last one for steps past the series)
   double *dXP, *dYP;           // face depths of the last updateAllFaceDepth (wind only)
-  const void *zf_map;          // CUtensorMap of the fine bottoms (r = 4 boxes of k_update_geo), or null
+  // Level-value cache of the fine geometry (null with tables): per cell the ten
+  // values of the last two levels it evaluated, one per parity of the level
+  // index; lvc plane (slot * 10 + value) and lvi plane slot (the level held,
+  // -1 = none) are padded grids like every cell array.
+  double *lvc;
+  int *lvi;
   Scratch *sc;
 };
 

@@ -31,7 +31,7 @@ struct frehd_domain {
          *b = nullptr;
   double *Hx = nullptr, *Hy = nullptr;
   float *fr0 = nullptr, *fr1 = nullptr, *fp0 = nullptr, *fp1 = nullptr, *fd = nullptr,
-        *fhx = nullptr, *fhy = nullptr;  // mixed-precision CG (allocated when enabled)
+        *fhx = nullptr, *fhy = nullptr, *fs = nullptr;  // mixed-precision CG (allocated when enabled)
   double *x = nullptr, *r = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr;
   double *cellV = nullptr, *Sm = nullptr, *Fuu = nullptr, *Fvv = nullptr;
   unsigned char *rmv = nullptr;
@@ -44,7 +44,9 @@ struct frehd_domain {
   int ninflow = 0, nwspd = 0, nwdir = 0;
   double *dXP = nullptr, *dYP = nullptr;  // face depths read by the wind term
   double *tables = nullptr, *zf = nullptr;
-  CUtensorMap *zf_map_dev = nullptr;  // window map of the fine bottoms (r = 4, no block check)
+  double *lvc = nullptr;  // level-value cache (fine geometry), 20 planes
+  int *lvi = nullptr;     // its level indices, 2 planes
+  long long zf_bytes = 0, lvc_bytes = 0;
   frehd::Scratch *sc = nullptr;
   frehd::StepOut *out = nullptr;
   frehd::StepOut *out_host = nullptr;  // pinned

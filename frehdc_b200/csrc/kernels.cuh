@@ -64,14 +64,6 @@ __global__ void k_solution_from_ref(View w, const double *xs);
 __global__ void k_cg(View w, int x0_surface, int eliminate);
 
 constexpr int kCgThreads = 512;
-// Window of fine bottoms (r = 4) one k_update_geo block stages: the 32 x 8 cells
-// and a ring of one cell, as 136 x 40 doubles; the dynamic shared memory it takes
-// (with slack to align the TMA destination to 128 bytes).
-constexpr int kFineBoxW = 136, kFineBoxH = 40;
-constexpr unsigned kGeoDynSmem = kFineBoxW * kFineBoxH * 8 + 128;
-// Allow the k_update_geo kernels their dynamic shared memory on the current
-// device (beyond the default 48 KB per block with their static arrays).
-cudaError_t geo_kernels_setup();
 
 }  // namespace frehd
 

@@ -20,7 +20,6 @@
 #include "domain.cuh"
 #include "kernels.cuh"
 #include "subgrid_levels.h"
-#include "tma.cuh"
 
 namespace frehd {
 
@@ -291,22 +290,21 @@ __device__ __forceinline__ double level_surf(const Params &p, int k) {
 }
 
 // Table values of cell (i, j) at level k: all ten, or (part) only the west- or
-// south-face pair.  zs: the cell's first fine pixel in the block's staged
-// window of fine bottoms (row pitch kFineBoxW), or null to read them from zf.
-// bz: the cell's bottom with the offset (the minimum of its fine bottoms): a
-// level below it leaves every fine depth zero, and then every value is +0,
-// exactly what the evaluation would add up (the margin covers the two
-// roundings of the offset).
+// south-face pair.  bz: the cell's bottom with the offset (the minimum of its
+// fine bottoms): a level below it leaves every fine depth zero, and then every
+// value is +0, exactly what the evaluation would add up (the margin covers the
+// two roundings of the offset).
+__device__ __forceinline__ bool level_dry(const Params &p, int k, double bz) {
+  return frehd_level(p.surfmin, p.dsurf, k) + p.offset < bz - 1e-9;
+}
+
 __device__ __forceinline__ void level_values(const Params &p, int i, int j, int k, frehd_cell_levels *o,
-                                             int part, const double *zs, double bz) {
+                                             int part, double bz) {
   if (p.geom_fine) {
-    if (frehd_level(p.surfmin, p.dsurf, k) + p.offset < bz - 1e-9) {
+    if (level_dry(p, k, bz)) {
       o->V = o->Z = o->Vxp = o->Vxm = o->Vyp = o->Vym = 0.0;
       o->Np = o->Nm = o->Op = o->Om = 0.0;
-    } else if (zs)
-      frehd_cell_levels_r4_at(zs, kFineBoxW, p.nx, p.ny, i, j, frehd_level(p.surfmin, p.dsurf, k),
-                              p.dxf * p.dyf, p.dxf, part, o);
-    else if (p.r == 4 && !p.check_block)
+    } else if (p.r == 4 && !p.check_block)
       frehd_cell_levels_r4(p.zf, p.fpitch, p.nx, p.ny, i, j, frehd_level(p.surfmin, p.dsurf, k),
                            p.dxf * p.dyf, p.dxf, part, o);
     else  // every value (a part's caller reads only its own)
@@ -320,6 +318,62 @@ __device__ __forceinline__ void level_values(const Params &p, int i, int j, int 
   }
 }
 
+__device__ __forceinline__ int ld_acquire(const int *a) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(a) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int *a, int v) {
+  asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(a), "r"(v) : "memory");
+}
+
+// level_values through the domain's level-value cache (fine geometry).  The
+// values of a level depend on the fine bottoms alone, and the two levels a
+// cell interpolates between are consecutive, so one even and one odd: each
+// cell keeps the last level of each parity it evaluated (slot = level & 1).
+// PART = FREHD_LV_ALL is the cell's own thread: on a miss it evaluates the
+// level, stores the ten values and then publishes the index (release); no
+// other thread writes the entry.  A halo evaluation (WEST / SOUTH) of another
+// block's cell takes the entry only if the index it acquires is the level it
+// needs -- then the values are the ones published with it -- and otherwise
+// evaluates the level itself.  Either way the doubles are the same.
+template <int PART>
+__device__ __forceinline__ void cell_level(const View &w, int i, int j, long k, int lev,
+                                           frehd_cell_levels *o, double bz) {
+  const Params &p = w.p;
+  if (!p.geom_fine || !w.lvc || level_dry(p, lev, bz)) {
+    level_values(p, i, j, lev, o, PART, bz);
+    return;
+  }
+  const long T = w.gr.total;
+  const int slot = lev & 1;
+  int *ip = w.lvi + slot * T + k;
+  double *c = w.lvc + (long)slot * 10 * T + k;
+  if (PART == FREHD_LV_ALL) {
+    if (*ip == lev) {
+      o->V = c[0]; o->Z = c[T]; o->Vxp = c[2 * T]; o->Vxm = c[3 * T]; o->Vyp = c[4 * T];
+      o->Vym = c[5 * T]; o->Np = c[6 * T]; o->Nm = c[7 * T]; o->Op = c[8 * T]; o->Om = c[9 * T];
+      return;
+    }
+    level_values(p, i, j, lev, o, FREHD_LV_ALL, bz);
+    c[0] = o->V; c[T] = o->Z; c[2 * T] = o->Vxp; c[3 * T] = o->Vxm; c[4 * T] = o->Vyp;
+    c[5 * T] = o->Vym; c[6 * T] = o->Np; c[7 * T] = o->Nm; c[8 * T] = o->Op; c[9 * T] = o->Om;
+    st_release(ip, lev);
+  } else {
+    if (ld_acquire(ip) == lev) {
+      if (PART == FREHD_LV_WEST) {
+        o->Vxm = __ldcg(c + 3 * T);
+        o->Nm = __ldcg(c + 7 * T);
+      } else {
+        o->Vym = __ldcg(c + 5 * T);
+        o->Om = __ldcg(c + 9 * T);
+      }
+      return;
+    }
+    level_values(p, i, j, lev, o, PART, bz);
+  }
+}
+
 struct SubCell {
   double V, Z, Vxp, Vxm, Vyp, Vym, Np, Nm, Op, Om;
 };
@@ -330,7 +384,7 @@ struct SubCell {
 // FREHD_LV_SOUTH only Om and Vym (what the west/south neighbour's face needs).
 template <int PART>
 __device__ SubCell compute_sub_area(const View &w, int i, int j, double s, int *ind_io,
-                                    double depth_old, const double *zs) {
+                                    double depth_old) {
   const Params &p = w.p;
   const Grid &g = w.gr;
   const double ds = p.dsurf;
@@ -349,9 +403,10 @@ __device__ SubCell compute_sub_area(const View &w, int i, int j, double s, int *
   else j2 = s > level_surf(p, j1) ? j1 + 1 : j1 - 1;
   const double a1 = level_surf(p, j1), a2 = level_surf(p, j2);
   frehd_cell_levels L1, L2;
-  const double bzc = rd(w.bottomZ, g, i, j);
-  level_values(p, i, j, j1, &L1, PART, zs, bzc);
-  if (j2 != j1) level_values(p, i, j, j2, &L2, PART, zs, bzc); else L2 = L1;
+  const long kc = g.at(i, j);
+  const double bzc = w.bottomZ[kc];
+  cell_level<PART>(w, i, j, kc, j1, &L1, bzc);
+  if (j2 != j1) cell_level<PART>(w, i, j, kc, j2, &L2, bzc); else L2 = L1;
   SubCell c;
 #define FREHD_FACE(out, wd, f)                                                         \
   {                                                                                    \
@@ -445,40 +500,8 @@ static __device__ __forceinline__ void update_geo_tile(const View &w, int bx, in
   __shared__ double sh_s[EY][EX], sh_Np[EY][EX], sh_Nm[EY][EX], sh_Op[EY][EX], sh_Om[EY][EX];
   __shared__ double sh_Vxp[EY][EX], sh_Vxm[EY][EX], sh_Vyp[EY][EX], sh_Vym[EY][EX];
   __shared__ double sh_V[EY][EX], sh_Z[EY][EX];
-  __shared__ unsigned long long geo_bar;
-  extern __shared__ unsigned char geo_dyn[];
   const int i0 = bx * TBX, j0 = by * TBY;
   const int tid = threadIdx.y * TBX + threadIdx.x;
-  // The fine bottoms of the block's cells and of the pixels its faces and halo
-  // cells read (fine columns 4*i0-4 .. 4*i0+131, rows 4*j0-4 .. 4*j0+35; zero
-  // outside the domain) arrive as one TMA box while the new surface is formed;
-  // the level evaluations then read shared memory.
-  double *box = reinterpret_cast<double *>(geo_dyn + ((128u - (smem_u32(geo_dyn) & 127u)) & 127u));
-  const bool staged = w.zf_map != nullptr && p.geom_fine && p.r == 4 && !p.check_block;
-  const int fx0 = 4 * i0 - 4, fy0 = 4 * j0 - 4;
-  if (staged) {
-    if (tid == 0) {
-      mbar_init(&geo_bar, 1);
-      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-      const CUtensorMap *map = static_cast<const CUtensorMap *>(w.zf_map);
-      acquire_maps(map, 1);
-      mbar_expect_tx(&geo_bar, (unsigned)(kFineBoxW * kFineBoxH * sizeof(double)));
-      tma_load_2d(box, map, &geo_bar, fx0, fy0);
-    }
-    __syncthreads();
-  }
-  bool box_ready = false;
-  auto cell_box = [&](int i, int j) -> const double * {
-    if (!staged) return nullptr;
-    if (!box_ready) {
-      if (!mbar_wait(&geo_bar, 0, kBarrierTimeoutNs)) {
-        set_status(w.sc, FREHD_ERR_TIMEOUT);
-        return nullptr;  // the global copy holds the same doubles
-      }
-      box_ready = true;
-    }
-    return box + (long)(4 * j - fy0) * kFineBoxW + (4 * i - fx0);
-  };
   // Each thread evaluates its own cell; threads 0..TBX-1 then evaluate the north
   // halo row (only Om, Vym, s are read from it) and threads TBX..TBX+TBY-1 the
   // east halo column (only Nm, Vxm, s).
@@ -525,22 +548,19 @@ static __device__ __forceinline__ void update_geo_tile(const View &w, int bx, in
     int ind = w.ind_cur[k];
     sh_s[ey][ex] = s;
     if (own) {
-      const SubCell c = compute_sub_area<FREHD_LV_ALL>(w, i, j, s, &ind, depth_old, cell_box(i, j));
+      const SubCell c = compute_sub_area<FREHD_LV_ALL>(w, i, j, s, &ind, depth_old);
       w.ind_nxt[k] = ind;
       sh_Np[ey][ex] = c.Np; sh_Nm[ey][ex] = c.Nm; sh_Op[ey][ex] = c.Op; sh_Om[ey][ex] = c.Om;
       sh_Vxp[ey][ex] = c.Vxp; sh_Vxm[ey][ex] = c.Vxm; sh_Vyp[ey][ex] = c.Vyp; sh_Vym[ey][ex] = c.Vym;
       sh_V[ey][ex] = c.V; sh_Z[ey][ex] = c.Z;
     } else if (ex == TBX) {
-      const SubCell c = compute_sub_area<FREHD_LV_WEST>(w, i, j, s, &ind, depth_old, cell_box(i, j));
+      const SubCell c = compute_sub_area<FREHD_LV_WEST>(w, i, j, s, &ind, depth_old);
       sh_Nm[ey][ex] = c.Nm; sh_Vxm[ey][ex] = c.Vxm;
     } else {
-      const SubCell c = compute_sub_area<FREHD_LV_SOUTH>(w, i, j, s, &ind, depth_old, cell_box(i, j));
+      const SubCell c = compute_sub_area<FREHD_LV_SOUTH>(w, i, j, s, &ind, depth_old);
       sh_Om[ey][ex] = c.Om; sh_Vym[ey][ex] = c.Vym;
     }
   }
-  // the box's copy has landed (or its second bounded wait gave up) before any
-  // thread of the block may leave
-  if (staged && tid == 0) mbar_wait(&geo_bar, 0, kBarrierTimeoutNs);
   __syncthreads();
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int i = i0 + tx, j = j0 + ty;
@@ -1202,15 +1222,6 @@ __global__ void k_finish_batch(const View *views2, const FinishJob *jobs, Scratc
   // the batch's owner sees a failed domain (CFL > 20, a wait that gave up) after
   // this step without reading the domain's statistics
   if (threadIdx.x == 0) *(volatile int *)f.status = *(volatile int *)&sv.sc->status;
-}
-
-cudaError_t geo_kernels_setup() {
-  cudaError_t e = cudaFuncSetAttribute(k_update_geo, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGeoDynSmem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_update_geo_init, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGeoDynSmem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_update_geo_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGeoDynSmem);
-  return e;
 }
 
 // ---------------------------------------------------------------- layout

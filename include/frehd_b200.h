@@ -427,7 +427,9 @@ typedef struct frehd_batch_info_t {
   long long steps;         /* batch steps taken */
 } frehd_batch_info_t;
 
-/* Device memory a domain of this configuration holds, with r x r fine bottoms. */
+/* Device memory a domain of this configuration holds in FP64, with r x r fine
+   bottoms.  The mixed form (frehd_domain_set_precision) adds eight FP32 arrays
+   of the padded grid; a batch admits by the bytes a domain actually holds. */
 int frehd_domain_footprint(const frehd_config *cfg, int r, long long *bytes);
 /* cells_per_cta: cells of a domain per CTA of its CG (the packing granularity):
  * in the CTA-group packing a domain's CG runs on ceil(cells / cells_per_cta) CTAs. */

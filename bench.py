@@ -650,6 +650,9 @@ def measure_batched(args, ws, rank, dev, n_mix, smin, smax, scalars, total_steps
         cpc = tuning["best"]["cells_per_cta"]
         eps_inner = tuning["best"]["eps_inner"]
         packing = tuning["best"]["packing"]
+        tpb = tuning["best"]["tiles_per_block"]
+    else:
+        tpb = args.tiles_per_block
     if eps_inner is None:
         eps_inner = 1e-4
     pk = native.BATCH_TILE_LIST if packing == "tile_list" else native.BATCH_CTA_GROUPS
@@ -657,6 +660,7 @@ def measure_batched(args, ws, rank, dev, n_mix, smin, smax, scalars, total_steps
             for dk in decks]
     b = native.Batch(budget, cpc if cpc > 0 else 1.0, dev)
     b.set_cg_packing(pk)
+    b.set_stencil_tiles(tpb)
     for g in doms:
         b.admit(g, 1)
     for _ in range(W):
@@ -751,6 +755,7 @@ def measure_batched(args, ws, rank, dev, n_mix, smin, smax, scalars, total_steps
                       "cells": int(total_cells), "packing": packing,
                       "cells_per_cta": cpc if packing == "cta_groups" else None,
                       "eps_inner": eps_inner if precision == "mixed" else None,
+                      "stencil_tiles_per_block": tpb,
                       "sharding": "by cell count over ranks" if ws > 1 else None,
                       "deck_gen_s": round(max(p["gen_s"] for p in parts), 1)},
            "plain_form_same_mix": {"value": total / (t_plain / 1e3), "unit": UNIT,
@@ -907,6 +912,9 @@ def main():
     ap.add_argument("--cells-per-cta", type=float, default=0.0,
                     help="batched/served: cells per CTA of a domain's CG (<= 0: batched form "
                          "autotunes it on the mix; served form uses 32768)")
+    ap.add_argument("--tiles-per-block", type=int, default=4,
+                    help="batched form with a given --cells-per-cta: 32x8 stencil tiles per "
+                         "block of the batched stencil kernels (1..8)")
     ap.add_argument("--budget-gb", type=int, default=120)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: FP32 inner CG iterations inside FP64 iterative refinement")

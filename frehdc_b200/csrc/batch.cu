@@ -46,9 +46,10 @@ using namespace frehd;
 
 namespace {
 
-// Stencil tiles (32 x 8) one block of the batched stencil kernels runs, one
-// after another along a tile row: the domain's view is staged once for them.
-constexpr int kTilesPerBlock = 4;
+// Stencil tiles (32 x 8) one block of the batched stencil kernels runs at most,
+// one after another along a tile row: the domain's view is staged once for
+// them (frehd_batch_set_stencil_tiles; the default, and the largest allowed).
+constexpr int kTilesPerBlock = 4, kMaxTilesPerBlock = 8;
 
 struct Slot {
   frehd_domain *d = nullptr;
@@ -102,6 +103,7 @@ struct frehd_batch {
   int any_mixed = 0;        // an admitted domain solves in mixed precision
   // tile-list packing
   int packing = FREHD_BATCH_CTA_GROUPS;
+  int tiles_per_block = kTilesPerBlock;
   DevArray<BDom> bdoms;
   DevArray<BTile> btiles;
   DevArray<BState> bstates;
@@ -221,8 +223,8 @@ int rebuild(frehd_batch *b) {
       if (!d || (d->p.scalarAdv == 2) != (pass == 1)) continue;
       const int gx = (d->gr.nx + 31) / 32, gy = (d->gr.ny + 7) / 8;
       for (int by = 0; by < gy; ++by)
-        for (int bx = 0; bx < gx; bx += kTilesPerBlock)
-          tiles.push_back(BatchTile{s, bx, by, gx, std::min(kTilesPerBlock, gx - bx), 0});
+        for (int bx = 0; bx < gx; bx += b->tiles_per_block)
+          tiles.push_back(BatchTile{s, bx, by, gx, std::min(b->tiles_per_block, gx - bx), 0});
     }
   long nup = 0;
   for (const BatchTile &t : tiles)
@@ -579,6 +581,16 @@ extern "C" int frehd_batch_set_cg_packing(frehd_batch *b, int packing) {
     }
   }
   b->packing = packing;
+  b->dirty = true;
+  return FREHD_OK;
+}
+
+extern "C" int frehd_batch_set_stencil_tiles(frehd_batch *b, int tiles_per_block) {
+  if (!b || tiles_per_block < 1 || tiles_per_block > kMaxTilesPerBlock)
+    return fail(FREHD_ERR_INVALID, "bad argument");
+  BATCH_TRY(cudaSetDevice(b->device));
+  BATCH_TRY(cudaStreamSynchronize(b->stream));  // queued steps use the current tables
+  b->tiles_per_block = tiles_per_block;
   b->dirty = true;
   return FREHD_OK;
 }

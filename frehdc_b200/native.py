@@ -449,6 +449,7 @@ def _declare_batch(L: C.CDLL) -> None:
     L.frehd_batch_stream.argtypes = [_vp, C.POINTER(_vp)]
     L.frehd_batch_set_graph.argtypes = [_vp, C.c_int]
     L.frehd_batch_set_cg_packing.argtypes = [_vp, C.c_int]
+    L.frehd_batch_set_stencil_tiles.argtypes = [_vp, C.c_int]
     L.frehd_server_create.argtypes = [C.c_int, C.c_longlong, C.c_double, C.POINTER(_vp)]
     L.frehd_server_submit.argtypes = [_vp, _vp, C.c_int, C.c_int, C.POINTER(C.c_longlong)]
     L.frehd_server_poll.argtypes = [_vp, C.POINTER(ServerDone), C.c_int, C.c_int, _ip]
@@ -544,8 +545,14 @@ class Batch:
         check(lib().frehd_batch_set_graph(self.h, int(on)), "frehd_batch_set_graph")
 
     def set_cg_packing(self, packing: int):
-        """BATCH_TILE_LIST (default) or BATCH_CTA_GROUPS (frehd_batch_set_cg_packing)."""
+        """BATCH_CTA_GROUPS (default) or BATCH_TILE_LIST (frehd_batch_set_cg_packing)."""
         check(lib().frehd_batch_set_cg_packing(self.h, int(packing)), "frehd_batch_set_cg_packing")
+
+    def set_stencil_tiles(self, tiles_per_block: int):
+        """32 x 8 stencil tiles per block of the batched stencil kernels, 1..8
+        (frehd_batch_set_stencil_tiles)."""
+        check(lib().frehd_batch_set_stencil_tiles(self.h, int(tiles_per_block)),
+              "frehd_batch_set_stencil_tiles")
 
     def close(self):
         if getattr(self, "h", None):

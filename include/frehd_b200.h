@@ -454,6 +454,11 @@ int frehd_batch_set_graph(frehd_batch *b, int on);
  * domains do not fit the CTA groups (the packing then stays the tile list). */
 enum { FREHD_BATCH_TILE_LIST = 0, FREHD_BATCH_CTA_GROUPS = 1 };
 int frehd_batch_set_cg_packing(frehd_batch *b, int packing);
+/* Stencil tiles (32 x 8 cells, consecutive along a row of one domain) each
+ * block of the batched stencil kernels runs, 1..8 (default 4): more tiles per
+ * block stage the domain's view fewer times, fewer give more blocks to spread
+ * over the SMs.  The arithmetic is the same for every value. */
+int frehd_batch_set_stencil_tiles(frehd_batch *b, int tiles_per_block);
 
 /* ------------------------------------------------------------ serving */
 /*

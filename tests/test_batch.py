@@ -29,11 +29,13 @@ def _need_gpu():
 
 
 def _run_batch(names, steps, scratch, cells_per_cta, graph=True, packing=None,
-               precision=native.PRECISION_FP64):
+               precision=native.PRECISION_FP64, tiles_per_block=None):
     b = native.Batch(BUDGET, cells_per_cta)
     b.set_graph(graph)
     if packing is not None:
         b.set_cg_packing(packing)
+    if tiles_per_block is not None:
+        b.set_stencil_tiles(tiles_per_block)
     doms = {}
     for n in names:
         d, _ = deck_for(n, str(scratch))
@@ -101,6 +103,25 @@ def test_same_alone_and_in_mix(graph, packing, scratch):
     for n in names:
         alone, _ = _run_batch([n], 10, scratch, cells_per_cta=1e9, graph=graph, packing=pk)
         assert mismatches(mix[n][0], alone[n][0], FIELDS) == [], n
+
+
+@pytest.mark.parametrize("tiles_per_block", [1, 3, 8])
+def test_stencil_tiles_per_block_same_doubles(tiles_per_block, scratch):
+    """The stencil blocks' tile count changes the launch shape, not the
+    arithmetic: the same doubles as the default four tiles per block."""
+    names = list(SPECS)
+    ref, _ = _run_batch(names, 6, scratch, cells_per_cta=1e9)
+    got, info = _run_batch(names, 6, scratch, cells_per_cta=1e9, tiles_per_block=tiles_per_block)
+    for n in names:
+        assert mismatches(got[n][0], ref[n][0], FIELDS) == [], n
+
+
+def test_stencil_tiles_per_block_checked():
+    b = native.Batch(BUDGET, 1e9)
+    for bad in (0, 9, -1):
+        with pytest.raises(native.FrehdError):
+            b.set_stencil_tiles(bad)
+    b.close()
 
 
 def test_mixed_precision_same_alone_and_in_mix(scratch):

@@ -53,12 +53,15 @@ def test_cache_equals_tables_every_step(kw):
 def test_cache_in_batch_equals_tables():
     """Two fast-tide domains and a bore batched together (32 x 8 stencil tiles of
     several domains per launch, whose halos read other blocks' entries): the
-    final state equals the table-geometry runs."""
+    final state equals the table-geometry runs stepped alone."""
     steps = 25
     decks = [D.make_deck(D.DeckSpec(steps=steps + 5, **kw), with_tables=True)
              for kw in (FAST_TIDE, dict(FAST_TIDE, seed=22, nx=64, ny=100), BORE)]
     fine = [native.domain_from_deck(dk, geometry="fine") for dk in decks]
-    b = native.Batch(8 << 30, 4096.0)
+    # CTA groups at one cell per CTA: every solve on the CTAs its single-domain
+    # run uses, so the batch reproduces those runs bit for bit
+    b = native.Batch(8 << 30, 1.0)
+    b.set_cg_packing(native.BATCH_CTA_GROUPS)
     slots = [b.admit(g, 1) for g in fine]
     for _ in range(steps):
         b.step()

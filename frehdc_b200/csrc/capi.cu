@@ -5,6 +5,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <set>
 #include <vector>
 
 #include "cg1.h"
@@ -26,13 +28,69 @@ using namespace frehd;
 
 namespace {
 
+// A domain's device memory comes from the device's stream-ordered pool on the
+// domain's own stream and goes back the same way.  cudaFree synchronises the
+// whole device, so a server destroying finished requests' domains would stall
+// the batch it steps for everyone else; cudaFreeAsync waits for nothing.  The
+// pool keeps what is freed (release threshold: everything), so the next
+// domain's arrays reuse it.
+void pool_setup(int device) {
+  static std::mutex mu;
+  static std::set<int> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count(device)) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
+  done.insert(device);
+}
+
+cudaError_t dev_alloc(frehd_domain *d, void **p, size_t bytes) {
+  return cudaMallocAsync(p, std::max<size_t>(bytes, 1), d->stream);
+}
+
+void dev_free(frehd_domain *d, void *p) {
+  if (p) cudaFreeAsync(p, d->stream);
+}
+
+// Pinned step-statistics blocks, reused across domains (cudaFreeHost
+// synchronises the device too).
+std::mutex g_out_mu;
+std::vector<StepOut *> g_out_free;
+
+StepOut *take_out_host() {
+  {
+    std::lock_guard<std::mutex> lk(g_out_mu);
+    if (!g_out_free.empty()) {
+      StepOut *o = g_out_free.back();
+      g_out_free.pop_back();
+      return o;
+    }
+  }
+  StepOut *o = nullptr;
+  if (cudaMallocHost((void **)&o, sizeof(StepOut)) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return o;
+}
+
+void give_out_host(StepOut *o) {
+  if (!o) return;
+  std::lock_guard<std::mutex> lk(g_out_mu);
+  g_out_free.push_back(o);
+}
+
 template <class T>
 int dalloc(frehd_domain *d, T **p, long n) {
   void *q = nullptr;
-  cudaError_t e = cudaMalloc(&q, sizeof(T) * (size_t)std::max(n, 1L));
+  cudaError_t e = dev_alloc(d, &q, sizeof(T) * (size_t)std::max(n, 1L));
   if (e != cudaSuccess) {
     cudaGetLastError();
-    return fail(FREHD_ERR_NOMEM, "cudaMalloc of %ld bytes: %s", (long)(sizeof(T) * n),
+    return fail(FREHD_ERR_NOMEM, "device allocation of %ld bytes: %s", (long)(sizeof(T) * n),
                 cudaGetErrorString(e));
   }
   cudaMemsetAsync(q, 0, sizeof(T) * (size_t)std::max(n, 1L), d->stream);
@@ -261,6 +319,7 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
   int rc = check_config(cfg);
   if (rc) return rc;
   CUDA_TRY(cudaSetDevice(device));
+  pool_setup(device);
   frehd_domain *d = new frehd_domain();
   d->cfg = *cfg;
   d->device = device;
@@ -338,8 +397,7 @@ extern "C" int frehd_domain_create(const frehd_config *cfg, int device, frehd_do
   if (!r && cudaMemcpyAsync(d->cg1_maps_dev, &d->cg1_maps, sizeof(Cg1Maps), cudaMemcpyHostToDevice,
                             d->stream) != cudaSuccess)
     r = fail(FREHD_ERR_CUDA, "copying the CG tensor maps to the device failed");
-  if (!r && cudaMallocHost((void **)&d->out_host, sizeof(StepOut)) != cudaSuccess)
-    r = fail(FREHD_ERR_NOMEM, "pinned host allocation failed");
+  if (!r && !(d->out_host = take_out_host())) r = fail(FREHD_ERR_NOMEM, "pinned host allocation failed");
   if (r) {
     frehd_domain_destroy(d);
     return r;
@@ -365,15 +423,13 @@ extern "C" int frehd_domain_destroy(frehd_domain *d) {
   if (d->in_batch) return fail(FREHD_ERR_STATE, "domain is in a batch: release it first");
   cudaSetDevice(d->device);
   if (d->stream) cudaStreamSynchronize(d->stream);
-  for (void *p : d->allocs) cudaFree(p);
-  if (d->tables) cudaFree(d->tables);
-  if (d->zf) cudaFree(d->zf);
-  if (d->lvc) cudaFree(d->lvc);
-  if (d->lvi) cudaFree(d->lvi);
-  if (d->tide) cudaFree(d->tide);
-  for (double *a : {d->inflow, d->wspd, d->wcos, d->wsin})
-    if (a) cudaFree(a);
-  if (d->out_host) cudaFreeHost(d->out_host);
+  if (d->stream) {  // the pool takes the memory back in the domain's stream order
+    for (void *p : d->allocs) dev_free(d, p);
+    for (void *p : {(void *)d->tables, (void *)d->zf, (void *)d->lvc, (void *)d->lvi, (void *)d->tide,
+                    (void *)d->inflow, (void *)d->wspd, (void *)d->wcos, (void *)d->wsin})
+      dev_free(d, p);
+  }
+  give_out_host(d->out_host);
   for (cudaEvent_t e : d->ev) cudaEventDestroy(e);
   if (d->stream) cudaStreamDestroy(d->stream);
   delete d;
@@ -386,16 +442,20 @@ extern "C" int frehd_domain_set_tables(frehd_domain *d, int Ne, const double *ta
     return fail(FREHD_ERR_INVALID, "tables hold %d levels, the config implies Ne=%d", Ne, d->p.Ne);
   CUDA_TRY(cudaSetDevice(d->device));
   const size_t bytes = sizeof(double) * 10 * (size_t)Ne * d->N;
-  if (d->tables) cudaFree(d->tables);
+  dev_free(d, d->tables);
   d->tables = nullptr;
-  if (cudaMalloc(&d->tables, bytes) != cudaSuccess) {
+  d->bytes -= d->tables_bytes;
+  d->tables_bytes = 0;
+  if (dev_alloc(d, (void **)&d->tables, bytes) != cudaSuccess) {
     cudaGetLastError();
+    d->tables = nullptr;
     return fail(FREHD_ERR_NOMEM, "tables: %zu bytes", bytes);
   }
   CUDA_TRY(cudaMemcpyAsync(d->tables, tables, bytes, cudaMemcpyHostToDevice, d->stream));
   d->p.geom_fine = 0;
   d->p.tab = d->tables;
-  d->bytes += (long long)bytes;
+  d->tables_bytes = (long long)bytes;
+  d->bytes += d->tables_bytes;
   d->geom_set = 1;
   return FREHD_OK;
 }
@@ -415,10 +475,11 @@ extern "C" int frehd_domain_set_fine_bottoms_ex(frehd_domain *d, int r, const do
     return fail(FREHD_ERR_INVALID, "r=%d does not match dx/dxf", r);
   CUDA_TRY(cudaSetDevice(d->device));
   const long rows = (long)d->gr.ny * r, cols = (long)d->gr.nx * r;
-  if (d->zf) cudaFree(d->zf);
+  dev_free(d, d->zf);
   d->zf = nullptr;
-  if (cudaMalloc(&d->zf, sizeof(double) * rows * cols) != cudaSuccess) {
+  if (dev_alloc(d, (void **)&d->zf, sizeof(double) * rows * cols) != cudaSuccess) {
     cudaGetLastError();
+    d->zf = nullptr;
     return fail(FREHD_ERR_NOMEM, "fine bottoms: %ld bytes", (long)(sizeof(double) * rows * cols));
   }
   CUDA_TRY(cudaMemcpy2DAsync(d->zf, sizeof(double) * cols, zf, sizeof(double) * fpitch,
@@ -434,9 +495,9 @@ extern "C" int frehd_domain_set_fine_bottoms_ex(frehd_domain *d, int r, const do
   const long tot = d->gr.total;
   if (!d->lvc) {
     const size_t vb = sizeof(double) * 20 * (size_t)tot, ib = sizeof(int) * 2 * (size_t)tot;
-    if (cudaMalloc(&d->lvc, vb) != cudaSuccess || cudaMalloc(&d->lvi, ib) != cudaSuccess) {
+    if (dev_alloc(d, (void **)&d->lvc, vb) != cudaSuccess || dev_alloc(d, (void **)&d->lvi, ib) != cudaSuccess) {
       cudaGetLastError();
-      if (d->lvc) cudaFree(d->lvc);
+      dev_free(d, d->lvc);
       d->lvc = nullptr;
       d->lvi = nullptr;
       return fail(FREHD_ERR_NOMEM, "level-value cache: %zu bytes", vb + ib);
@@ -452,9 +513,9 @@ extern "C" int frehd_domain_set_fine_bottoms_ex(frehd_domain *d, int r, const do
 extern "C" int frehd_domain_set_tide(frehd_domain *d, int n, const double *tideP) {
   if (!d || (n > 0 && !tideP) || n < 0) return fail(FREHD_ERR_INVALID, "bad argument");
   CUDA_TRY(cudaSetDevice(d->device));
-  if (d->tide) cudaFree(d->tide);
+  dev_free(d, d->tide);
   d->tide = nullptr;
-  CUDA_TRY(cudaMalloc(&d->tide, sizeof(double) * std::max(n, 1)));
+  CUDA_TRY(dev_alloc(d, (void **)&d->tide, sizeof(double) * std::max(n, 1)));
   if (n) CUDA_TRY(cudaMemcpyAsync(d->tide, tideP, sizeof(double) * n, cudaMemcpyHostToDevice, d->stream));
   d->ntide = n;
   return FREHD_OK;
@@ -462,11 +523,14 @@ extern "C" int frehd_domain_set_tide(frehd_domain *d, int n, const double *tideP
 
 namespace {
 int upload_series(frehd_domain *d, double **dst, const std::vector<double> &h) {
-  if (*dst) cudaFree(*dst);
+  dev_free(d, *dst);
   *dst = nullptr;
-  CUDA_TRY(cudaMalloc(dst, sizeof(double) * std::max<size_t>(h.size(), 1)));
-  if (!h.empty())
-    CUDA_TRY(cudaMemcpy(*dst, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(dev_alloc(d, (void **)dst, sizeof(double) * std::max<size_t>(h.size(), 1)));
+  if (!h.empty()) {  // h is the caller's temporary: the copy completes before it goes
+    CUDA_TRY(cudaMemcpyAsync(*dst, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice,
+                             d->stream));
+    CUDA_TRY(cudaStreamSynchronize(d->stream));
+  }
   return FREHD_OK;
 }
 }  // namespace

@@ -46,7 +46,7 @@ struct frehd_domain {
   double *tables = nullptr, *zf = nullptr;
   double *lvc = nullptr;  // level-value cache (fine geometry), 20 planes
   int *lvi = nullptr;     // its level indices, 2 planes
-  long long zf_bytes = 0, lvc_bytes = 0;
+  long long zf_bytes = 0, lvc_bytes = 0, tables_bytes = 0;
   frehd::Scratch *sc = nullptr;
   frehd::StepOut *out = nullptr;
   frehd::StepOut *out_host = nullptr;  // pinned

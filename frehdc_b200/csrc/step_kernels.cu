@@ -488,9 +488,12 @@ __device__ NewSurf new_surface(const View &w, int i, int j) {
 // Shared-memory tile: each 32x8 block evaluates the subgrid half-cell values of
 // its cells plus one column east and one row north, then combines them.
 // Blocks of k_update_geo per SM the register allocation aims for (2: 128
-// registers without spills; 3: 80 registers with some spill traffic to L1).
+// registers without spills; 3: 80; 4: 64, with spill traffic to L1).  With the
+// level-value cache the kernel waits on dependent loads, so the extra warps of
+// four blocks pay for the spills: 1.85 ms per 4096^2 step against 2.01 at 3
+// and 2.27 at 2.
 #ifndef FREHD_GEO_MIN_BLOCKS
-#define FREHD_GEO_MIN_BLOCKS 3
+#define FREHD_GEO_MIN_BLOCKS 4
 #endif
 
 template <bool kInit>

@@ -165,10 +165,15 @@ typedef struct frehd_step_stats {
 } frehd_step_stats;
 
 /* Create an empty domain on CUDA device `device`.  Unsupported Config options
- * give FREHD_ERR_UNSUPPORTED. */
+ * give FREHD_ERR_UNSUPPORTED.  A domain's device arrays come from the device's
+ * default stream-ordered memory pool (cudaMallocAsync on the domain's stream);
+ * the first domain on a device sets that pool's release threshold to keep
+ * freed memory for reuse. */
 int frehd_domain_create(const frehd_config *cfg, int device, frehd_domain **out);
-/* Free a domain.  Refused with FREHD_ERR_STATE while the domain is admitted to
- * a batch (frehd_batch_release hands it back first). */
+/* Free a domain: waits for the domain's own stream, then returns its memory to
+ * the pool in that stream's order (no device-wide synchronisation).  Refused
+ * with FREHD_ERR_STATE while the domain is admitted to a batch
+ * (frehd_batch_release hands it back first). */
 int frehd_domain_destroy(frehd_domain *d);
 
 /* Geometry source, one of the two:

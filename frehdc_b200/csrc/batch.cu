@@ -60,12 +60,14 @@ template <class T>
 struct DevArray {
   T *p = nullptr;
   size_t cap = 0;
+  // grows by half at least, so that a stream of admissions reallocates (and
+  // cudaFree synchronises the device) only a logarithmic number of times
   int reserve(size_t n) {
     if (n <= cap) return FREHD_OK;
+    const size_t want = std::max<size_t>(std::max<size_t>(n, cap + cap / 2), 16);
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
-    const size_t want = std::max<size_t>(n, 16);
     if (cudaMalloc(&p, sizeof(T) * want) != cudaSuccess) {
       cudaGetLastError();
       return fail(FREHD_ERR_NOMEM, "batch tables: %zu bytes", sizeof(T) * want);
